@@ -1,0 +1,784 @@
+// C ABI of libaslb.so (declared in include/aslb.h): domain handles, host-side
+// construction of the compact boundary-link lists, and the time loop.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "aslb.h"
+#include "kernels.h"
+#include "mlp.cuh"
+
+using namespace aslb;
+
+namespace {
+thread_local std::string g_err;
+int g_device = 0;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+}  // namespace
+
+#define ASLB_CUDA(expr)                                                                              \
+  do {                                                                                               \
+    cudaError_t e_ = (expr);                                                                         \
+    if (e_ != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define ASLB_CHECK_HANDLE(h) \
+  if (!(h)) return fail(ASLB_ERR_ARG, std::string(__func__) + ": null handle")
+
+struct aslb_lbgk {
+  DomainDev d{};
+  StepParams p{};
+  int closure = CL_NONE;
+  int parity = 0;  // 0: representation A, 1: representation B
+  unsigned flags = 0;
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  long long steps = 0;
+  bool comp_vel = true, comp_rho = true, macro_once = false;
+  double pos0[3] = {0, 0, 0};
+  double dx = 1.0;
+  void* mlp_dev = nullptr;
+  double* red_partials = nullptr;  // moments scratch
+  double* red_out = nullptr;
+  double* host_out = nullptr;      // pinned
+  // time-loop graph cache
+  cudaGraphExec_t graph = nullptr;
+  std::vector<aslb_bc*> graph_bcs;
+  int graph_parity = -1;
+  long long graph_version = -1;
+  long long version = 0;  // bumped by every parameter change
+};
+
+struct aslb_bc {
+  aslb_lbgk* h = nullptr;
+  int4* anchors = nullptr;
+  int n = 0;
+  long long links = 0;
+  BcParams bp{};
+};
+
+struct aslb_force {
+  aslb_lbgk* h = nullptr;
+  int4* cells = nullptr;
+  uint32_t* mask_in = nullptr;
+  int n = 0;
+  float* field = nullptr;
+  double* partials = nullptr;
+  double* out = nullptr;
+  double* host_out = nullptr;
+};
+
+namespace {
+
+void prepare_params(aslb_lbgk* h) {
+  h->p.write_rho = (h->comp_rho || h->macro_once) ? 1 : 0;
+  h->p.write_vel = (h->comp_vel || h->macro_once) ? 1 : 0;
+  h->p.write_macro = h->p.write_rho | h->p.write_vel;
+  h->p.mlp = h->mlp_dev;
+}
+
+int do_step(aslb_lbgk* h) {
+  prepare_params(h);
+  cudaError_t e = launch_step(h->d, h->p, h->closure, h->parity, h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("stream-collide launch: ") + cudaGetErrorString(e));
+  h->parity ^= 1;
+  h->steps += 1;
+  if (h->macro_once) {
+    h->macro_once = false;
+    h->version++;
+  }
+  return ASLB_OK;
+}
+
+int do_bc(aslb_bc* bc) {
+  aslb_lbgk* h = bc->h;
+  cudaError_t e = launch_bc(h->d, bc->anchors, bc->n, bc->bp, h->parity, h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("boundary launch: ") + cudaGetErrorString(e));
+  return ASLB_OK;
+}
+
+void drop_graph(aslb_lbgk* h) {
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  h->graph = nullptr;
+  h->graph_bcs.clear();
+  h->graph_parity = -1;
+}
+
+template <class T>
+int upload(T** dptr, const std::vector<T>& v) {
+  *dptr = nullptr;
+  if (v.empty()) return ASLB_OK;
+  ASLB_CUDA(cudaMalloc((void**)dptr, v.size() * sizeof(T)));
+  ASLB_CUDA(cudaMemcpy(*dptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return ASLB_OK;
+}
+
+bool periodic_axis(const aslb_lbgk* h, int a) { return (h->d.g.periodic >> a) & 1; }
+
+int wrapc(const aslb_lbgk* h, int v, int a) {
+  const int n = a == 0 ? h->d.g.nx : (a == 1 ? h->d.g.ny : h->d.g.nz);
+  return wrap_axis(v, n, periodic_axis(h, a));
+}
+
+bool on_periodic_ghost(const aslb_lbgk* h, int x, int y, int z) {
+  const GridDesc& g = h->d.g;
+  return (periodic_axis(h, 0) && (x < 1 || x > g.nx)) || (periodic_axis(h, 1) && (y < 1 || y > g.ny)) ||
+         (periodic_axis(h, 2) && (z < 1 || z > g.nz));
+}
+
+bool interior(const GridDesc& g, int x, int y, int z) {
+  return x >= 1 && x <= g.nx && y >= 1 && y <= g.ny && z >= 1 && z <= g.nz;
+}
+
+float map_at(const GridDesc& g, const float* map, int x, int y, int z) {
+  if (x < 0 || y < 0 || z < 0 || x >= g.gx || y >= g.gy || z >= g.gz) return -0.9f;  // generateDCFullSafe(map, -.9)
+  return map[aidx(g, x, y, z)];
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* aslb_last_error(void) { return g_err.c_str(); }
+const char* aslb_version(void) { return "aslb 0.1 (sm_100a)"; }
+
+int aslb_set_device(int device) {
+  int n = 0;
+  ASLB_CUDA(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return fail(ASLB_ERR_ARG, "aslb_set_device: no such device");
+  g_device = device;
+  ASLB_CUDA(cudaSetDevice(device));
+  return ASLB_OK;
+}
+
+int aslb_lbgk_create(int nx, int ny, int nz, int q, int storage, double nu, unsigned flags, aslb_lbgk** out) {
+  if (!out) return fail(ASLB_ERR_ARG, "aslb_lbgk_create: out is null");
+  *out = nullptr;
+  if (nx < 1 || ny < 1 || nz < 1) return fail(ASLB_ERR_ARG, "aslb_lbgk_create: sizes must be >= 1");
+  if (q != 15 && q != 19 && q != 27) return fail(ASLB_ERR_ARG, "aslb_lbgk_create: q must be 15, 19 or 27");
+  if (storage != ASLB_F32 && storage != ASLB_F16 && storage != ASLB_F64)
+    return fail(ASLB_ERR_ARG, "aslb_lbgk_create: unknown storage");
+  if (!(nu > 0.0)) return fail(ASLB_ERR_ARG, "aslb_lbgk_create: viscosity must be positive");
+  ASLB_CUDA(cudaSetDevice(g_device));
+  auto* h = new aslb_lbgk();
+  h->device = g_device;
+  h->flags = flags;
+  GridDesc& g = h->d.g;
+  g.nx = nx; g.ny = ny; g.nz = nz;
+  g.gx = nx + 2; g.gy = ny + 2; g.gz = nz + 2;
+  g.pitch = ((g.gz + kZOff + 7) / 8) * 8;
+  g.periodic = int((flags >> 3) & 7u);
+  g.plane = (long long)g.gy * g.pitch;
+  g.dstride = (((long long)g.gx * g.plane + 63) / 64) * 64;
+  g.L = (long long)g.gx * g.gy * g.gz;
+  if (g.dstride >= (1ll << 31)) {
+    delete h;
+    return fail(ASLB_ERR_ARG, "aslb_lbgk_create: domain too large for 32-bit per-direction indexing");
+  }
+  h->d.q = q;
+  h->d.storage = storage;
+  h->comp_vel = !(flags & ASLB_NO_VELOCITY);
+  h->comp_rho = !(flags & ASLB_NO_RHO);
+  h->p.nu = nu;
+  h->p.compressible = (flags & ASLB_INCOMPRESSIBLE) ? 0 : 1;
+  h->p.scale = 1024.0f;
+  h->p.inv_scale = 1.0f / 1024.0f;
+  h->p.cs = 0.17;
+  const size_t fbytes = (size_t)q * g.dstride * storage_bytes(storage);
+  const size_t mb = macro_bytes(storage);
+  cudaError_t e = cudaMalloc(&h->d.F, fbytes);
+  if (e == cudaSuccess) e = cudaMalloc(&h->d.rho, (size_t)g.L * mb);
+  if (e == cudaSuccess) e = cudaMalloc(&h->d.u, 3 * (size_t)g.L * mb);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&h->red_out, 8 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&h->host_out, 8 * sizeof(double));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    std::string msg = std::string("aslb_lbgk_create: ") + cudaGetErrorString(e);
+    aslb_lbgk_destroy(h);
+    return fail(e == cudaErrorMemoryAllocation ? ASLB_ERR_NOMEM : ASLB_ERR_CUDA, msg);
+  }
+  h->stream = h->own_stream;
+  e = cudaMemsetAsync(h->d.F, 0, fbytes, h->stream);
+  if (e == cudaSuccess) {
+    const double u0[3] = {0, 0, 0};
+    e = launch_init_f(h->d, h->p, 1.0, u0, nullptr, nullptr, h->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    std::string msg = std::string("aslb_lbgk_create: ") + cudaGetErrorString(e);
+    aslb_lbgk_destroy(h);
+    return fail(ASLB_ERR_CUDA, msg);
+  }
+  *out = h;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_destroy(aslb_lbgk* h) {
+  if (!h) return ASLB_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  drop_graph(h);
+  cudaFree(h->d.F);
+  cudaFree(h->d.rho);
+  cudaFree(h->d.u);
+  cudaFree(h->mlp_dev);
+  cudaFree(h->red_partials);
+  cudaFree(h->red_out);
+  if (h->host_out) cudaFreeHost(h->host_out);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+  return ASLB_OK;
+}
+
+void* aslb_lbgk_stream(aslb_lbgk* h) { return h ? (void*)h->stream : nullptr; }
+
+int aslb_lbgk_set_stream(aslb_lbgk* h, void* stream) {
+  ASLB_CHECK_HANDLE(h);
+  ASLB_CUDA(cudaStreamSynchronize(h->stream));
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  drop_graph(h);
+  return ASLB_OK;
+}
+
+int aslb_lbgk_set_viscosity(aslb_lbgk* h, double nu) {
+  ASLB_CHECK_HANDLE(h);
+  if (!(nu > 0.0)) return fail(ASLB_ERR_ARG, "aslb_lbgk_set_viscosity: viscosity must be positive");
+  h->p.nu = nu;
+  h->version++;
+  return ASLB_OK;
+}
+
+double aslb_lbgk_get_viscosity(aslb_lbgk* h) { return h ? h->p.nu : 0.0; }
+
+int aslb_lbgk_set_compressible(aslb_lbgk* h, int compressible) {
+  ASLB_CHECK_HANDLE(h);
+  h->p.compressible = compressible ? 1 : 0;
+  h->version++;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_set_omega(aslb_lbgk* h, const double omega[3]) {
+  ASLB_CHECK_HANDLE(h);
+  if (!omega) return fail(ASLB_ERR_ARG, "aslb_lbgk_set_omega: null vector");
+  for (int d = 0; d < 3; ++d) h->p.Om[d] = omega[d];
+  h->p.has_coriolis = 1;
+  h->version++;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_set_macro_output(aslb_lbgk* h, int comp_vel, int comp_rho) {
+  ASLB_CHECK_HANDLE(h);
+  h->comp_vel = comp_vel != 0;
+  h->comp_rho = comp_rho != 0;
+  h->version++;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_request_macro(aslb_lbgk* h) {
+  ASLB_CHECK_HANDLE(h);
+  h->macro_once = true;
+  h->version++;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_set_body_force(aslb_lbgk* h, const double g[3]) {
+  ASLB_CHECK_HANDLE(h);
+  if (!g) return fail(ASLB_ERR_ARG, "aslb_lbgk_set_body_force: null vector");
+  for (int d = 0; d < 3; ++d) h->p.g[d] = g[d];
+  h->p.has_force = (g[0] != 0.0 || g[1] != 0.0 || g[2] != 0.0) ? 1 : 0;
+  h->version++;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_set_closure(aslb_lbgk* h, int closure, double cs) {
+  ASLB_CHECK_HANDLE(h);
+  if (closure < CL_NONE || closure > CL_MLP) return fail(ASLB_ERR_ARG, "aslb_lbgk_set_closure: unknown closure");
+  if (closure == CL_MLP && !h->mlp_dev)
+    return fail(ASLB_ERR_STATE, "aslb_lbgk_set_closure: load a network with aslb_lbgk_set_mlp first");
+  h->closure = closure;
+  h->p.cs = cs;
+  h->version++;
+  return ASLB_OK;
+}
+
+size_t aslb_mlp_layout_bytes(void) { return sizeof(MlpNet); }
+
+int aslb_lbgk_set_mlp(aslb_lbgk* h, const void* net_host, size_t bytes) {
+  ASLB_CHECK_HANDLE(h);
+  if (!net_host || bytes != sizeof(MlpNet))
+    return fail(ASLB_ERR_ARG, "aslb_lbgk_set_mlp: expected " + std::to_string(sizeof(MlpNet)) + " bytes");
+  if (!h->mlp_dev) ASLB_CUDA(cudaMalloc(&h->mlp_dev, sizeof(MlpNet)));
+  ASLB_CUDA(cudaMemcpyAsync(h->mlp_dev, net_host, sizeof(MlpNet), cudaMemcpyHostToDevice, h->stream));
+  ASLB_CUDA(cudaStreamSynchronize(h->stream));
+  h->version++;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_set_fp16_scale(aslb_lbgk* h, double scale) {
+  ASLB_CHECK_HANDLE(h);
+  if (!(scale > 0.0)) return fail(ASLB_ERR_ARG, "aslb_lbgk_set_fp16_scale: scale must be positive");
+  if (h->d.storage == ASLB_F16 && h->steps > 0)
+    return fail(ASLB_ERR_STATE, "aslb_lbgk_set_fp16_scale: set the scale before the first step");
+  h->p.scale = (float)scale;
+  h->p.inv_scale = (float)(1.0 / scale);
+  h->version++;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_set_position(aslb_lbgk* h, const double pos0[3], double dx) {
+  ASLB_CHECK_HANDLE(h);
+  if (!pos0 || !(dx > 0)) return fail(ASLB_ERR_ARG, "aslb_lbgk_set_position: bad arguments");
+  for (int d = 0; d < 3; ++d) h->pos0[d] = pos0[d];
+  h->dx = dx;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_shape(aslb_lbgk* h, int out[6]) {
+  ASLB_CHECK_HANDLE(h);
+  out[0] = h->d.g.nx; out[1] = h->d.g.ny; out[2] = h->d.g.nz;
+  out[3] = h->d.q; out[4] = h->d.storage; out[5] = (int)h->flags;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_init_f(aslb_lbgk* h, double rho, const double u[3]) {
+  ASLB_CHECK_HANDLE(h);
+  const double z[3] = {0, 0, 0};
+  cudaError_t e = launch_init_f(h->d, h->p, rho, u ? u : z, nullptr, nullptr, h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_init_f: ") + cudaGetErrorString(e));
+  h->parity = 0;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_init_f_fields(aslb_lbgk* h, const double* rho, const double* u) {
+  ASLB_CHECK_HANDLE(h);
+  if (!u) return fail(ASLB_ERR_ARG, "aslb_lbgk_init_f_fields: velocity field required");
+  const size_t L = (size_t)h->d.g.L;
+  double *drho = nullptr, *du = nullptr;
+  ASLB_CUDA(cudaMalloc(&du, 3 * L * sizeof(double)));
+  ASLB_CUDA(cudaMemcpyAsync(du, u, 3 * L * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  if (rho) {
+    ASLB_CUDA(cudaMalloc(&drho, L * sizeof(double)));
+    ASLB_CUDA(cudaMemcpyAsync(drho, rho, L * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  }
+  const double z[3] = {0, 0, 0};
+  cudaError_t e = launch_init_f(h->d, h->p, 1.0, z, drho, du, h->stream);
+  cudaError_t e2 = cudaStreamSynchronize(h->stream);
+  cudaFree(du);
+  cudaFree(drho);
+  if (e != cudaSuccess || e2 != cudaSuccess)
+    return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_init_f_fields: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+  h->parity = 0;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_step(aslb_lbgk* h, int nsteps) {
+  ASLB_CHECK_HANDLE(h);
+  if (nsteps < 0) return fail(ASLB_ERR_ARG, "aslb_lbgk_step: negative step count");
+  for (int i = 0; i < nsteps; ++i) {
+    int r = do_step(h);
+    if (r) return r;
+  }
+  return ASLB_OK;
+}
+
+int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int use_graph) {
+  ASLB_CHECK_HANDLE(h);
+  if (nsteps < 0 || nbc < 0 || (nbc > 0 && !bcs)) return fail(ASLB_ERR_ARG, "aslb_lbgk_run: bad arguments");
+  for (int b = 0; b < nbc; ++b)
+    if (!bcs[b] || bcs[b]->h != h) return fail(ASLB_ERR_ARG, "aslb_lbgk_run: boundary of another domain");
+  auto eager = [&](int n) -> int {
+    for (int i = 0; i < n; ++i) {
+      int r = do_step(h);
+      if (r) return r;
+      for (int b = 0; b < nbc; ++b) {
+        r = do_bc(bcs[b]);
+        if (r) return r;
+      }
+    }
+    return ASLB_OK;
+  };
+  if (!use_graph || h->stream == nullptr || nsteps < 4) return eager(nsteps);
+  int done = 0;
+  if (h->macro_once) {
+    int r = eager(1);
+    if (r) return r;
+    done = 1;
+  }
+  std::vector<aslb_bc*> key(bcs, bcs + nbc);
+  const bool valid = h->graph && h->graph_version == h->version && h->graph_bcs == key;
+  if (valid && h->graph_parity != h->parity && done < nsteps) {
+    int r = eager(1);
+    if (r) return r;
+    done += 1;
+  }
+  if (!(h->graph && h->graph_version == h->version && h->graph_bcs == key && h->graph_parity == h->parity)) {
+    drop_graph(h);
+    const int start_parity = h->parity;
+    const long long start_steps = h->steps;
+    cudaGraph_t graph = nullptr;
+    ASLB_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int r = eager(2);
+    cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+    h->parity = start_parity;  // capture enqueued nothing
+    h->steps = start_steps;
+    if (r) {
+      if (graph) cudaGraphDestroy(graph);
+      return r;
+    }
+    if (ce != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&h->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) {
+      h->graph = nullptr;
+      return fail(ASLB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+    }
+    h->graph_bcs = key;
+    h->graph_parity = start_parity;
+    h->graph_version = h->version;
+  }
+  const int pairs = (nsteps - done) / 2;
+  for (int i = 0; i < pairs; ++i) ASLB_CUDA(cudaGraphLaunch(h->graph, h->stream));
+  h->steps += 2LL * pairs;
+  done += 2 * pairs;
+  return eager(nsteps - done);
+}
+
+int aslb_lbgk_sync(aslb_lbgk* h) {
+  ASLB_CHECK_HANDLE(h);
+  ASLB_CUDA(cudaStreamSynchronize(h->stream));
+  return ASLB_OK;
+}
+
+long long aslb_lbgk_steps(aslb_lbgk* h) { return h ? h->steps : -1; }
+
+int aslb_lbgk_read(aslb_lbgk* h, int field, int dtype, void* host_out) {
+  ASLB_CHECK_HANDLE(h);
+  if (!host_out) return fail(ASLB_ERR_ARG, "aslb_lbgk_read: null output");
+  if (dtype != ASLB_F32 && dtype != ASLB_F64) return fail(ASLB_ERR_ARG, "aslb_lbgk_read: dtype must be F32 or F64");
+  const size_t L = (size_t)h->d.g.L;
+  const size_t mb = macro_bytes(h->d.storage);
+  size_t count;
+  void* dev = nullptr;
+  bool own = false;
+  if (field == ASLB_FIELD_RHO) {
+    count = L;
+    dev = h->d.rho;
+  } else if (field == ASLB_FIELD_VELOCITY) {
+    count = 3 * L;
+    dev = h->d.u;
+  } else if (field == ASLB_FIELD_F) {
+    count = (size_t)h->d.q * L;
+    ASLB_CUDA(cudaMalloc(&dev, count * mb));
+    own = true;
+    cudaError_t e = launch_export_f(h->d, h->p, h->parity, dev, h->stream);
+    if (e != cudaSuccess) {
+      cudaFree(dev);
+      return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_read: ") + cudaGetErrorString(e));
+    }
+  } else {
+    return fail(ASLB_ERR_ARG, "aslb_lbgk_read: unknown field");
+  }
+  // Copy straight into the caller's buffer when the types agree (pinned
+  // buffers then transfer at full speed), through a host staging copy otherwise.
+  const bool direct = (mb == 4) == (dtype == ASLB_F32);
+  std::vector<char> tmp(direct ? 0 : count * mb);
+  void* dst = direct ? host_out : (void*)tmp.data();
+  cudaError_t e = cudaMemcpyAsync(dst, dev, count * mb, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (own) cudaFree(dev);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_read: ") + cudaGetErrorString(e));
+  if (!direct) {
+    if (mb == 4) {
+      const float* src = (const float*)tmp.data();
+      for (size_t i = 0; i < count; ++i) ((double*)host_out)[i] = src[i];
+    } else {
+      const double* src = (const double*)tmp.data();
+      for (size_t i = 0; i < count; ++i) ((float*)host_out)[i] = (float)src[i];
+    }
+  }
+  return ASLB_OK;
+}
+
+int aslb_lbgk_write(aslb_lbgk* h, int field, int dtype, const void* host_in) {
+  ASLB_CHECK_HANDLE(h);
+  if (field != ASLB_FIELD_F || !host_in) return fail(ASLB_ERR_ARG, "aslb_lbgk_write: only the F field is writable");
+  if (dtype != ASLB_F32 && dtype != ASLB_F64) return fail(ASLB_ERR_ARG, "aslb_lbgk_write: dtype must be F32 or F64");
+  const size_t count = (size_t)h->d.q * h->d.g.L;
+  const size_t mb = macro_bytes(h->d.storage);
+  const bool direct = (mb == 4) == (dtype == ASLB_F32);
+  std::vector<char> tmp(direct ? 0 : count * mb);
+  if (!direct) {
+    if (mb == 4)
+      for (size_t i = 0; i < count; ++i) ((float*)tmp.data())[i] = (float)((const double*)host_in)[i];
+    else
+      for (size_t i = 0; i < count; ++i) ((double*)tmp.data())[i] = ((const float*)host_in)[i];
+  }
+  void* dev = nullptr;
+  ASLB_CUDA(cudaMalloc(&dev, count * mb));
+  cudaError_t e = cudaMemcpyAsync(dev, direct ? host_in : (const void*)tmp.data(), count * mb,
+                                  cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = launch_import_f(h->d, h->p, dev, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(dev);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_write: ") + cudaGetErrorString(e));
+  h->parity = 0;
+  return ASLB_OK;
+}
+
+void* aslb_lbgk_device_field(aslb_lbgk* h, int field) {
+  if (!h) return nullptr;
+  if (field == ASLB_FIELD_RHO) return h->d.rho;
+  if (field == ASLB_FIELD_VELOCITY) return h->d.u;
+  return nullptr;
+}
+
+int aslb_lbgk_moments(aslb_lbgk* h, double out[4]) {
+  ASLB_CHECK_HANDLE(h);
+  if (!out) return fail(ASLB_ERR_ARG, "aslb_lbgk_moments: null output");
+  const int nb = moments_blocks(h->d.g);
+  if (!h->red_partials) ASLB_CUDA(cudaMalloc((void**)&h->red_partials, (size_t)nb * 4 * sizeof(double)));
+  cudaError_t e = launch_moments(h->d, h->p, h->parity, h->red_partials, h->red_out, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h->host_out, h->red_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_moments: ") + cudaGetErrorString(e));
+  for (int i = 0; i < 4; ++i) out[i] = h->host_out[i];
+  return ASLB_OK;
+}
+
+// ---- boundary conditions ---------------------------------------------------
+
+int aslb_bc_slice_create(aslb_lbgk* h, int kind, unsigned wallmask, double p, const double u[3], aslb_bc** out) {
+  ASLB_CHECK_HANDLE(h);
+  if (!out) return fail(ASLB_ERR_ARG, "aslb_bc_slice_create: out is null");
+  *out = nullptr;
+  if (kind < ASLB_BC_NOSLIP || kind > ASLB_BC_PRESSURE_VELOCITY)
+    return fail(ASLB_ERR_ARG, "aslb_bc_slice_create: unknown slice kind");
+  if (wallmask == 0 || wallmask > 63u) return fail(ASLB_ERR_ARG, "aslb_bc_slice_create: bad wall mask");
+  const GridDesc& g = h->d.g;
+  const int q = h->d.q;
+  // Walls X0, XE, Y0, YE, Z0, ZE with inward normals c_1, c_4, c_2, c_5, c_3, c_6
+  // (src/num/aslBCond.cxx:373-493).
+  static const int normal_dir[6] = {1, 4, 2, 5, 3, 6};
+  const int G[3] = {g.gx, g.gy, g.gz};
+  std::vector<std::pair<long long, int>> links;
+  for (int w = 0; w < 6; ++w) {
+    if (!(wallmask >> w & 1u)) continue;
+    const int ax = w / 2;
+    if (periodic_axis(h, ax)) return fail(ASLB_ERR_ARG, "aslb_bc_slice_create: wall on a periodic axis");
+    const int layer = (w % 2 == 0) ? 1 : G[ax] - 2;
+    const int nd = normal_dir[w];
+    const int t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
+    for (int k = 1; k < q; ++k) {
+      int dot = 0;
+      for (int d = 0; d < 3; ++d) dot += lattice_c(q, k, d) * lattice_c(q, nd, d);
+      if (dot <= 0) continue;
+      for (int i = 1; i < G[t1] - 1; ++i)
+        for (int j = 1; j < G[t2] - 1; ++j) {
+          int a[3];
+          a[ax] = layer;
+          a[t1] = i;
+          a[t2] = j;
+          const int px = a[0] - lattice_c(q, k, 0), py = a[1] - lattice_c(q, k, 1), pz = a[2] - lattice_c(q, k, 2);
+          links.emplace_back(aidx(g, px, py, pz), k);
+        }
+    }
+  }
+  std::sort(links.begin(), links.end());
+  std::vector<int4> anchors;
+  for (size_t i = 0; i < links.size();) {
+    const long long a = links[i].first;
+    unsigned mask = 0;
+    while (i < links.size() && links[i].first == a) mask |= 1u << links[i++].second;
+    const int z = int(a % g.gz);
+    const int y = int((a / g.gz) % g.gy);
+    const int x = int(a / ((long long)g.gz * g.gy));
+    anchors.push_back(make_int4(x, y, z, (int)mask));
+  }
+  auto* bc = new aslb_bc();
+  bc->h = h;
+  bc->n = (int)anchors.size();
+  for (auto& a : anchors) bc->links += __builtin_popcount((unsigned)a.w);
+  bc->bp.kind = kind;
+  bc->bp.compressible = h->p.compressible;
+  bc->bp.p = p;
+  for (int d = 0; d < 3; ++d) bc->bp.u[d] = u ? u[d] : 0.0;
+  bc->bp.scale = h->p.scale;
+  bc->bp.inv_scale = h->p.inv_scale;
+  int r = upload(&bc->anchors, anchors);
+  if (r) {
+    delete bc;
+    return r;
+  }
+  *out = bc;
+  return ASLB_OK;
+}
+
+int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const double u[3], const double omega[3],
+                       const double center[3], aslb_bc** out) {
+  ASLB_CHECK_HANDLE(h);
+  if (!out || !map) return fail(ASLB_ERR_ARG, "aslb_bc_map_create: null argument");
+  *out = nullptr;
+  if (kind < ASLB_BC_MAP_NOSLIP || kind > ASLB_BC_MAP_PRESSURE_VELOCITY)
+    return fail(ASLB_ERR_ARG, "aslb_bc_map_create: unknown map kind");
+  const GridDesc& g = h->d.g;
+  const int q = h->d.q;
+  std::vector<int4> anchors;
+  long long links = 0;
+  // Cell x is processed iff -0.9999 < map(x) <= 0; link k iff map(x + c_k) > 0
+  // (src/num/aslLBGKBC.cxx:235-251), counted when x + c_k is an interior cell.
+  for (int x = 0; x < g.gx; ++x)
+    for (int y = 0; y < g.gy; ++y)
+      for (int z = 0; z < g.gz; ++z) {
+        if (on_periodic_ghost(h, x, y, z)) continue;
+        const float m0 = map[aidx(g, x, y, z)];
+        if (!(m0 <= 0.f && m0 > -0.9999f)) continue;
+        unsigned mask = 0;
+        for (int k = 1; k < q; ++k) {
+          const int qx = wrapc(h, x + lattice_c(q, k, 0), 0), qy = wrapc(h, y + lattice_c(q, k, 1), 1),
+                    qz = wrapc(h, z + lattice_c(q, k, 2), 2);
+          if (!interior(g, qx, qy, qz)) continue;
+          if (map_at(g, map, qx, qy, qz) > 0.f) mask |= 1u << k;
+        }
+        if (mask) {
+          anchors.push_back(make_int4(x, y, z, (int)mask));
+          links += __builtin_popcount(mask);
+        }
+      }
+  if (anchors.size() >= (size_t)(1u << 31)) return fail(ASLB_ERR_ARG, "aslb_bc_map_create: too many boundary cells");
+  auto* bc = new aslb_bc();
+  bc->h = h;
+  bc->n = (int)anchors.size();
+  bc->links = links;
+  bc->bp.kind = kind;
+  bc->bp.compressible = h->p.compressible;
+  bc->bp.p = p;
+  for (int d = 0; d < 3; ++d) {
+    bc->bp.u[d] = u ? u[d] : 0.0;
+    bc->bp.om[d] = omega ? omega[d] : 0.0;
+    bc->bp.cen[d] = center ? center[d] : 0.0;
+    bc->bp.pos0[d] = h->pos0[d];
+  }
+  bc->bp.dx = h->dx;
+  bc->bp.scale = h->p.scale;
+  bc->bp.inv_scale = h->p.inv_scale;
+  int r = upload(&bc->anchors, anchors);
+  if (r) {
+    delete bc;
+    return r;
+  }
+  *out = bc;
+  return ASLB_OK;
+}
+
+int aslb_bc_execute(aslb_bc* bc) {
+  if (!bc) return fail(ASLB_ERR_ARG, "aslb_bc_execute: null handle");
+  return do_bc(bc);
+}
+
+int aslb_bc_destroy(aslb_bc* bc) {
+  if (!bc) return ASLB_OK;
+  if (bc->h) {
+    cudaStreamSynchronize(bc->h->stream);
+    drop_graph(bc->h);
+  }
+  cudaFree(bc->anchors);
+  delete bc;
+  return ASLB_OK;
+}
+
+long long aslb_bc_num_links(aslb_bc* bc) { return bc ? bc->links : -1; }
+
+// ---- surface force ---------------------------------------------------------
+
+int aslb_force_create(aslb_lbgk* h, const float* map, aslb_force** out) {
+  ASLB_CHECK_HANDLE(h);
+  if (!out || !map) return fail(ASLB_ERR_ARG, "aslb_force_create: null argument");
+  *out = nullptr;
+  const GridDesc& g = h->d.g;
+  const int q = h->d.q;
+  std::vector<int4> cells;
+  std::vector<uint32_t> mask_in;
+  // Cells with |map| < 0.9999 (src/num/aslLBGKBC.cxx:730-733); mask0 links from
+  // a solid cell to a fluid interior neighbour, mask_in links from a fluid
+  // interior cell to a solid neighbour (src/num/aslLBGKBC.cxx:713-726).
+  for (int x = 0; x < g.gx; ++x)
+    for (int y = 0; y < g.gy; ++y)
+      for (int z = 0; z < g.gz; ++z) {
+        if (on_periodic_ghost(h, x, y, z)) continue;
+        const float m0 = map[aidx(g, x, y, z)];
+        if (!(std::fabs(m0) < 0.9999f)) continue;
+        const bool in0 = interior(g, x, y, z);
+        unsigned k0 = 0, ki = 0;
+        for (int k = 1; k < q; ++k) {
+          const int qx = wrapc(h, x + lattice_c(q, k, 0), 0), qy = wrapc(h, y + lattice_c(q, k, 1), 1),
+                    qz = wrapc(h, z + lattice_c(q, k, 2), 2);
+          const float mk = map_at(g, map, qx, qy, qz);
+          if (m0 <= 0.f && mk > 0.f && interior(g, qx, qy, qz)) k0 |= 1u << k;
+          if (mk <= 0.f && m0 > 0.f && in0) ki |= 1u << k;
+        }
+        if (k0 | ki) {
+          cells.push_back(make_int4(x, y, z, (int)k0));
+          mask_in.push_back(ki);
+        }
+      }
+  auto* fc = new aslb_force();
+  fc->h = h;
+  fc->n = (int)cells.size();
+  int r = upload(&fc->cells, cells);
+  if (!r) r = upload(&fc->mask_in, mask_in);
+  if (r) {
+    aslb_force_destroy(fc);
+    return r;
+  }
+  cudaError_t e = cudaMalloc((void**)&fc->field, 3 * (size_t)g.L * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemsetAsync(fc->field, 0, 3 * (size_t)g.L * sizeof(float), h->stream);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&fc->partials, (size_t)force_blocks(fc->n) * 6 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&fc->out, 6 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&fc->host_out, 6 * sizeof(double));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    aslb_force_destroy(fc);
+    return fail(ASLB_ERR_CUDA, std::string("aslb_force_create: ") + cudaGetErrorString(e));
+  }
+  *out = fc;
+  return ASLB_OK;
+}
+
+int aslb_force_compute(aslb_force* fc, const double r0[3], float* field_host, double out6[6]) {
+  if (!fc || !out6) return fail(ASLB_ERR_ARG, "aslb_force_compute: null argument");
+  aslb_lbgk* h = fc->h;
+  const double zero[3] = {0, 0, 0};
+  cudaError_t e = launch_force(h->d, fc->cells, fc->mask_in, fc->n, fc->field, r0 ? r0 : zero, h->pos0, h->dx,
+                               h->p.inv_scale, fc->partials, fc->out, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(fc->host_out, fc->out, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess && field_host)
+    e = cudaMemcpyAsync(field_host, fc->field, 3 * (size_t)h->d.g.L * sizeof(float), cudaMemcpyDeviceToHost,
+                        h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_force_compute: ") + cudaGetErrorString(e));
+  for (int i = 0; i < 6; ++i) out6[i] = fc->host_out[i];
+  return ASLB_OK;
+}
+
+int aslb_force_destroy(aslb_force* fc) {
+  if (!fc) return ASLB_OK;
+  if (fc->h) cudaStreamSynchronize(fc->h->stream);
+  cudaFree(fc->cells);
+  cudaFree(fc->mask_in);
+  cudaFree(fc->field);
+  cudaFree(fc->partials);
+  cudaFree(fc->out);
+  if (fc->host_out) cudaFreeHost(fc->host_out);
+  delete fc;
+  return ASLB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,476 @@
+// CUDA kernels of the LBGK hot path for sm_100a: the fused AA-pattern
+// stream-collide, field initialisation and population export/import, the
+// boundary-link kernel shared by every boundary condition, the surface force
+// with its FP64 reduction, and global moments.
+#include <type_traits>
+#include "kernels.h"
+#include "stream_collide.cuh"
+
+namespace aslb {
+
+cudaError_t step_q15(const DomainDev&, const StepParams&, int, int, cudaStream_t);
+cudaError_t step_q19(const DomainDev&, const StepParams&, int, int, cudaStream_t);
+cudaError_t step_q27(const DomainDev&, const StepParams&, int, int, cudaStream_t);
+
+cudaError_t launch_step(const DomainDev& d, const StepParams& p, int closure, int parity_in, cudaStream_t st) {
+  switch (d.q) {
+    case 15: return step_q15(d, p, closure, parity_in, st);
+    case 19: return step_q19(d, p, closure, parity_in, st);
+    case 27: return step_q27(d, p, closure, parity_in, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// Generic dispatch for the remaining kernels (lattice x storage).
+#define ASLB_DISPATCH(d, FN, ...)                                                   \
+  switch ((d).q * 8 + (d).storage) {                                                \
+    case 15 * 8 + ST_F32: return FN<15, float>(__VA_ARGS__);                        \
+    case 15 * 8 + ST_F16: return FN<15, __half>(__VA_ARGS__);                       \
+    case 15 * 8 + ST_F64: return FN<15, double>(__VA_ARGS__);                       \
+    case 19 * 8 + ST_F32: return FN<19, float>(__VA_ARGS__);                        \
+    case 19 * 8 + ST_F16: return FN<19, __half>(__VA_ARGS__);                       \
+    case 19 * 8 + ST_F64: return FN<19, double>(__VA_ARGS__);                       \
+    case 27 * 8 + ST_F32: return FN<27, float>(__VA_ARGS__);                        \
+    case 27 * 8 + ST_F16: return FN<27, __half>(__VA_ARGS__);                       \
+    case 27 * 8 + ST_F64: return FN<27, double>(__VA_ARGS__);                       \
+    default: return cudaErrorInvalidValue;                                          \
+  }
+
+// ---------------------------------------------------------------------------
+// initF: f_i = rho (1 + 3 c.u + 4.5 (c.u)^2 - 1.5 u.u) on every ghosted cell
+// (src/num/aslLBGK.cxx:262-280), representation A.
+template <int Q, class S>
+__global__ void k_init_f(S* __restrict__ F, const GridDesc g, const StepParams p, double rho0, double u0x,
+                         double u0y, double u0z, const double* __restrict__ rho_field,
+                         const double* __restrict__ u_field, typename MacroT<S>::T* __restrict__ rho_out,
+                         typename MacroT<S>::T* __restrict__ u_out) {
+  using Lt = Lattice<Q>;
+  using C = typename Store<S>::C;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  const int x = blockIdx.z;
+  if (z >= g.gz) return;
+  const long long a = aidx(g, x, y, z);
+  const long long s = sidx(g, x, y, z);
+  const C r = rho_field ? C(rho_field[a]) : C(rho0);
+  const C ux = u_field ? C(u_field[a]) : C(u0x);
+  const C uy = u_field ? C(u_field[g.L + a]) : C(u0y);
+  const C uz = u_field ? C(u_field[2 * g.L + a]) : C(u0z);
+  const C vv = ux * ux + uy * uy + uz * uz;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const C cu = ux * C(Lt::c(i, 0)) + uy * C(Lt::c(i, 1)) + uz * C(Lt::c(i, 2));
+    const C fi = r * (C(1) + C(3) * cu + C(4.5) * (cu * cu) - C(1.5) * vv);
+    Store<S>::store(F + (size_t)i * g.dstride + s, fi, p);
+  }
+  rho_out[a] = r;
+  u_out[a] = ux;
+  u_out[g.L + a] = uy;
+  u_out[2 * g.L + a] = uz;
+}
+
+template <int Q, class S>
+static cudaError_t init_impl(const DomainDev& d, const StepParams& p, double rho0, const double* u0,
+                             const double* rho_field, const double* u_field, cudaStream_t st) {
+  using M = typename MacroT<S>::T;
+  dim3 block(128), grid((d.g.gz + 127) / 128, d.g.gy, d.g.gx);
+  k_init_f<Q, S><<<grid, block, 0, st>>>((S*)d.F, d.g, p, rho0, u0[0], u0[1], u0[2], rho_field, u_field,
+                                         (M*)d.rho, (M*)d.u);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init_f(const DomainDev& d, const StepParams& p, double rho0, const double* u0,
+                          const double* rho_field, const double* u_field, cudaStream_t st) {
+  ASLB_DISPATCH(d, init_impl, d, p, rho0, u0, rho_field, u_field, st)
+}
+
+// ---------------------------------------------------------------------------
+// Export f*_i(x) in ASL's layout. In representation B the value sits at the
+// cell it was pushed to; ghost cells whose target leaves the block read NaN.
+template <int Q, class S>
+__global__ void k_export_f(const S* __restrict__ F, const GridDesc g, const StepParams p, int parity,
+                           typename MacroT<S>::T* __restrict__ out) {
+  using Lt = Lattice<Q>;
+  using M = typename MacroT<S>::T;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  const int x = blockIdx.z;
+  if (z >= g.gz) return;
+  const long long a = aidx(g, x, y, z);
+  const bool inter = x >= 1 && x <= g.nx && y >= 1 && y <= g.ny && z >= 1 && z <= g.nz;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    M v;
+    if (parity == 0) {
+      v = M(Store<S>::val(F + (size_t)i * g.dstride + sidx(g, x, y, z), p.inv_scale));
+    } else {
+      int tx = x + Lt::c(i, 0), ty = y + Lt::c(i, 1), tz = z + Lt::c(i, 2);
+      if (inter) {
+        tx = wrap_axis(tx, g.nx, g.periodic & 1);
+        ty = wrap_axis(ty, g.ny, g.periodic & 2);
+        tz = wrap_axis(tz, g.nz, g.periodic & 4);
+      }
+      if (tx < 0 || ty < 0 || tz < 0 || tx >= g.gx || ty >= g.gy || tz >= g.gz)
+        v = M(NAN);
+      else
+        v = M(Store<S>::val(F + (size_t)Lt::inv(i) * g.dstride + sidx(g, tx, ty, tz), p.inv_scale));
+    }
+    out[(long long)i * g.L + a] = v;
+  }
+}
+
+template <int Q, class S>
+static cudaError_t export_impl(const DomainDev& d, const StepParams& p, int parity, void* out, cudaStream_t st) {
+  using M = typename MacroT<S>::T;
+  dim3 block(128), grid((d.g.gz + 127) / 128, d.g.gy, d.g.gx);
+  k_export_f<Q, S><<<grid, block, 0, st>>>((const S*)d.F, d.g, p, parity, (M*)out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_export_f(const DomainDev& d, const StepParams& p, int parity, void* out, cudaStream_t st) {
+  ASLB_DISPATCH(d, export_impl, d, p, parity, out, st)
+}
+
+template <int Q, class S>
+__global__ void k_import_f(S* __restrict__ F, const GridDesc g, const StepParams p,
+                           const typename MacroT<S>::T* __restrict__ in) {
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  const int x = blockIdx.z;
+  if (z >= g.gz) return;
+  const long long a = aidx(g, x, y, z);
+  const long long s = sidx(g, x, y, z);
+#pragma unroll
+  for (int i = 0; i < Q; ++i)
+    Store<S>::set_val(F + (size_t)i * g.dstride + s, typename Store<S>::C(in[(long long)i * g.L + a]), p.scale);
+}
+
+template <int Q, class S>
+static cudaError_t import_impl(const DomainDev& d, const StepParams& p, const void* in, cudaStream_t st) {
+  using M = typename MacroT<S>::T;
+  dim3 block(128), grid((d.g.gz + 127) / 128, d.g.gy, d.g.gx);
+  k_import_f<Q, S><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (const M*)in);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_import_f(const DomainDev& d, const StepParams& p, const void* in, cudaStream_t st) {
+  ASLB_DISPATCH(d, import_impl, d, p, in, st)
+}
+
+// ---------------------------------------------------------------------------
+// Boundary links. An anchor a (ghost or solid cell) with mask bit k stands for
+// the link into the interior fluid cell q = a + c_k along c_k. Two slots are
+// involved: IN, holding f*_k(a) that q pulls next step, and OUT, holding
+// f*_inv(k)(q) that leaves q towards a:
+//   representation A: IN = F[k][a],      OUT = F[inv k][q]
+//   representation B: IN = F[inv k][q],  OUT = F[k][a]
+// Within one boundary condition no OUT slot is an IN slot (IN belongs to a
+// ghost/solid cell, OUT to a fluid cell), so links run in parallel; separate
+// boundary conditions run in the user's order, later writers winning as in ASL.
+template <class S>
+struct BcArith {
+  using C = typename Store<S>::C;
+  static constexpr bool kDev = std::is_same<S, __half>::value;
+  // value of f, in the arithmetic the storage keeps exact (deviation for FP16)
+  __device__ static __forceinline__ C get(const S* p, const BcParams& bp) {
+    return kDev ? Store<S>::dev(p, bp.inv_scale) : Store<S>::val(p, bp.inv_scale);
+  }
+  __device__ static __forceinline__ void put(S* p, C v, const BcParams& bp) {
+    if (kDev)
+      Store<S>::set_dev(p, v, bp.scale);
+    else
+      Store<S>::set_val(p, v, bp.scale);
+  }
+  // representation of a constant population value P (absolute) in get/put arithmetic
+  __device__ static __forceinline__ C rep(C v) { return kDev ? v - C(1) : v; }
+};
+
+template <int Q, class S>
+__global__ void __launch_bounds__(256) k_bc(S* __restrict__ F, const GridDesc g, const int4* __restrict__ anchors,
+                                            int n, const BcParams bp, int parity) {
+  using Lt = Lattice<Q>;
+  using C = typename Store<S>::C;
+  using A = BcArith<S>;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int4 an = anchors[t];
+  const unsigned mask = (unsigned)an.w;
+  const bool px = g.periodic & 1, py = g.periodic & 2, pz = g.periodic & 4;
+  const long long sa = sidx(g, wrap_axis(an.x, g.nx, px), wrap_axis(an.y, g.ny, py), wrap_axis(an.z, g.nz, pz));
+  long long sq[Q];
+#pragma unroll
+  for (int k = 1; k < Q; ++k)
+    sq[k] = sidx(g, wrap_axis(an.x + Lt::c(k, 0), g.nx, px), wrap_axis(an.y + Lt::c(k, 1), g.ny, py),
+                 wrap_axis(an.z + Lt::c(k, 2), g.nz, pz));
+
+  const int kind = bp.kind;
+  C rb = C(0), vel[3] = {C(bp.u[0]), C(bp.u[1]), C(bp.u[2])};
+  if (kind == BCK_MAP_VELOCITY || kind == BCK_MAP_VELOCITY_ROTATION) {
+    // rho_b = sum_k w_k f_inv(k)(a + c_k) / sum_k w_k over fluid neighbours (aslLBGKBC.cxx:312-326)
+    C coef = C(0);
+#pragma unroll
+    for (int k = 1; k < Q; ++k)
+      if (mask >> k & 1u) {
+        const S* out = parity == 0 ? F + (size_t)Lt::inv(k) * g.dstride + sq[k] : F + (size_t)k * g.dstride + sa;
+        coef += C(Lt::w(k));
+        rb += A::get(out, bp) * C(Lt::w(k));
+      }
+    rb /= coef;
+    if (A::kDev) rb += C(1);  // deviations averaged; rb is now absolute
+    if (kind == BCK_MAP_VELOCITY_ROTATION) {
+      const double r0 = bp.pos0[0] + (an.x - 1) * bp.dx - bp.cen[0];
+      const double r1 = bp.pos0[1] + (an.y - 1) * bp.dx - bp.cen[1];
+      const double r2 = bp.pos0[2] + (an.z - 1) * bp.dx - bp.cen[2];
+      vel[0] = C(bp.om[1] * r2 - bp.om[2] * r1);
+      vel[1] = C(bp.om[2] * r0 - bp.om[0] * r2);
+      vel[2] = C(bp.om[0] * r1 - bp.om[1] * r0);
+    }
+  }
+  const C P = C(bp.p);
+  const C vv = vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2];
+#pragma unroll
+  for (int k = 1; k < Q; ++k) {
+    if (!(mask >> k & 1u)) continue;
+    S* in;
+    S* out;
+    if (parity == 0) {
+      in = F + (size_t)k * g.dstride + sa;
+      out = F + (size_t)Lt::inv(k) * g.dstride + sq[k];
+    } else {
+      in = F + (size_t)Lt::inv(k) * g.dstride + sq[k];
+      out = F + (size_t)k * g.dstride + sa;
+    }
+    const C cu = vel[0] * C(Lt::c(k, 0)) + vel[1] * C(Lt::c(k, 1)) + vel[2] * C(Lt::c(k, 2));
+    switch (kind) {
+      case BCK_NOSLIP:
+      case BCK_MAP_NOSLIP:
+        *in = *out;  // f_k(a) = f_inv(k)(a + c_k)   (aslLBGKBC.cxx:106-108, 243-244)
+        break;
+      case BCK_VELOCITY:  // + 6 u.c_k  (aslLBGKBC.cxx:164-167)
+        A::put(in, A::get(out, bp) + C(6) * cu, bp);
+        break;
+      case BCK_PRESSURE:  // = p  (aslLBGKBC.cxx:135-137)
+        A::put(in, A::rep(P), bp);
+        break;
+      case BCK_PRESSURE_VELOCITY:  // = p + 3 u.c_k  (aslLBGKBC.cxx:195-197)
+        A::put(in, A::rep(P) + C(3) * cu, bp);
+        break;
+      case BCK_MAP_VELOCITY:
+      case BCK_MAP_VELOCITY_ROTATION: {  // rho_b + 3 rho_b u.c_k  (aslLBGKBC.cxx:327-338)
+        const C mc = (vel[0] * rb) * C(Lt::c(k, 0)) + (vel[1] * rb) * C(Lt::c(k, 1)) + (vel[2] * rb) * C(Lt::c(k, 2));
+        A::put(in, A::rep(rb) + mc * C(3), bp);
+        break;
+      }
+      case BCK_MAP_PRESSURE_VELOCITY: {  // f_eq(p, u)  (aslLBGKBC.cxx:404-415)
+        C fe;
+        if (bp.compressible)
+          fe = P + C(3) * P * cu + C(4.5) * P * cu * cu - C(1.5) * P * vv;
+        else
+          fe = P + C(3) * cu + C(4.5) * cu * cu - C(1.5) * vv;
+        A::put(in, A::rep(fe), bp);
+        break;
+      }
+    }
+  }
+}
+
+template <int Q, class S>
+static cudaError_t bc_impl(const DomainDev& d, const int4* anchors, int n, const BcParams& bp, int parity,
+                           cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_bc<Q, S><<<(n + 255) / 256, 256, 0, st>>>((S*)d.F, d.g, anchors, n, bp, parity);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bc(const DomainDev& d, const int4* anchors, int n, const BcParams& bp, int parity,
+                      cudaStream_t st) {
+  ASLB_DISPATCH(d, bc_impl, d, anchors, n, bp, parity, st)
+}
+
+// ---------------------------------------------------------------------------
+// Reductions: warp shuffle, then one row of partial sums per block.
+template <int W>
+__device__ __forceinline__ void block_reduce_rows(double (&v)[W], double* __restrict__ partials) {
+  __shared__ double sh[32][W];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < W; ++j)
+    for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_down_sync(0xffffffffu, v[j], o);
+  if (lane == 0)
+#pragma unroll
+    for (int j = 0; j < W; ++j) sh[warp][j] = v[j];
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int j = 0; j < W; ++j) {
+      double a = lane < nw ? sh[lane][j] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+      if (lane == 0) partials[(size_t)blockIdx.x * W + j] = a;
+    }
+  }
+}
+
+// ComputeSurfaceForceMap (aslLBGKBC.cxx:691-736): per listed cell x,
+//   F(x) = sum_k s_k (f_k(x) + f_inv(k)(x + c_k) - 2) w_k c_k
+// with s_k = +1 for links from a solid x (mask0) and -1 from a fluid x (mask_in).
+// f_k(x) + f_inv(k)(x + c_k) is the same pair of slots in both representations.
+constexpr int kForceThreads = 256;
+int force_blocks(int n) { return n > 0 ? (n + kForceThreads - 1) / kForceThreads : 1; }
+
+template <int Q, class S>
+__global__ void __launch_bounds__(kForceThreads)
+    k_force(const S* __restrict__ F, const GridDesc g, const int4* __restrict__ cells,
+            const uint32_t* __restrict__ mask_in, int n, float* __restrict__ field, double r00, double r01,
+            double r02, double p00, double p01, double p02, double dx, float inv_scale,
+            double* __restrict__ partials) {
+  using Lt = Lattice<Q>;
+  using C = typename Store<S>::C;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  if (t < n) {
+    const int4 an = cells[t];
+    const unsigned m0 = (unsigned)an.w, mi = mask_in[t];
+    const bool px = g.periodic & 1, py = g.periodic & 2, pz = g.periodic & 4;
+    const long long sa = sidx(g, an.x, an.y, an.z);
+    C Fx = C(0), Fy = C(0), Fz = C(0);
+#pragma unroll
+    for (int k = 1; k < Q; ++k) {
+      const bool b0 = m0 >> k & 1u, bi = mi >> k & 1u;
+      if (!(b0 || bi)) continue;
+      const long long sq = sidx(g, wrap_axis(an.x + Lt::c(k, 0), g.nx, px), wrap_axis(an.y + Lt::c(k, 1), g.ny, py),
+                                wrap_axis(an.z + Lt::c(k, 2), g.nz, pz));
+      C a;
+      if (std::is_same<S, __half>::value)
+        a = Store<S>::dev(F + (size_t)k * g.dstride + sa, inv_scale) +
+            Store<S>::dev(F + (size_t)Lt::inv(k) * g.dstride + sq, inv_scale);
+      else
+        a = Store<S>::val(F + (size_t)k * g.dstride + sa, inv_scale) +
+            Store<S>::val(F + (size_t)Lt::inv(k) * g.dstride + sq, inv_scale) - C(2);
+      if (bi) a = -a;
+      const C wa = a * C(Lt::w(k));
+      if (Lt::c(k, 0)) Fx += Lt::c(k, 0) > 0 ? wa : -wa;
+      if (Lt::c(k, 1)) Fy += Lt::c(k, 1) > 0 ? wa : -wa;
+      if (Lt::c(k, 2)) Fz += Lt::c(k, 2) > 0 ? wa : -wa;
+    }
+    if (field) {
+      const long long a = aidx(g, an.x, an.y, an.z);
+      field[a] = float(Fx);
+      field[g.L + a] = float(Fy);
+      field[2 * g.L + a] = float(Fz);
+    }
+    const double r0 = p00 + (an.x - 1) * dx - r00;
+    const double r1 = p01 + (an.y - 1) * dx - r01;
+    const double r2 = p02 + (an.z - 1) * dx - r02;
+    const double F0 = double(Fx), F1 = double(Fy), F2 = double(Fz);
+    v[0] = F0;
+    v[1] = F1;
+    v[2] = F2;
+    v[3] = r1 * F2 - r2 * F1;
+    v[4] = r2 * F0 - r0 * F2;
+    v[5] = r0 * F1 - r1 * F0;
+  }
+  block_reduce_rows<6>(v, partials);
+}
+
+__global__ void k_reduce_rows(const double* __restrict__ partials, int nrows, int width, double* __restrict__ out) {
+  __shared__ double sh[256];
+  for (int j = 0; j < width; ++j) {
+    double a = 0.0;
+    for (int r = threadIdx.x; r < nrows; r += blockDim.x) a += partials[(size_t)r * width + j];
+    sh[threadIdx.x] = a;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[j] = sh[0];
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_reduce_rows(const double* partials, int nblocks, int width, double* out, cudaStream_t st) {
+  k_reduce_rows<<<1, 256, 0, st>>>(partials, nblocks, width, out);
+  return cudaGetLastError();
+}
+
+template <int Q, class S>
+static cudaError_t force_impl(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,
+                              const double* r0, const double* pos0, double dx, float inv_scale, double* partials,
+                              double* out6, cudaStream_t st) {
+  const int nb = force_blocks(n);
+  k_force<Q, S><<<nb, kForceThreads, 0, st>>>((const S*)d.F, d.g, cells, mask_in, n, field, r0[0], r0[1], r0[2],
+                                              pos0[0], pos0[1], pos0[2], dx, inv_scale, partials);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_reduce_rows(partials, nb, 6, out6, st);
+}
+
+cudaError_t launch_force(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,
+                         const double* r0, const double* pos0, double dx, float inv_scale, double* partials,
+                         double* out6, cudaStream_t st) {
+  ASLB_DISPATCH(d, force_impl, d, cells, mask_in, n, field, r0, pos0, dx, inv_scale, partials, out6, st)
+}
+
+// ---------------------------------------------------------------------------
+// Mass and momentum of the post-collision populations over interior cells.
+constexpr int kMomentThreads = 256;
+int moments_blocks(const GridDesc& g) {
+  long long cells = (long long)g.nx * g.ny * g.nz;
+  long long b = (cells + kMomentThreads * 8 - 1) / (kMomentThreads * 8);
+  if (b > 4096) b = 4096;
+  return (int)(b < 1 ? 1 : b);
+}
+
+template <int Q, class S>
+__global__ void __launch_bounds__(kMomentThreads)
+    k_moments(const S* __restrict__ F, const GridDesc g, const StepParams p, int parity,
+              double* __restrict__ partials) {
+  using Lt = Lattice<Q>;
+  double v[4] = {0, 0, 0, 0};
+  const long long total = (long long)g.nx * g.ny * g.nz;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int z = int(c % g.nz) + 1;
+    const long long r = c / g.nz;
+    const int y = int(r % g.ny) + 1;
+    const int x = int(r / g.ny) + 1;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      long long s;
+      int dir;
+      if (parity == 0) {
+        s = sidx(g, x, y, z);
+        dir = i;
+      } else {
+        s = sidx(g, wrap_axis(x + Lt::c(i, 0), g.nx, g.periodic & 1), wrap_axis(y + Lt::c(i, 1), g.ny, g.periodic & 2),
+                 wrap_axis(z + Lt::c(i, 2), g.nz, g.periodic & 4));
+        dir = Lt::inv(i);
+      }
+      const double fi = double(Store<S>::val(F + (size_t)dir * g.dstride + s, p.inv_scale));
+      const double wf = Lt::w(i) * fi;
+      v[0] += wf;
+      v[1] += Lt::c(i, 0) * wf;
+      v[2] += Lt::c(i, 1) * wf;
+      v[3] += Lt::c(i, 2) * wf;
+    }
+  }
+  block_reduce_rows<4>(v, partials);
+}
+
+template <int Q, class S>
+static cudaError_t moments_impl(const DomainDev& d, const StepParams& p, int parity, double* partials, double* out4,
+                                cudaStream_t st) {
+  const int nb = moments_blocks(d.g);
+  k_moments<Q, S><<<nb, kMomentThreads, 0, st>>>((const S*)d.F, d.g, p, parity, partials);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_reduce_rows(partials, nb, 4, out4, st);
+}
+
+cudaError_t launch_moments(const DomainDev& d, const StepParams& p, int parity, double* partials, double* out4,
+                           cudaStream_t st) {
+  ASLB_DISPATCH(d, moments_impl, d, p, parity, partials, out4, st)
+}
+
+}  // namespace aslb

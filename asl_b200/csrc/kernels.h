@@ -1,0 +1,50 @@
+// Host-side launch interface of the CUDA kernels (implemented in kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "internal.cuh"
+
+namespace aslb {
+
+enum StorageKind { ST_F32 = 0, ST_F16 = 1, ST_F64 = 2 };
+
+struct DomainDev {
+  GridDesc g;
+  int q;
+  int storage;
+  void* F;     // populations (Q direction arrays)
+  void* rho;   // density, ASL ghosted layout (float, or double for ST_F64)
+  void* u;     // velocity, 3 components of L each
+};
+
+inline size_t storage_bytes(int st) { return st == ST_F16 ? 2 : (st == ST_F64 ? 8 : 4); }
+inline size_t macro_bytes(int st) { return st == ST_F64 ? 8 : 4; }
+
+// One stream-collide step of the AA pattern. parity_in is the representation
+// the populations are in before the step (0 = A, 1 = B).
+cudaError_t launch_step(const DomainDev& d, const StepParams& p, int closure, int parity_in, cudaStream_t st);
+// f = f_eq(rho, u) in representation A for every ghosted cell, rho/u written too.
+// rho_field / u_field: device arrays in ASL layout (double) or null for constants.
+cudaError_t launch_init_f(const DomainDev& d, const StepParams& p, double rho0, const double* u0,
+                          const double* rho_field, const double* u_field, cudaStream_t st);
+// Copy populations to / from ASL's layout (f_i at i*L + ghosted index), values
+// in the macro type (float or double).
+cudaError_t launch_export_f(const DomainDev& d, const StepParams& p, int parity, void* out, cudaStream_t st);
+cudaError_t launch_import_f(const DomainDev& d, const StepParams& p, const void* in, cudaStream_t st);
+// Boundary links: anchors (x, y, z, direction mask) in ghosted coordinates.
+cudaError_t launch_bc(const DomainDev& d, const int4* anchors, int n, const BcParams& bp, int parity,
+                      cudaStream_t st);
+// Surface force: per-cell field (ASL layout, optional) and per-block FP64
+// partial sums of (F, (r - r0) x F), then a fixed-order final sum into out6.
+int force_blocks(int n);
+cudaError_t launch_force(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,
+                         const double* r0, const double* pos0, double dx, float inv_scale, double* partials,
+                         double* out6, cudaStream_t st);
+// Global diagnostics over interior cells: (mass, momentum x, y, z) in FP64.
+int moments_blocks(const GridDesc& g);
+cudaError_t launch_moments(const DomainDev& d, const StepParams& p, int parity, double* partials, double* out4,
+                           cudaStream_t st);
+// Sum `nblocks` rows of `width` doubles into out (fixed order, one block).
+cudaError_t launch_reduce_rows(const double* partials, int nblocks, int width, double* out, cudaStream_t st);
+
+}  // namespace aslb

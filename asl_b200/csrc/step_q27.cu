@@ -1,0 +1,8 @@
+// Stream-collide instantiations for the D3Q27 lattice.
+#include "stream_collide.cuh"
+
+namespace aslb {
+cudaError_t step_q27(const DomainDev& d, const StepParams& p, int closure, int parity_in, cudaStream_t st) {
+  return step_q<27>(d, p, closure, parity_in, st);
+}
+}  // namespace aslb

@@ -1,0 +1,139 @@
+// Fused AA-pattern stream-collide kernel (one interior cell per thread) and its
+// launch helpers. Instantiated per lattice in step_q15.cu / step_q19.cu /
+// step_q27.cu so the instantiations compile in parallel.
+#pragma once
+#include <type_traits>
+#include "kernels.h"
+#include "collide.cuh"
+
+namespace aslb {
+
+template <class S>
+struct MacroT {
+  using T = float;
+};
+template <>
+struct MacroT<double> {
+  using T = double;
+};
+
+// Storage offsets of the neighbours at displacement d in {-1,0,1} per axis
+// (index d + 1), with periodic axes wrapping across the interior.
+__device__ __forceinline__ void nb_offsets(const GridDesc& g, int x, int y, int z, int (&ox)[3], int (&oy)[3],
+                                           int (&oz)[3]) {
+  const int pl = (int)g.plane;
+  ox[0] = -pl; ox[1] = 0; ox[2] = pl;
+  oy[0] = -g.pitch; oy[1] = 0; oy[2] = g.pitch;
+  oz[0] = -1; oz[1] = 0; oz[2] = 1;
+  if (g.periodic & 1) {
+    if (x == 1) ox[0] = (g.nx - 1) * pl;
+    if (x == g.nx) ox[2] = -(g.nx - 1) * pl;
+  }
+  if (g.periodic & 2) {
+    if (y == 1) oy[0] = (g.ny - 1) * g.pitch;
+    if (y == g.ny) oy[2] = -(g.ny - 1) * g.pitch;
+  }
+  if (g.periodic & 4) {
+    if (z == 1) oz[0] = g.nz - 1;
+    if (z == g.nz) oz[2] = -(g.nz - 1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stream + collide, one interior cell per thread. ODD: representation A -> B
+// (reads F[i][x - c_i], writes F[inv i][x + c_i]); EVEN: B -> A (reads
+// F[inv i][x], writes F[i][x]).
+template <int Q, class S, int CL, bool ODD>
+__global__ void __launch_bounds__(256) k_stream_collide(S* __restrict__ F, const GridDesc g, const StepParams p,
+                                                        typename MacroT<S>::T* __restrict__ rho_out,
+                                                        typename MacroT<S>::T* __restrict__ u_out) {
+  using Lt = Lattice<Q>;
+  using C = typename Store<S>::C;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int x = blockIdx.z + 1;
+  if (z > g.nz || y > g.ny) return;
+  const int s = (int)sidx(g, x, y, z);
+  int ox[3], oy[3], oz[3];
+  if (ODD) nb_offsets(g, x, y, z, ox, oy, oz);
+  C f[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const S* src;
+    if (ODD)
+      src = F + (size_t)i * g.dstride +
+            (s + ox[1 - Lt::c(i, 0)] + oy[1 - Lt::c(i, 1)] + oz[1 - Lt::c(i, 2)]);
+    else
+      src = F + (size_t)Lt::inv(i) * g.dstride + s;
+    f[i] = Store<S>::load(src, p);
+  }
+  C rho, u[3];
+  collide_cell<Q, C, CL>(f, p, rho, u);
+  if (p.write_macro) {
+    const long long a = aidx(g, x, y, z);
+    if (p.write_rho) rho_out[a] = rho;
+    if (p.write_vel) {
+      u_out[a] = u[0];
+      u_out[g.L + a] = u[1];
+      u_out[2 * g.L + a] = u[2];
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    S* dst;
+    if (ODD)
+      dst = F + (size_t)Lt::inv(i) * g.dstride +
+            (s + ox[1 + Lt::c(i, 0)] + oy[1 + Lt::c(i, 1)] + oz[1 + Lt::c(i, 2)]);
+    else
+      dst = F + (size_t)i * g.dstride + s;
+    Store<S>::store(dst, f[i], p);
+  }
+}
+
+inline void step_launch_shape(const GridDesc& g, dim3& grid, dim3& block) {
+  int tz = ((g.nz + 31) / 32) * 32;
+  if (tz > 256) tz = 256;
+  int ty = 256 / tz;
+  block = dim3(tz, ty, 1);
+  grid = dim3((g.nz + tz - 1) / tz, (g.ny + ty - 1) / ty, g.nx);
+}
+
+template <int Q, class S, int CL>
+cudaError_t step_q_s_cl(const DomainDev& d, const StepParams& p, int parity_in, cudaStream_t st) {
+  dim3 grid, block;
+  step_launch_shape(d.g, grid, block);
+  using M = typename MacroT<S>::T;
+  if (parity_in == 0)
+    k_stream_collide<Q, S, CL, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+  else
+    k_stream_collide<Q, S, CL, false><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+  return cudaGetLastError();
+}
+
+template <int Q, class S>
+cudaError_t step_q_s(const DomainDev& d, const StepParams& p, int closure, int parity_in, cudaStream_t st) {
+  switch (closure) {
+    case CL_NONE: return step_q_s_cl<Q, S, CL_NONE>(d, p, parity_in, st);
+    case CL_ASL_INTENT: return step_q_s_cl<Q, S, CL_ASL_INTENT>(d, p, parity_in, st);
+    case CL_SMAGORINSKY: return step_q_s_cl<Q, S, CL_SMAGORINSKY>(d, p, parity_in, st);
+    case CL_MLP:
+      // The learned closure is built for the lattices and storages it is trained for.
+      if constexpr ((Q == 19 || Q == 27) && !std::is_same<S, double>::value)
+        return step_q_s_cl<Q, S, CL_MLP>(d, p, parity_in, st);
+      else
+        return cudaErrorNotSupported;
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <int Q>
+cudaError_t step_q(const DomainDev& d, const StepParams& p, int closure, int parity_in, cudaStream_t st) {
+  switch (d.storage) {
+    case ST_F32: return step_q_s<Q, float>(d, p, closure, parity_in, st);
+    case ST_F16: return step_q_s<Q, __half>(d, p, closure, parity_in, st);
+    case ST_F64: return step_q_s<Q, double>(d, p, closure, parity_in, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace aslb

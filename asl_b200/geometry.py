@@ -1,0 +1,248 @@
+"""Signed distance functions and their rasterisation onto a ghosted block.
+
+Follows ASL's DistanceFunction family (src/math/aslDistanceFunction.cxx and
+src/aslGeomInc.cxx of AvtechScientific/ASL): distances are negative inside a
+solid, union is min (``|``), intersection is max (``&``), inversion is ``-``,
+and ``normalize(df, dx)`` clips df / (1.8 dx) to [-1, 1]. ``initData``
+evaluates a function at the physical position of every ghosted cell, in FP32
+like ASL's generated kernels (src/aslGeomInc.cxx:197-219).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+NORMALIZATION_SCALE = 1.8  # DistFNormalization::scaleFactor (aslDistanceFunction.cxx:142)
+
+
+class DistanceFunction:
+    def distance(self, pos: np.ndarray) -> np.ndarray:  # pos: (3, ...) float32
+        raise NotImplementedError
+
+    def __or__(self, other):  # union
+        return _Binary(self, other, np.minimum)
+
+    def __and__(self, other):  # intersection
+        return _Binary(self, other, np.maximum)
+
+    def __neg__(self):
+        return _Unary(self, lambda d: -d)
+
+
+class _Binary(DistanceFunction):
+    def __init__(self, a, b, op):
+        self.a, self.b, self.op = a, b, op
+
+    def distance(self, pos):
+        return self.op(self.a.distance(pos), self.b.distance(pos))
+
+
+class _Unary(DistanceFunction):
+    def __init__(self, a, fn):
+        self.a, self.fn = a, fn
+
+    def distance(self, pos):
+        return self.fn(self.a.distance(pos))
+
+
+def _f32(v):
+    return np.asarray(v, dtype=np.float32).reshape(3, *([1] * 0))
+
+
+class DFSphere(DistanceFunction):
+    """|p - c| - r (aslDistanceFunction.cxx:92-104)."""
+
+    def __init__(self, r, c):
+        self.r = np.float32(r)
+        self.c = np.asarray(c, dtype=np.float32)
+
+    def distance(self, pos):
+        d = pos - self.c.reshape(3, *([1] * (pos.ndim - 1)))
+        return np.sqrt((d * d).sum(0)) - self.r
+
+
+class DFCylinderInf(DistanceFunction):
+    """Infinite cylinder: |(p-c) - ((p-c).l) l| - r (aslDistanceFunction.cxx:104-114)."""
+
+    def __init__(self, r, l, c):
+        l = np.asarray(l, dtype=np.float64)
+        self.r = np.float32(r)
+        self.l = (l / np.linalg.norm(l)).astype(np.float32)
+        self.c = np.asarray(c, dtype=np.float32)
+
+    def distance(self, pos):
+        sh = (3, *([1] * (pos.ndim - 1)))
+        d = pos - self.c.reshape(sh)
+        proj = (d * self.l.reshape(sh)).sum(0)
+        v = d - proj[None] * self.l.reshape(sh)
+        return np.sqrt((v * v).sum(0)) - self.r
+
+
+class DFPlane(DistanceFunction):
+    """p.n/|n| - p0.n/|n| (aslDistanceFunction.cxx:130-140)."""
+
+    def __init__(self, n, p0):
+        n = np.asarray(n, dtype=np.float64)
+        nn = n / math.sqrt(float((n * n).sum()))
+        self.n = nn.astype(np.float32)
+        self.b = np.float32(np.dot(np.asarray(p0, dtype=np.float64), n) / math.sqrt(float((n * n).sum())))
+
+    def distance(self, pos):
+        sh = (3, *([1] * (pos.ndim - 1)))
+        return (pos * self.n.reshape(sh)).sum(0) - self.b
+
+
+class _Normalized(DistanceFunction):
+    def __init__(self, a, dx):
+        self.a = a
+        self.factor = np.float32(1.0 / dx / NORMALIZATION_SCALE)
+
+    def distance(self, pos):
+        d = self.factor * self.a.distance(pos)
+        d = np.where(d > 1.0, np.float32(1.0), d)
+        return np.where(d < -1.0, np.float32(-1.0), d).astype(np.float32)
+
+
+def generateDFSphere(r, c) -> DistanceFunction:
+    return DFSphere(r, c)
+
+
+def generateDFCylinderInf(r, l, c) -> DistanceFunction:
+    return DFCylinderInf(r, l, c)
+
+
+def generateDFPlane(n, p0) -> DistanceFunction:
+    return DFPlane(n, p0)
+
+
+def generateDFCylinder(r, l, c) -> DistanceFunction:
+    """Finite cylinder of axis vector l (its length is the height), aslGeomInc.cxx:98-106."""
+    l = np.asarray(l, dtype=np.float64)
+    c = np.asarray(c, dtype=np.float64)
+    return DFCylinderInf(r, l, c) & DFPlane(l, c + l * 0.5) & DFPlane(-l, c - l * 0.5)
+
+
+def generateDFBox(center, half) -> DistanceFunction:
+    """Axis-aligned box as the intersection of six planes (an extension built the
+    way generateDFConvexPolygonPrism builds prisms, aslGeomInc.cxx:123-140)."""
+    c = np.asarray(center, dtype=np.float64)
+    h = np.asarray(half, dtype=np.float64)
+    res = None
+    for a in range(3):
+        e = np.zeros(3)
+        e[a] = 1.0
+        pair = DFPlane(e, c + h * e) & DFPlane(-e, c - h * e)
+        res = pair if res is None else (res & pair)
+    return res
+
+
+def normalize(df: DistanceFunction, dx: float) -> DistanceFunction:
+    return _Normalized(df, dx)
+
+
+def block_positions(block) -> np.ndarray:
+    """Positions of the ghosted cells in FP32, shape (3, gx, gy, gz)."""
+    gx, gy, gz = block.ghosted
+    axes = [np.float32(block.position[a]) + (np.arange((gx, gy, gz)[a], dtype=np.float32) - np.float32(1.0))
+            * np.float32(block.dx) for a in range(3)]
+    return np.stack(np.meshgrid(*axes, indexing="ij")).astype(np.float32)
+
+
+def initData(block, df: DistanceFunction) -> np.ndarray:
+    """Rasterise a distance function onto the ghosted block (float32 map)."""
+    return np.ascontiguousarray(df.distance(block_positions(block)).astype(np.float32))
+
+
+# ---- seeded porous medium (random non-overlapping spheres) -------------------
+
+@dataclass
+class SpherePack:
+    centers: np.ndarray  # (n, 3), interior-cell coordinates (cell i at position i)
+    radii: np.ndarray    # (n,)
+
+
+def pack_spheres(size, rmin: float, rmax: float, solid_fraction: float, seed: int, periodic_x: bool = True,
+                 attempts: int = 400) -> SpherePack:
+    """Random sequential addition of non-overlapping spheres, radii U[rmin, rmax],
+    placed largest first until the sphere volume reaches ``solid_fraction`` of
+    the box. Spheres stay inside y/z; x is periodic when ``periodic_x``."""
+    nx, ny, nz = size
+    rng = np.random.default_rng(seed)
+    target = solid_fraction * nx * ny * nz
+    radii = []
+    vol = 0.0
+    while vol < target * 1.25:
+        r = float(rng.uniform(rmin, rmax))
+        radii.append(r)
+        vol += 4.0 / 3.0 * math.pi * r ** 3
+    radii.sort(reverse=True)
+    bucket = 2.0 * rmax
+    nbx, nby, nbz = (int(math.ceil(n / bucket)) for n in size)
+    grid: dict = {}
+    centers, placed = [], []
+    placed_vol = 0.0
+    for r in radii:
+        if placed_vol >= target:
+            break
+        for _ in range(attempts):
+            c = np.array([rng.uniform(0, nx) if periodic_x else rng.uniform(r, nx - 1 - r),
+                          rng.uniform(r, ny - 1 - r), rng.uniform(r, nz - 1 - r)])
+            bx, by, bz = int(c[0] // bucket), int(c[1] // bucket), int(c[2] // bucket)
+            ok = True
+            for ix in (bx - 1, bx, bx + 1):
+                jx = ix % nbx if periodic_x else ix
+                for iy in (by - 1, by, by + 1):
+                    for iz in (bz - 1, bz, bz + 1):
+                        for k in grid.get((jx, iy, iz), ()):
+                            d = centers[k] - c
+                            if periodic_x:
+                                d[0] -= nx * round(d[0] / nx)
+                            if d @ d < (placed[k] + r) ** 2:
+                                ok = False
+                                break
+                        if not ok:
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if ok:
+                grid.setdefault((bx % nbx if periodic_x else bx, by, bz), []).append(len(centers))
+                centers.append(c)
+                placed.append(r)
+                placed_vol += 4.0 / 3.0 * math.pi * r ** 3
+                break
+    return SpherePack(np.array(centers).reshape(-1, 3), np.array(placed))
+
+
+def rasterize_spheres(block, pack: SpherePack, periodic_x: bool = True, margin: float = 2.0) -> np.ndarray:
+    """normalize(union of spheres, dx) on the ghosted block without evaluating
+    every sphere everywhere: each sphere updates its bounding box only (cells
+    farther than 1.8 dx from every surface clip to +1 anyway)."""
+    gx, gy, gz = block.ghosted
+    nx = block.size[0]
+    m = np.ones((gx, gy, gz), dtype=np.float32)
+    scale = np.float32(1.0 / (block.dx * NORMALIZATION_SCALE))
+    for c, r in zip(pack.centers, pack.radii):
+        ext = r + margin
+        lo = [int(math.floor(c[a] - ext)) + 1 for a in range(3)]
+        hi = [int(math.ceil(c[a] + ext)) + 1 for a in range(3)]
+        shifts = [0]
+        if periodic_x:
+            shifts = [-nx, 0, nx]
+        for sx in shifts:
+            x0, x1 = max(lo[0] + sx, 0), min(hi[0] + sx, gx - 1)
+            y0, y1 = max(lo[1], 0), min(hi[1], gy - 1)
+            z0, z1 = max(lo[2], 0), min(hi[2], gz - 1)
+            if x0 > x1 or y0 > y1 or z0 > z1:
+                continue
+            xs = (np.arange(x0, x1 + 1, dtype=np.float32) - 1 - np.float32(sx) - np.float32(c[0]))
+            ys = (np.arange(y0, y1 + 1, dtype=np.float32) - 1 - np.float32(c[1]))
+            zs = (np.arange(z0, z1 + 1, dtype=np.float32) - 1 - np.float32(c[2]))
+            d = np.sqrt(xs[:, None, None] ** 2 + ys[None, :, None] ** 2 + zs[None, None, :] ** 2) - np.float32(r)
+            d = np.clip(d * scale, -1.0, 1.0).astype(np.float32)
+            sub = m[x0:x1 + 1, y0:y1 + 1, z0:z1 + 1]
+            np.minimum(sub, d, out=sub)
+    return m

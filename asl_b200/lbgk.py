@@ -1,0 +1,449 @@
+"""Python mirror of ASL's LBGK API over the C ABI of libaslb.so.
+
+Names and argument meaning follow the reference's C++ interface
+(src/num/aslLBGK.h, src/num/aslLBGKBC.h, src/num/aslNumMethod.h of
+AvtechScientific/ASL) so that a script reads like an ASL example program:
+
+    block = Block((128, 64, 64), 1.0)
+    lbgk = LBGK(block, 0.01, d3q19())
+    lbgk.init()
+    LBGKUtilities(lbgk).initF((0.0, 0.0, 0.0))
+    bc = [generateBCConstantVelocity(lbgk, (0.05, 0, 0), [X0]), ...]
+    initAll(bc)
+    for n in range(1000):
+        lbgk.execute(); executeAll(bc)
+
+Fields come back as numpy arrays over the ghosted block, shape
+(nx+2, ny+2, nz+2) (vector fields: (3, nx+2, ny+2, nz+2)), in ASL's
+flattening order (z fastest).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from enum import IntEnum
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+
+class SlicesNames(IntEnum):
+    """Walls of the box (src/num/aslBCond.h:309)."""
+    X0 = 0
+    XE = 1
+    Y0 = 2
+    YE = 3
+    Z0 = 4
+    ZE = 5
+
+
+X0, XE, Y0, YE, Z0, ZE = (SlicesNames(i) for i in range(6))
+
+
+@dataclass(frozen=True)
+class VectorTemplate:
+    """Velocity set (src/math/aslTemplates.h): q directions in ASL's order."""
+    q: int
+
+    @property
+    def vectors(self) -> np.ndarray:
+        return lattice_vectors(self.q)
+
+    @property
+    def quasiparticlesCoefs(self) -> np.ndarray:
+        return lattice_weights(self.q)
+
+
+def lattice_vectors(q: int) -> np.ndarray:
+    v27 = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (-1, 0, 0), (0, -1, 0), (0, 0, -1),
+           (1, 1, 0), (1, -1, 0), (-1, -1, 0), (-1, 1, 0), (0, 1, 1), (0, 1, -1), (0, -1, -1),
+           (0, -1, 1), (1, 0, 1), (1, 0, -1), (-1, 0, -1), (-1, 0, 1), (1, 1, 1), (1, 1, -1),
+           (1, -1, 1), (1, -1, -1), (-1, 1, 1), (-1, 1, -1), (-1, -1, 1), (-1, -1, -1)]
+    if q == 15:
+        return np.array(v27[:7] + v27[19:], dtype=np.int64)
+    return np.array(v27[:q], dtype=np.int64)
+
+
+def lattice_weights(q: int) -> np.ndarray:
+    n2 = (lattice_vectors(q) ** 2).sum(1)
+    table = {15: {0: 2 / 9, 1: 1 / 9, 3: 1 / 72},
+             19: {0: 1 / 3, 1: 1 / 18, 2: 1 / 36},
+             27: {0: 8 / 27, 1: 2 / 27, 2: 1 / 54, 3: 1 / 216}}[q]
+    return np.array([table[int(a)] for a in n2])
+
+
+def d3q15() -> VectorTemplate:
+    return VectorTemplate(15)
+
+
+def d3q19() -> VectorTemplate:
+    return VectorTemplate(19)
+
+
+def d3q27() -> VectorTemplate:
+    return VectorTemplate(27)
+
+
+class Block:
+    """Simulation grid (src/data/aslBlocks.h:56-88): interior size, spacing and
+    the physical position of interior cell (0, 0, 0)."""
+
+    def __init__(self, size: Sequence[int], dx: float = 1.0, position: Sequence[float] = (0.0, 0.0, 0.0)):
+        self.size = tuple(int(s) for s in size)
+        if len(self.size) != 3 or min(self.size) < 1:
+            raise L.ASLError("ASL ERROR: Block: three positive sizes required")
+        self.dx = float(dx)
+        self.position = tuple(float(p) for p in position)
+
+    def getSize(self):
+        return self.size
+
+    @property
+    def ghosted(self):
+        return tuple(s + 2 for s in self.size)
+
+    def c2i(self, c):
+        """Flattened index of ghosted coordinates (z fastest)."""
+        gx, gy, gz = self.ghosted
+        return (c[0] * gy + c[1]) * gz + c[2]
+
+    def positions(self):
+        """Physical coordinates of every ghosted cell, shape (3, gx, gy, gz)."""
+        axes = [self.position[a] + (np.arange(self.ghosted[a]) - 1) * self.dx for a in range(3)]
+        return np.stack(np.meshgrid(*axes, indexing="ij"))
+
+
+_STORAGE = {"f32": L.F32, "f16": L.F16, "f64": L.F64, np.float32: L.F32, np.float64: L.F64}
+
+
+class LBGK:
+    """Fused stream-collide LBGK (src/num/aslLBGK.h:77-131).
+
+    ``storage`` picks the population format: "f32" (ASL with FlT=float), "f64"
+    (FlT=double) or "f16" (shifted FP16 deviations, FP32 arithmetic).
+    ``periodic`` (x, y, z) and ``body_force`` are extensions without an ASL
+    analogue."""
+
+    closure = L.CLOSURE_NONE
+
+    def __init__(self, block: Block, nu: float, vt: VectorTemplate, compVel: bool = True, compRho: bool = True,
+                 storage="f32", periodic=(False, False, False), body_force=None):
+        self.lib = L.load()
+        self.block = block
+        self.vectorTemplate = vt
+        st = _STORAGE[storage]
+        flags = (0 if compVel else L.NO_VELOCITY) | (0 if compRho else L.NO_RHO)
+        for a, p in enumerate(periodic):
+            if p:
+                flags |= (L.PERIODIC_X, L.PERIODIC_Y, L.PERIODIC_Z)[a]
+        self.periodic = tuple(bool(p) for p in periodic)
+        self.storage = storage
+        h = C.c_void_p()
+        nx, ny, nz = block.size
+        L.check(self.lib.aslb_lbgk_create(nx, ny, nz, vt.q, st, float(nu), flags, C.byref(h)), "LBGK")
+        self.h = h
+        L.check(self.lib.aslb_lbgk_set_position(h, L.dvec(block.position), block.dx), "LBGK")
+        if body_force is not None:
+            self.setBodyForce(body_force)
+        self._inited = False
+
+    # lifecycle (NumMethod: src/num/aslNumMethod.h:34-77)
+    def init(self):
+        if self.closure != L.CLOSURE_NONE:
+            L.check(self.lib.aslb_lbgk_set_closure(self.h, self.closure, getattr(self, "cs", 0.17)), "LBGK::init")
+        self._inited = True
+
+    def execute(self, nsteps: int = 1):
+        L.check(self.lib.aslb_lbgk_step(self.h, int(nsteps)), "LBGK::execute")
+
+    def run(self, nsteps: int, bcs: Sequence["BC"] = (), use_graph: bool = True):
+        """`for n: execute(); executeAll(bcs)` in one call (graph replay)."""
+        arr = (C.c_void_p * max(1, len(bcs)))(*[b.h for b in bcs])
+        L.check(self.lib.aslb_lbgk_run(self.h, int(nsteps), arr, len(bcs), 1 if use_graph else 0), "LBGK::run")
+
+    def sync(self):
+        L.check(self.lib.aslb_lbgk_sync(self.h), "LBGK::sync")
+
+    @property
+    def steps(self) -> int:
+        return int(self.lib.aslb_lbgk_steps(self.h))
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.aslb_lbgk_stream(self.h) or 0)
+
+    # parameters
+    def setViscosity(self, nu: float):
+        L.check(self.lib.aslb_lbgk_set_viscosity(self.h, float(nu)), "LBGK::setViscosity")
+
+    def getViscosity(self) -> float:
+        return float(self.lib.aslb_lbgk_get_viscosity(self.h))
+
+    def setOmega(self, w):
+        L.check(self.lib.aslb_lbgk_set_omega(self.h, L.dvec(w)), "LBGK::setOmega")
+
+    def setCompressible(self, flag: bool = True):
+        L.check(self.lib.aslb_lbgk_set_compressible(self.h, 1 if flag else 0), "LBGK::setCompressible")
+
+    def setBodyForce(self, g):
+        L.check(self.lib.aslb_lbgk_set_body_force(self.h, L.dvec(g)), "LBGK::setBodyForce")
+
+    def setMacroOutput(self, compVel: bool, compRho: bool):
+        L.check(self.lib.aslb_lbgk_set_macro_output(self.h, int(compVel), int(compRho)), "LBGK")
+
+    def requestMacro(self):
+        L.check(self.lib.aslb_lbgk_request_macro(self.h), "LBGK")
+
+    def setClosure(self, closure: int, cs: float = 0.17):
+        L.check(self.lib.aslb_lbgk_set_closure(self.h, int(closure), float(cs)), "LBGK::setClosure")
+
+    def setFP16Scale(self, scale: float):
+        L.check(self.lib.aslb_lbgk_set_fp16_scale(self.h, float(scale)), "LBGK")
+
+    def setMLP(self, blob: bytes):
+        buf = C.create_string_buffer(bytes(blob), len(blob))
+        L.check(self.lib.aslb_lbgk_set_mlp(self.h, C.cast(buf, C.c_void_p), len(blob)), "LBGK::setMLP")
+
+    def getVectorTemplate(self) -> VectorTemplate:
+        return self.vectorTemplate
+
+    # data (getRho / getVelocity / getF + acl::map)
+    def _read(self, field: int, ncomp: int, dtype=np.float64) -> np.ndarray:
+        gx, gy, gz = self.block.ghosted
+        out = np.empty((ncomp, gx, gy, gz), dtype=dtype)
+        code = L.F64 if dtype == np.float64 else L.F32
+        L.check(self.lib.aslb_lbgk_read(self.h, field, code, out.ctypes.data_as(C.c_void_p)), "LBGK::read")
+        return out
+
+    def getRho(self, dtype=np.float64) -> np.ndarray:
+        return self._read(L.FIELD_RHO, 1, dtype)[0]
+
+    def getVelocity(self, dtype=np.float64) -> np.ndarray:
+        return self._read(L.FIELD_VELOCITY, 3, dtype)
+
+    def getF(self, dtype=np.float64) -> np.ndarray:
+        return self._read(L.FIELD_F, self.vectorTemplate.q, dtype)
+
+    def setF(self, f: np.ndarray):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        if f.shape != (self.vectorTemplate.q, *self.block.ghosted):
+            raise L.ASLError("ASL ERROR: setF: wrong shape")
+        L.check(self.lib.aslb_lbgk_write(self.h, L.FIELD_F, L.F64, f.ctypes.data_as(C.c_void_p)), "LBGK::setF")
+
+    def moments(self) -> np.ndarray:
+        out = (C.c_double * 4)()
+        L.check(self.lib.aslb_lbgk_moments(self.h, out), "LBGK::moments")
+        return np.array(out[:])
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.aslb_lbgk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class LBGKTurbulence(LBGK):
+    """asl::LBGKTurbulence (src/num/aslLBGK.h:163-171) with its limiter
+    evaluated on a defined f_eq (the reference reads f_eq before assigning it)."""
+    closure = L.CLOSURE_ASL_INTENT
+
+
+class LBGKSmagorinsky(LBGK):
+    """Extension: Smagorinsky closure (Hou et al. 1996), constant ``cs``."""
+    closure = L.CLOSURE_SMAGORINSKY
+
+    def __init__(self, *args, cs: float = 0.17, **kw):
+        self.cs = float(cs)
+        super().__init__(*args, **kw)
+
+
+class LBGKUtilities:
+    """src/num/aslLBGK.h:137-159: initF(vel) or initF(rho, vel); rho and vel
+    are constants or ghosted-block arrays."""
+
+    def __init__(self, lbgk: LBGK):
+        self.num = lbgk
+
+    def initF(self, a, b=None):
+        rho, vel = (1.0, a) if b is None else (a, b)
+        lib = self.num.lib
+        if np.ndim(vel) == 1 and np.ndim(rho) == 0:
+            L.check(lib.aslb_lbgk_init_f(self.num.h, float(rho), L.dvec(vel)), "LBGKUtilities::initF")
+            return
+        g = self.num.block.ghosted
+        v = np.asarray(vel, dtype=np.float64)
+        if v.ndim == 1:
+            v = v.reshape(3, 1, 1, 1)
+        u = np.ascontiguousarray(np.broadcast_to(v, (3, *g)))
+        r = None if np.ndim(rho) == 0 and float(rho) == 1.0 else np.ascontiguousarray(
+            np.broadcast_to(np.asarray(rho, dtype=np.float64), g))
+        L.check(lib.aslb_lbgk_init_f_fields(self.num.h, None if r is None else r.ctypes.data_as(L._pd),
+                                            u.ctypes.data_as(L._pd)), "LBGKUtilities::initF")
+
+
+# ---- boundary conditions -----------------------------------------------------
+
+class BC:
+    """A boundary condition bound to one LBGK (BCond / BCondWithMap)."""
+
+    def __init__(self, lbgk: LBGK, h: C.c_void_p):
+        self.num = lbgk
+        self.h = h
+
+    def init(self):
+        pass
+
+    def execute(self):
+        L.check(self.num.lib.aslb_bc_execute(self.h), "BCond::execute")
+
+    @property
+    def num_links(self) -> int:
+        return int(self.num.lib.aslb_bc_num_links(self.h))
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.num.lib.aslb_bc_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def _wallmask(slices: Iterable[SlicesNames]) -> int:
+    m = 0
+    for s in slices:
+        m |= 1 << int(s)
+    return m
+
+
+def _is_map(x) -> bool:
+    return isinstance(x, np.ndarray)
+
+
+def _map_array(lbgk: LBGK, m: np.ndarray) -> np.ndarray:
+    m = np.ascontiguousarray(m, dtype=np.float32)
+    if m.shape != lbgk.block.ghosted:
+        raise L.ASLError(f"ASL ERROR: map must cover the ghosted block {lbgk.block.ghosted}, got {m.shape}")
+    return m
+
+
+def _slice_bc(lbgk: LBGK, kind: int, slices, p: float = 0.0, u=(0.0, 0.0, 0.0)) -> BC:
+    h = C.c_void_p()
+    L.check(lbgk.lib.aslb_bc_slice_create(lbgk.h, kind, _wallmask(slices), float(p), L.dvec(u), C.byref(h)),
+            "generateBC")
+    return BC(lbgk, h)
+
+
+def _map_bc(lbgk: LBGK, kind: int, m, p=0.0, u=(0.0, 0.0, 0.0), omega=(0.0, 0.0, 0.0), center=(0.0, 0.0, 0.0)) -> BC:
+    arr = _map_array(lbgk, m)
+    h = C.c_void_p()
+    L.check(lbgk.lib.aslb_bc_map_create(lbgk.h, kind, arr.ctypes.data_as(L._pf), float(p), L.dvec(u), L.dvec(omega),
+                                        L.dvec(center), C.byref(h)), "generateBC")
+    return BC(lbgk, h)
+
+
+def generateBCNoSlip(lbgk: LBGK, where) -> BC:
+    """Bounce-back on walls (src/num/aslLBGKBC.cxx:745-751) or on a map (:801-805)."""
+    if _is_map(where):
+        return _map_bc(lbgk, L.BC_MAP_NOSLIP, where)
+    return _slice_bc(lbgk, L.BC_NOSLIP, where)
+
+
+def generateBCConstantVelocity(lbgk: LBGK, v, slices) -> BC:
+    return _slice_bc(lbgk, L.BC_VELOCITY, slices, u=v)
+
+
+def generateBCConstantPressure(lbgk: LBGK, p: float, where) -> BC:
+    if _is_map(where):
+        return _map_bc(lbgk, L.BC_MAP_PRESSURE_VELOCITY, where, p=p)
+    return _slice_bc(lbgk, L.BC_PRESSURE, where, p=p)
+
+
+def generateBCConstantPressureVelocity(lbgk: LBGK, p: float, v, where) -> BC:
+    if _is_map(where):
+        return _map_bc(lbgk, L.BC_MAP_PRESSURE_VELOCITY, where, p=p, u=v)
+    return _slice_bc(lbgk, L.BC_PRESSURE_VELOCITY, where, p=p, u=v)
+
+
+@dataclass
+class PFConstant:
+    """generatePFConstant(v)."""
+    value: tuple
+
+
+@dataclass
+class PFRotationField:
+    """generatePFRotationField(omega, center): u = omega x (r - center)."""
+    omega: tuple
+    center: tuple
+
+
+def generatePFConstant(v) -> PFConstant:
+    return PFConstant(tuple(float(a) for a in v))
+
+
+def generatePFRotationField(omega, center) -> PFRotationField:
+    return PFRotationField(tuple(float(a) for a in omega), tuple(float(a) for a in center))
+
+
+def generateBCVelocity(lbgk: LBGK, velocity, m) -> BC:
+    """BCVelocityMap (src/num/aslLBGKBC.cxx:262-354) with a constant or rotation field."""
+    if isinstance(velocity, PFRotationField):
+        return _map_bc(lbgk, L.BC_MAP_VELOCITY_ROTATION, m, omega=velocity.omega, center=velocity.center)
+    if isinstance(velocity, PFConstant):
+        velocity = velocity.value
+    return _map_bc(lbgk, L.BC_MAP_VELOCITY, m, u=velocity)
+
+
+class ComputeSurfaceForce:
+    """ComputeSurfaceForceMap (src/num/aslLBGKBC.cxx:674-742) plus an FP64
+    reduction to total force and torque about ``r0``."""
+
+    def __init__(self, lbgk: LBGK, m: np.ndarray):
+        self.num = lbgk
+        arr = _map_array(lbgk, m)
+        h = C.c_void_p()
+        L.check(lbgk.lib.aslb_force_create(lbgk.h, arr.ctypes.data_as(L._pf), C.byref(h)), "ComputeSurfaceForce")
+        self.h = h
+
+    def init(self):
+        pass
+
+    def execute(self, r0=(0.0, 0.0, 0.0), field: bool = False):
+        out = (C.c_double * 6)()
+        fld = None
+        if field:
+            fld = np.zeros((3, *self.num.block.ghosted), dtype=np.float32)
+        L.check(self.num.lib.aslb_force_compute(self.h, L.dvec(r0), None if fld is None else fld.ctypes.data_as(L._pf),
+                                                out), "ComputeSurfaceForce::execute")
+        res = np.array(out[:])
+        return (res, fld) if field else res
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.num.lib.aslb_force_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def generateComputeSurfaceForce(lbgk: LBGK, m: np.ndarray) -> ComputeSurfaceForce:
+    return ComputeSurfaceForce(lbgk, m)
+
+
+def initAll(items):
+    for it in items:
+        it.init()
+
+
+def executeAll(items):
+    for it in items:
+        it.execute()

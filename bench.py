@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark: LBGK million lattice-cell updates per second (MLUPS) on one or
+more B200s, on the porous-channel workload (D3Q19, 512x256x256 cells, seeded
+random spheres with solid fraction 0.4, periodic x, no-slip Y/Z walls, body
+force 1e-6, tau 0.6; synthetic data generated from a seed).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0. `value` is whole-job MLUPS (all ranks; one replica
+of the workload per GPU, weak scaling) with populations resident in HBM;
+`e2e` is the same metric through the C ABI with the initial populations
+uploaded from pinned host memory and density/velocity downloaded to pinned
+host memory inside the timed region; `roofline` describes the dominant
+stream-collide kernel; `cpu_baseline` is the CPU oracle on the host cores.
+`--impl reference` times that CPU restatement of the reference's algorithm
+alone (the reference's own OpenCL build is unavailable here).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "D3Q19/27 MLUPS & % HBM roofline; plain FP32 vs FP16/learned at stated error"
+BYTES_PER_CELL = {("f32", 19): 152, ("f16", 19): 76, ("f64", 19): 304, ("f32", 27): 216, ("f16", 27): 108}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", default="512,256,256")
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp16", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=20)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic(name: str):
+    """DRAM bytes per launch from a committed ncu summary (line
+    'traffic_bytes_per_launch: N'), or None."""
+    p = ROOT / "profiles" / name
+    try:
+        for line in p.read_text().splitlines():
+            if line.strip().startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.tmp = None
+
+    def start(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.tmp.flush()
+        rows = [r.split(",") for r in Path(self.tmp.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.tmp.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def parse_size(s):
+    return tuple(int(v) for v in s.split(","))
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(w, steps: int, warm: int = 2):
+    """The CPU oracle (a C++ restatement of the reference's LBGK) on the same
+    workload, FP32, all host threads, over a bounded number of steps."""
+    from oracle import oracle as O
+    O.build()
+    from asl_b200 import workloads as W
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    o = O.Oracle(w.size, w.q, 4, w.nu, flags=8 if w.periodic[0] else 0)
+    if w.body_force:
+        o.set_body_force(w.body_force)
+    o.init_f(1.0, (0, 0, 0))
+    ids = []
+    for s in w.bcs:
+        if s.kind == "map_noslip":
+            ids.append(o.bc_map(10, w.map))
+        else:
+            ids.append(o.bc_slice(W.SLICE_KIND[s.kind], sum(W.WALL_BITS[x] for x in s.walls), s.p, s.u))
+
+    def one():
+        o.step(1)
+        for i in ids:
+            o.bc_execute(i)
+
+    for _ in range(warm):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    dt = time.perf_counter() - t0
+    return {"value": w.cells * steps / dt / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
+            "sample": f"{steps} steps (after {warm} warm-up) of the full {w.size[0]}x{w.size[1]}x{w.size[2]} "
+                      f"workload, FP32, {threads} OpenMP threads"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from asl_b200 import workloads as W
+    w = W.porous_channel(size=parse_size(args.size))
+    steps = max(1, min(args.steps, args.cpu_steps))
+    cb = cpu_baseline(w, steps, warm=max(0, min(args.warmup, 2)))
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "MLUPS", "n_gpus": args.gpus,
+            "steps": steps, "warmup": min(args.warmup, 2), "ms_per_step": w.cells / (cb["value"] * 1e6) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded random spheres)",
+            "config": {"workload": w.name, "lattice": "D3Q19", "cells": w.cells, "storage": "f32",
+                       "implementation": "CPU restatement of the reference LBGK (oracle/lbgk_oracle.cpp); "
+                                         "the reference's OpenCL build is unavailable on this box"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import numpy as np
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from asl_b200 import _lib
+    from asl_b200 import workloads as W
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    _lib.check(_lib.load().aslb_set_device(local), "set_device")
+    w = W.porous_channel(size=parse_size(args.size))
+    K, Wm = args.steps, args.warmup
+
+    def timed_device_run(storage):
+        lb, bcs = W.build_lbgk(w, storage=storage, compVel=False, compRho=False)
+        st = torch.cuda.ExternalStream(lb.stream)
+        lb.run(Wm, bcs, use_graph=True)
+        lb.sync()
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clocks = ClockSampler(local)
+        clocks.start()
+        time.sleep(0.3)
+        e0.record(st)
+        lb.run(K, bcs, use_graph=True)
+        e1.record(st)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        barrier()
+        t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        # Dominant kernel alone: back-to-back stream-collide launches on the same stream.
+        nk = min(K, 200)
+        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k0.record(st)
+        lb.execute(nk)
+        k1.record(st)
+        k1.synchronize()
+        tk = max_over_ranks(k0.elapsed_time(k1) / 1e3 / nk)
+        mom = lb.moments()
+        return lb, bcs, t, tk, clk, mom
+
+    lb, bcs, t, tk, clk, mom = timed_device_run(args.storage)
+    value = w.cells * K * world / t / 1e6
+    nbc = len(bcs)
+    links = sum(b.num_links for b in bcs)
+
+    # End to end through the C ABI: initial populations from pinned host memory,
+    # the ASL time loop (execute + executeAll per step), rho/u back to pinned host memory.
+    q = w.q
+    gx, gy, gz = (s + 2 for s in w.size)
+    L = gx * gy * gz
+    f_host = torch.empty(q * L, dtype=torch.float32, pin_memory=True)
+    rho_host = torch.empty(L, dtype=torch.float32, pin_memory=True)
+    u_host = torch.empty(3 * L, dtype=torch.float32, pin_memory=True)
+    lib = lb.lib
+    _lib.check(lib.aslb_lbgk_read(lb.h, _lib.FIELD_F, _lib.F32, f_host.data_ptr()), "read")
+    st = torch.cuda.ExternalStream(lb.stream)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    _lib.check(lib.aslb_lbgk_write(lb.h, _lib.FIELD_F, _lib.F32, f_host.data_ptr()), "write")
+    for n in range(K):
+        if n == K - 1:
+            lb.requestMacro()
+        lb.execute()
+        for b in bcs:
+            b.execute()
+    _lib.check(lib.aslb_lbgk_read(lb.h, _lib.FIELD_RHO, _lib.F32, rho_host.data_ptr()), "read")
+    _lib.check(lib.aslb_lbgk_read(lb.h, _lib.FIELD_VELOCITY, _lib.F32, u_host.data_ptr()), "read")
+    e1.record(st)
+    e1.synchronize()
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    e2e = {"value": w.cells * K * world / t_e2e / 1e6, "unit": "MLUPS",
+           "h2d_bytes_per_step": q * L * 4 / K, "d2h_bytes_per_step": 4 * L * 4 / K,
+           "timed": "upload of the populations from pinned host memory, K steps of execute()+executeAll(bc) "
+                    "through the C ABI, density and velocity download to pinned host memory"}
+    rho_np = rho_host.numpy().reshape(gx, gy, gz)
+    finite = bool(np.isfinite(rho_np[1:-1, 1:-1, 1:-1]).all())
+    del lb, bcs
+
+    fp16 = None
+    if not args.no_fp16 and args.storage == "f32":
+        lb16, bcs16, t16, tk16, _, mom16 = timed_device_run("f16")
+        v16 = w.cells * K * world / t16 / 1e6
+        fp16 = {"value": v16, "unit": "MLUPS", "speedup_vs_f32": v16 / value,
+                "kernel_ms": tk16 * 1e3,
+                "kernel_frac_of_peak": (BYTES_PER_CELL[("f16", 19)] * w.cells / tk16 / 1e9) / peak_hbm()[0],
+                "mass_drift_vs_f32": abs(mom16[0] - mom[0]) / abs(mom[0])}
+        del lb16, bcs16
+
+    peak, peak_kind = peak_hbm()
+    bpc = BYTES_PER_CELL[(args.storage, w.q)]
+    achieved = bpc * w.cells / tk / 1e9
+    traffic = profile_traffic(f"stream_collide_d3q19_{args.storage}_porous.md")
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_source": peak_kind,
+            "kernel": f"k_stream_collide<19,{args.storage}> (AA pattern, alternating odd/even)",
+            "bytes_per_cell": bpc, "cells_per_launch": w.cells, "kernel_ms": tk * 1e3}
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(w, args.cpu_steps)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": K, "warmup": Wm,
+                "ms_per_step": t / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": args.storage, "data": "synthetic (seeded random spheres, base seed 20261203)",
+                "config": {"workload": w.name, "lattice": "D3Q19", "cells": w.cells, "storage": args.storage,
+                           "solid_fraction": round(w.info["solid_fraction"], 4), "spheres": w.info["spheres"],
+                           "boundary_kernels_per_step": nbc, "boundary_links": links,
+                           "l2": "populations (%.2f GB) far exceed L2; no flush needed" % (bpc / 2 * w.cells / 1e9),
+                           "parallelism": "replica per GPU" if world > 1 else "single GPU",
+                           "time_loop": "CUDA graph of two steps (stream-collide + boundary kernels), replayed"},
+                "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "clocks": clk,
+                "gpu_launches": K * (1 + nbc), "fp16": fp16, "finite": finite,
+                "mass": mom[0]}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,199 @@
+/*
+ * aslb.h -- C ABI of the B200 lattice-Boltzmann library (libaslb.so).
+ *
+ * A drop-in compute layer for the LBGK hot path of the Advanced Simulation
+ * Library (ASL). Every entry point takes plain pointers and sizes, returns
+ * ASLB_OK (0) or a negative error code, and records a message retrievable with
+ * aslb_last_error() (thread-local). Citations name the reference project's
+ * interface each call replaces (paths inside AvtechScientific/ASL).
+ *
+ * Conventions shared with ASL:
+ *  - A domain has nx x ny x nz interior cells and one ghost layer. Host arrays
+ *    use ASL's flattening of the ghosted block, z fastest:
+ *      idx = (x * (ny+2) + y) * (nz+2) + z,   x in [0, nx+1] ...
+ *    (src/data/aslBlocks.h:118-130, src/data/aslDataWithGhostNodes.h:97-145).
+ *    L = (nx+2)(ny+2)(nz+2). Vector fields store component c at c*L + idx.
+ *  - Populations are ASL-normalised (rest state f_i = 1; rho = sum w_i f_i).
+ *    Direction order is ASL's (src/math/aslTemplates.cxx:146-200).
+ *  - Calls enqueue work on the domain's CUDA stream and return; calls that
+ *    deliver data to the host synchronise that stream first, so a program sees
+ *    the blocking semantics of ASL's acl::Kernel::compute()
+ *    (src/acl/Kernels/aclKernel.cxx:289-313).
+ *  - Not thread-safe per handle, as in the reference.
+ */
+#ifndef ASLB_H
+#define ASLB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ASLB_OK 0
+#define ASLB_ERR_ARG (-1)
+#define ASLB_ERR_CUDA (-2)
+#define ASLB_ERR_NOMEM (-3)
+#define ASLB_ERR_STATE (-4)
+
+/* storage of the populations */
+#define ASLB_F32 0 /* FP32 populations, FP32 arithmetic (ASL with FlT=float) */
+#define ASLB_F16 1 /* FP16 shifted deviations (f-1)*scale, FP32 arithmetic */
+#define ASLB_F64 2 /* FP64 populations and arithmetic (ASL with FlT=double) */
+
+/* aslb_lbgk_create flags */
+#define ASLB_NO_VELOCITY 1u    /* LBGK(..., compVel=false, ...)            */
+#define ASLB_NO_RHO 2u         /* LBGK(..., compRho=false, ...)            */
+#define ASLB_INCOMPRESSIBLE 4u /* LBGK::setCompressible(false)             */
+#define ASLB_PERIODIC_X 8u     /* extension: periodic axes (no ASL analogue) */
+#define ASLB_PERIODIC_Y 16u
+#define ASLB_PERIODIC_Z 32u
+
+/* closures (aslb_lbgk_set_closure) */
+#define ASLB_CLOSURE_NONE 0        /* asl::LBGK                                        */
+#define ASLB_CLOSURE_ASL_INTENT 1  /* asl::LBGKTurbulence, f_eq evaluated before use     */
+#define ASLB_CLOSURE_SMAGORINSKY 2 /* extension: Smagorinsky, Hou et al. (1996)          */
+#define ASLB_CLOSURE_MLP 3         /* extension: learned Cs^2 from a 9-64-64-1 network  */
+
+/* boundary conditions (slice kinds 0-3, map kinds 10-13) */
+#define ASLB_BC_NOSLIP 0
+#define ASLB_BC_VELOCITY 1
+#define ASLB_BC_PRESSURE 2
+#define ASLB_BC_PRESSURE_VELOCITY 3
+#define ASLB_BC_MAP_NOSLIP 10
+#define ASLB_BC_MAP_VELOCITY 11
+#define ASLB_BC_MAP_VELOCITY_ROTATION 12
+#define ASLB_BC_MAP_PRESSURE_VELOCITY 13
+
+/* walls for slice BCs: bit w for asl::SlicesNames {X0,XE,Y0,YE,Z0,ZE}
+ * (src/num/aslBCond.h:309) */
+#define ASLB_WALL(w) (1u << (w))
+
+/* fields for aslb_lbgk_read / aslb_lbgk_write */
+#define ASLB_FIELD_RHO 0
+#define ASLB_FIELD_VELOCITY 1
+#define ASLB_FIELD_F 2
+
+typedef struct aslb_lbgk aslb_lbgk;
+typedef struct aslb_bc aslb_bc;
+typedef struct aslb_force aslb_force;
+
+/* Last error message of the calling thread ("" if none). */
+const char* aslb_last_error(void);
+/* Library version string. */
+const char* aslb_version(void);
+/* Select the CUDA device used by subsequent create calls
+ * (ApplicationParametersManager --device, src/acl/aclHardware.cxx:98-120). */
+int aslb_set_device(int device);
+
+/* ---- LBGK domain ------------------------------------------------------- */
+
+/* asl::LBGK::LBGK(Block b, Param nu, const VectorTemplate* vT, bool compVel,
+ *                 bool compRho, CommandQueue)  (src/num/aslLBGK.cxx:114-158).
+ * q = 15, 19 or 27; storage = ASLB_F32/F16/F64 (ASL selects FP32/FP64 by the
+ * type of nu). Allocates the populations once (AA pattern: one copy, not
+ * ASL's 2L+4m pool), density and velocity fields, and a CUDA stream. */
+int aslb_lbgk_create(int nx, int ny, int nz, int q, int storage, double nu, unsigned flags, aslb_lbgk** out);
+int aslb_lbgk_destroy(aslb_lbgk* h);
+
+/* CUDA stream the domain enqueues on (cudaStream_t as void*). set_stream
+ * replaces it with a caller-owned stream (NULL restores the own stream). */
+void* aslb_lbgk_stream(aslb_lbgk* h);
+int aslb_lbgk_set_stream(aslb_lbgk* h, void* stream);
+
+/* LBGK::setViscosity / getViscosity (declared, never defined in the reference:
+ * src/num/aslLBGK.h:117-118). */
+int aslb_lbgk_set_viscosity(aslb_lbgk* h, double nu);
+double aslb_lbgk_get_viscosity(aslb_lbgk* h);
+/* LBGK::setCompressible (src/num/aslLBGK.h:198-201). */
+int aslb_lbgk_set_compressible(aslb_lbgk* h, int compressible);
+/* LBGK::setOmega: angular velocity of the rotating frame (Coriolis term,
+ * src/num/aslLBGK.cxx:207-208,252-255). */
+int aslb_lbgk_set_omega(aslb_lbgk* h, const double omega[3]);
+/* Which of rho / u the step writes (compVel/compRho of the constructor). */
+int aslb_lbgk_set_macro_output(aslb_lbgk* h, int comp_vel, int comp_rho);
+/* Write rho and u on the next step only, whatever the flags say. */
+int aslb_lbgk_request_macro(aslb_lbgk* h);
+/* Extension: body force per unit mass (Guo et al. 2002 forcing). */
+int aslb_lbgk_set_body_force(aslb_lbgk* h, const double g[3]);
+/* asl::LBGKTurbulence (src/num/aslLBGK.cxx:298-355) and extensions; cs is the
+ * Smagorinsky constant (ignored otherwise). */
+int aslb_lbgk_set_closure(aslb_lbgk* h, int closure, double cs);
+/* Learned closure network: `bytes` of the packed device layout produced by
+ * the training code (see aslb_mlp_layout_bytes). Copied to the device. */
+size_t aslb_mlp_layout_bytes(void);
+int aslb_lbgk_set_mlp(aslb_lbgk* h, const void* net_host, size_t bytes);
+/* FP16 storage scale: stored half = (f - 1) * scale (default 1024). */
+int aslb_lbgk_set_fp16_scale(aslb_lbgk* h, double scale);
+/* Physical position of interior cell (0,0,0) and the spacing
+ * (asl::Block::position / dx, src/data/aslBlocks.h:56-88). */
+int aslb_lbgk_set_position(aslb_lbgk* h, const double pos0[3], double dx);
+/* Domain shape: out[0..2] interior sizes, out[3] q, out[4] storage,
+ * out[5] flags. */
+int aslb_lbgk_shape(aslb_lbgk* h, int out[6]);
+
+/* LBGKUtilities::initF(rho, vel) with constants (src/num/aslLBGK.cxx:262-280). */
+int aslb_lbgk_init_f(aslb_lbgk* h, double rho, const double u[3]);
+/* initF with fields: rho (L doubles, or NULL for 1) and u (3L doubles), host. */
+int aslb_lbgk_init_f_fields(aslb_lbgk* h, const double* rho, const double* u);
+
+/* LBGK::execute(): one stream + collide step (src/num/aslLBGK.cxx:237-250,
+ * src/num/aslSingleKernelNM.cxx:48-53), nsteps times. Boundary conditions are
+ * separate objects, executed by the caller after each step as in ASL. */
+int aslb_lbgk_step(aslb_lbgk* h, int nsteps);
+/* The reference's time loop `for n: lbgk->execute(); executeAll(bc);`
+ * (examples/flow/flow.cc:124-134) as one call. use_graph != 0 records two
+ * steps into a CUDA graph once and replays it. */
+int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int use_graph);
+/* Wait for all work of the domain. */
+int aslb_lbgk_sync(aslb_lbgk* h);
+/* Steps taken so far. */
+long long aslb_lbgk_steps(aslb_lbgk* h);
+
+/* Host copies in ASL layout (they synchronise): RHO (L), VELOCITY (3L),
+ * F (q*L, post-collision populations f*_i). dtype is ASLB_F32 (float) or
+ * ASLB_F64 (double). getRho()/getVelocity()/getF() + acl::map
+ * (src/acl/DataTypes/aclMemBlock.cxx:111-136). */
+int aslb_lbgk_read(aslb_lbgk* h, int field, int dtype, void* host_out);
+/* Load populations (field F only), ASL layout; used for restart. */
+int aslb_lbgk_write(aslb_lbgk* h, int field, int dtype, const void* host_in);
+/* Device pointer of RHO or VELOCITY (ASL layout; float, double for F64). */
+void* aslb_lbgk_device_field(aslb_lbgk* h, int field);
+/* Global FP64 moments of the post-collision populations over interior cells:
+ * out[0] mass, out[1..3] momentum (a blow-up watchdog). Synchronises. */
+int aslb_lbgk_moments(aslb_lbgk* h, double out[4]);
+
+/* ---- boundary conditions ----------------------------------------------- */
+
+/* generateBCNoSlip / generateBCConstantVelocity / generateBCConstantPressure /
+ * generateBCConstantPressureVelocity on walls (src/num/aslLBGKBC.cxx:745-798,
+ * point lists src/num/aslBCond.cxx:373-510). wallmask: ASLB_WALL bits. */
+int aslb_bc_slice_create(aslb_lbgk* h, int kind, unsigned wallmask, double p, const double u[3], aslb_bc** out);
+/* Map BCs on a distance map (L floats, host, ASL layout; map > 0 fluid):
+ * generateBCNoSlip(map), generateBCVelocity(PF, map) with a constant field or
+ * a rotation field u = omega x (r - center), generateBCConstantPressure(map) /
+ * generateBCConstantPressureVelocity(map) (src/num/aslLBGKBC.cxx:205-438). */
+int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const double u[3], const double omega[3],
+                       const double center[3], aslb_bc** out);
+/* BCond::execute() (src/num/aslLBGKBC.cxx:80-83, 257-260). */
+int aslb_bc_execute(aslb_bc* bc);
+int aslb_bc_destroy(aslb_bc* bc);
+/* Number of boundary links (direction slots written per execute). */
+long long aslb_bc_num_links(aslb_bc* bc);
+
+/* ---- surface force ------------------------------------------------------- */
+
+/* generateComputeSurfaceForce(lbgk, forceField, map)
+ * (src/num/aslLBGKBC.cxx:674-742, 915-921). */
+int aslb_force_create(aslb_lbgk* h, const float* map, aslb_force** out);
+/* ComputeSurfaceForceMap::execute() plus the FP64 reduction the reference
+ * lacks: out6 = (sum F, sum (r - r0) x F). field_host (3L floats, optional)
+ * receives the per-cell force field. Synchronises. */
+int aslb_force_compute(aslb_force* fc, const double r0[3], float* field_host, double out6[6]);
+int aslb_force_destroy(aslb_force* fc);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ASLB_H */

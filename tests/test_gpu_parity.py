@@ -1,0 +1,254 @@
+"""GPU parity: the CUDA path (through libaslb.so's C ABI) against the CPU oracle.
+
+Tolerances: FP64 storage must match the FP64 oracle to 1e-12 (rounding
+only); FP32 storage the FP32 oracle to 2e-6 absolute on populations for a few
+steps (fused multiply-add contraction differs); the canonical cylinder
+channel to relative L2 <= 1e-4 on rho and u over interior fluid cells and
+<= 1e-4 on the drag after 1000 steps.
+"""
+import numpy as np
+import pytest
+
+from asl_b200 import lbgk as A
+from asl_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+I4 = (slice(None), slice(1, -1), slice(1, -1), slice(1, -1))
+WALLS = {"X0": 1, "XE": 2, "Y0": 4, "YE": 8, "Z0": 16, "ZE": 32}
+SLICE = {"noslip": 0, "velocity": 1, "pressure": 2, "pressure_velocity": 3}
+MAPK = {"noslip": 10, "velocity": 11, "pressure_velocity": 13}
+VT = {15: A.d3q15(), 19: A.d3q19(), 27: A.d3q27()}
+
+
+def smooth_field(g, seed, amp=0.04):
+    rng = np.random.default_rng(seed)
+    x = np.stack(np.meshgrid(*[np.arange(n) for n in g], indexing="ij")).astype(float)
+    u = np.zeros((3, *g))
+    for d in range(3):
+        k = rng.integers(1, 3, size=3)
+        ph = rng.uniform(0, 2 * np.pi, 3)
+        u[d] = amp * np.sin(2 * np.pi * k[0] * x[0] / g[0] + ph[0]) * np.cos(2 * np.pi * k[1] * x[1] / g[1] + ph[1]) \
+            * np.cos(2 * np.pi * k[2] * x[2] / g[2] + ph[2])
+    rho = 1.0 + 0.01 * np.sin(2 * np.pi * x[0] / g[0])
+    return rho, u
+
+
+def sphere_map(g, center, r):
+    pos = np.stack(np.meshgrid(*[np.arange(n) - 1.0 for n in g], indexing="ij"))
+    d = np.sqrt(((pos - np.asarray(center, float).reshape(3, 1, 1, 1)) ** 2).sum(0)) - r
+    return np.clip(d / 1.8, -1, 1).astype(np.float32)
+
+
+@pytest.mark.parametrize("q", [15, 19, 27])
+@pytest.mark.parametrize("closure", [0, 1, 2])
+@pytest.mark.parametrize("storage,prec,tol", [("f64", 8, 1e-12), ("f32", 4, 2e-6)])
+def test_periodic_steps_match_oracle(gpu, oracle_mod, q, closure, storage, prec, tol):
+    size = (10, 9, 8)
+    g = tuple(s + 2 for s in size)
+    rho, u = smooth_field(g, 100 + q + closure)
+    nu = 0.02
+    lb = A.LBGK(A.Block(size), nu, VT[q], storage=storage, periodic=(True, True, True), body_force=(1e-3, -5e-4, 2e-4))
+    lb.setClosure(closure, 0.3)
+    A.LBGKUtilities(lb).initF(rho, u)
+    o = oracle_mod.Oracle(size, q, prec, nu, flags=8 | 16 | 32)
+    o.set_closure(closure, 0.3)
+    o.set_body_force((1e-3, -5e-4, 2e-4))
+    o.init_f_fields(rho, u)
+    for nsteps in (1, 6):  # odd and even step counts: both AA representations
+        lb.execute(nsteps)
+        o.step(nsteps)
+        assert np.abs(lb.getF()[I4] - o.get_f()[I4]).max() < tol
+        assert np.abs(lb.getVelocity()[I4] - o.get_u()[I4]).max() < tol
+        assert np.abs(lb.getRho()[1:-1, 1:-1, 1:-1] - o.get_rho()[1:-1, 1:-1, 1:-1]).max() < tol
+
+
+def test_coriolis_incompressible_match_oracle(gpu, oracle_mod):
+    size = (8, 7, 9)
+    g = tuple(s + 2 for s in size)
+    rho, u = smooth_field(g, 5)
+    lb = A.LBGK(A.Block(size), 0.05, A.d3q19(), storage="f64", periodic=(True, True, True))
+    lb.setCompressible(False)
+    lb.setOmega((0.01, -0.02, 0.03))
+    A.LBGKUtilities(lb).initF(rho, u)
+    o = oracle_mod.Oracle(size, 19, 8, 0.05, flags=4 | 8 | 16 | 32)
+    o.set_omega((0.01, -0.02, 0.03))
+    o.init_f_fields(rho, u)
+    lb.execute(5)
+    o.step(5)
+    assert np.abs(lb.getF()[I4] - o.get_f()[I4]).max() < 1e-12
+
+
+@pytest.mark.parametrize("q", [15, 19, 27])
+@pytest.mark.parametrize("storage,prec,tol", [("f64", 8, 1e-12), ("f32", 4, 3e-6)])
+def test_boundaries_and_force_match_oracle(gpu, oracle_mod, q, storage, prec, tol):
+    size = (11, 9, 10)
+    g = tuple(s + 2 for s in size)
+    rho, u = smooth_field(g, 40 + q, amp=0.02)
+    sphere = sphere_map(g, (4.0, 3.5, 4.0), 2.2)
+    vmap = sphere_map(g, (8.5, 5.0, 6.0), 1.5)
+    plan = [("slice", "velocity", ("X0",), 0.0, (0.03, 0.01, 0.0)),
+            ("slice", "pressure", ("XE",), 1.01, (0, 0, 0)),
+            ("slice", "noslip", ("Y0", "YE"), 0.0, (0, 0, 0)),
+            ("slice", "pressure_velocity", ("Z0", "ZE"), 0.99, (0.01, 0.0, -0.02)),
+            ("map", "noslip", sphere, 0.0, (0, 0, 0)),
+            ("map", "velocity", vmap, 0.0, (0.0, 0.02, 0.01)),
+            ("map", "pressure_velocity", vmap, 1.02, (0.01, 0.0, 0.0))]
+    lb = A.LBGK(A.Block(size), 0.03, VT[q], storage=storage)
+    A.LBGKUtilities(lb).initF(rho, u)
+    o = oracle_mod.Oracle(size, q, prec, 0.03)
+    o.init_f_fields(rho, u)
+    bcs, ids = [], []
+    for kind, name, where, p, uu in plan:
+        if kind == "slice":
+            walls = [getattr(A, w) for w in where]
+            bcs.append({"noslip": lambda: A.generateBCNoSlip(lb, walls),
+                        "velocity": lambda: A.generateBCConstantVelocity(lb, uu, walls),
+                        "pressure": lambda: A.generateBCConstantPressure(lb, p, walls),
+                        "pressure_velocity": lambda: A.generateBCConstantPressureVelocity(lb, p, uu, walls)}[name]())
+            ids.append(o.bc_slice(SLICE[name], sum(WALLS[w] for w in where), p, uu))
+        else:
+            bcs.append({"noslip": lambda: A.generateBCNoSlip(lb, where),
+                        "velocity": lambda: A.generateBCVelocity(lb, A.generatePFConstant(uu), where),
+                        "pressure_velocity": lambda: A.generateBCConstantPressureVelocity(lb, p, uu, where)}[name]())
+            ids.append(o.bc_map(MAPK[name], where, p, uu))
+    force = A.generateComputeSurfaceForce(lb, sphere)
+    for step in range(5):
+        lb.execute()
+        o.step(1)
+        A.executeAll(bcs)
+        for bid in ids:
+            o.bc_execute(bid)
+        got, fld = force.execute(r0=(4.0, 3.5, 4.0), field=True)
+        want, wfld = o.force(sphere, r0=(4.0, 3.5, 4.0), field=True)
+        assert np.abs(got - want).max() < 50 * tol * max(1.0, np.abs(want).max())
+        assert np.abs(fld - wfld).max() < 10 * tol + 1e-6
+        assert np.abs(lb.getF()[I4] - o.get_f()[I4]).max() < tol
+
+
+def test_rotation_velocity_map_matches_oracle(gpu, oracle_mod):
+    size = (12, 12, 6)
+    g = tuple(s + 2 for s in size)
+    cyl = np.clip((np.sqrt((np.arange(g[0])[:, None, None] - 1 - 5.5) ** 2 + (np.arange(g[1])[None, :, None] - 1 - 5.5) ** 2
+                           + 0 * np.arange(g[2])[None, None, :]) - 2.5) / 1.8, -1, 1).astype(np.float32)
+    lb = A.LBGK(A.Block(size), 0.05, A.d3q19(), storage="f64", periodic=(False, False, True))
+    A.LBGKUtilities(lb).initF((0.0, 0.0, 0.0))
+    bc = [A.generateBCNoSlip(lb, [A.X0, A.XE, A.Y0, A.YE]),
+          A.generateBCVelocity(lb, A.generatePFRotationField((0, 0, 0.01), (5.5, 5.5, 0.0)), cyl)]
+    o = oracle_mod.Oracle(size, 19, 8, 0.05, flags=32)
+    o.init_f(1.0, (0, 0, 0))
+    ids = [o.bc_slice(0, 1 | 2 | 4 | 8), o.bc_map(12, cyl, omega=(0, 0, 0.01), center=(5.5, 5.5, 0.0))]
+    for _ in range(8):
+        lb.execute()
+        A.executeAll(bc)
+        o.step(1)
+        for i in ids:
+            o.bc_execute(i)
+    assert np.abs(lb.getF()[I4] - o.get_f()[I4]).max() < 1e-12
+
+
+def test_graph_run_bitwise_equals_eager(gpu):
+    w = W.channel_cylinder(size=(40, 24, 20), radius=4.0, center=(12.0, 12.0), steps=0)
+    a, abcs = W.build_lbgk(w)
+    b, bbcs = W.build_lbgk(w)
+    a.run(37, abcs, use_graph=False)
+    b.run(37, bbcs, use_graph=True)
+    assert np.array_equal(a.getF(np.float32)[I4], b.getF(np.float32)[I4])
+    assert np.array_equal(a.getVelocity(np.float32), b.getVelocity(np.float32))
+
+
+def test_checkpoint_roundtrip(gpu):
+    w = W.channel_cylinder(size=(24, 16, 12), radius=3.0, center=(8.0, 8.0), steps=0)
+    a, abcs = W.build_lbgk(w, storage="f64")
+    a.run(11, abcs, use_graph=False)
+    f = a.getF()
+    b, bbcs = W.build_lbgk(w, storage="f64")
+    b.setF(f)
+    a.run(6, abcs, use_graph=False)
+    b.run(6, bbcs, use_graph=False)
+    assert np.array_equal(a.getF()[I4], b.getF()[I4])
+
+
+def test_mass_reduction_known_answers(gpu):
+    # test/testMath/testReductionFunction.cc:37-67 known answers, through the
+    # FP64 device reduction: 101 cells of density 2 sum to 202, 100001 cells
+    # of density 6 sum to 600006 (sum of weights is 1 to rounding).
+    for size, rho, want in [((101, 1, 1), 2.0, 202.0), ((11, 9091, 1), 6.0, 600006.0)]:
+        lb = A.LBGK(A.Block(size), 0.1, A.d3q19(), storage="f64", periodic=(True, True, True))
+        A.LBGKUtilities(lb).initF(rho, (0.0, 0.0, 0.0))
+        mom = lb.moments()
+        assert abs(mom[0] - want) <= 1e-13 * want
+        assert np.abs(mom[1:]).max() < 1e-12
+
+
+def test_mass_conservation_closed_box_fp64(gpu):
+    size = (20, 18, 16)
+    g = tuple(s + 2 for s in size)
+    rho, u = smooth_field(g, 9, amp=0.03)
+    lb = A.LBGK(A.Block(size), 0.02, A.d3q19(), storage="f64")
+    A.LBGKUtilities(lb).initF(rho, u)
+    bc = [A.generateBCNoSlip(lb, [A.X0, A.XE, A.Y0, A.YE, A.Z0, A.ZE])]
+    A.executeAll(bc)
+    m0 = lb.moments()[0]
+    lb.run(200, bc)
+    assert abs(lb.moments()[0] - m0) < 1e-11 * m0
+
+
+def test_fp16_storage_error_bound(gpu, oracle_mod):
+    # FP16 shifted storage with FP32 arithmetic against the FP64 oracle on a
+    # decaying periodic field: velocity error stays below 1e-4 (|u| ~ 0.04).
+    size = (24, 20, 16)
+    g = tuple(s + 2 for s in size)
+    rho, u = smooth_field(g, 77)
+    lb = A.LBGK(A.Block(size), 0.02, A.d3q19(), storage="f16", periodic=(True, True, True))
+    A.LBGKUtilities(lb).initF(rho, u)
+    o = oracle_mod.Oracle(size, 19, 8, 0.02, flags=8 | 16 | 32)
+    o.init_f_fields(rho, u)
+    lb.execute(50)
+    o.step(50)
+    err = np.abs(lb.getVelocity()[I4] - o.get_u()[I4]).max()
+    assert err < 1e-4, err
+
+
+def test_errors_raise(gpu):
+    with pytest.raises(A.L.ASLError):
+        A.LBGK(A.Block((4, 4, 4)), -1.0, A.d3q19())
+    lb = A.LBGK(A.Block((4, 4, 4)), 0.1, A.d3q19(), periodic=(True, False, False))
+    with pytest.raises(A.L.ASLError):
+        A.generateBCNoSlip(lb, [A.X0])  # wall on a periodic axis
+    with pytest.raises(A.L.ASLError):
+        lb.setClosure(3)  # learned closure without a network
+    with pytest.raises(A.L.ASLError):
+        A.generateBCNoSlip(lb, np.ones((3, 3, 3), np.float32))  # map of the wrong shape
+
+
+@pytest.mark.slow
+def test_channel_cylinder_parity_1000_steps(gpu, oracle_mod):
+    """The canonical cylinder channel (128x64x64, D3Q19, FP32, 1000 steps)
+    against the FP32 oracle: relative L2 of rho and u over interior fluid
+    cells <= 1e-4, drag within 1e-4 relative."""
+    w = W.channel_cylinder()
+    lb, bcs = W.build_lbgk(w, storage="f32")
+    o = oracle_mod.Oracle(w.size, 19, 4, w.nu)
+    o.init_f(1.0, (0, 0, 0))
+    ids = []
+    for s in w.bcs:
+        if s.kind == "map_noslip":
+            ids.append(o.bc_map(10, w.map))
+        else:
+            ids.append(o.bc_slice(W.SLICE_KIND[s.kind], sum(W.WALL_BITS[x] for x in s.walls), s.p, s.u))
+    lb.run(w.steps, bcs)
+    for _ in range(w.steps):
+        o.step(1)
+        for i in ids:
+            o.bc_execute(i)
+    fluid = w.map[1:-1, 1:-1, 1:-1] > 0
+    r_g, r_o = lb.getRho()[1:-1, 1:-1, 1:-1][fluid], o.get_rho()[1:-1, 1:-1, 1:-1][fluid]
+    u_g = lb.getVelocity()[I4][:, fluid]
+    u_o = o.get_u()[I4][:, fluid]
+    assert np.linalg.norm(r_g - r_o) / np.linalg.norm(r_o) <= 1e-4
+    assert np.linalg.norm(u_g - u_o) / np.linalg.norm(u_o) <= 1e-4
+    force = A.generateComputeSurfaceForce(lb, w.map)
+    got = force.execute(r0=(32.0, 32.0, 31.5))
+    want = o.force(w.map, r0=(32.0, 32.0, 31.5))
+    assert abs(got[0] - want[0]) <= 1e-4 * abs(want[0])

@@ -1,0 +1,228 @@
+"""CPU tests of the oracle: known answers, physics pins and a cross-check
+against an independent numpy restatement. No GPU needed."""
+import numpy as np
+import pytest
+
+from tests.numpy_lbgk import NumpyLBGK, lattice as np_lattice
+
+WALLS = {"X0": 1, "XE": 2, "Y0": 4, "YE": 8, "Z0": 16, "ZE": 32}
+SLICE = {"noslip": 0, "velocity": 1, "pressure": 2, "pressure_velocity": 3}
+MAPK = {"noslip": 10, "velocity": 11, "pressure_velocity": 13}
+
+
+@pytest.mark.parametrize("q", [15, 19, 27])
+def test_lattice_tables(oracle_mod, q):
+    c, w, inv = oracle_mod.lattice(q)
+    assert abs(w.sum() - 1.0) < 1e-15
+    assert np.allclose((w[:, None] * c).sum(0), 0)
+    assert np.allclose(np.einsum("i,ia,ib->ab", w, c, c), np.eye(3) / 3)
+    assert (c[inv] == -c).all()
+    c2, w2, inv2 = np_lattice(q)
+    assert (c == c2).all() and np.allclose(w, w2) and (inv == inv2).all()
+    # ASL's direction order: rest, +x, +y, +z, -x, -y, -z first (aslTemplates.cxx:146-185)
+    assert c[:7].tolist() == [[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [-1, 0, 0], [0, -1, 0], [0, 0, -1]]
+
+
+def test_reduction_known_answers(oracle_mod):
+    # test/testMath/testReductionFunction.cc:37-67: sum of 101 twos is 202,
+    # sum of 100001 products 2*3 is 600006.
+    assert oracle_mod.reduction_sum(np.full(101, 2.0)) == 202.0
+    assert oracle_mod.reduction_sum(np.full(100001, 2.0) * 3.0) == 600006.0
+
+
+@pytest.mark.parametrize("prec,tol", [(8, 1e-13), (4, 1e-6)])
+def test_rest_state_invariant(oracle_mod, prec, tol):
+    # In FP32 sum(w_i) rounds to 1 + O(1e-8), so ASL's rest state drifts by
+    # about omega * 2.4e-8 per step; FP64 keeps it to rounding.
+    o = oracle_mod.Oracle((8, 6, 5), 19, prec, 0.05, flags=8 | 16 | 32)
+    o.init_f(1.0, (0, 0, 0))
+    o.step(20)
+    assert np.abs(o.get_f()[:, 1:-1, 1:-1, 1:-1] - 1.0).max() < tol
+
+
+def _smooth_field(g, seed, amp=0.04):
+    rng = np.random.default_rng(seed)
+    x = np.stack(np.meshgrid(*[np.arange(n) for n in g], indexing="ij")).astype(float)
+    u = np.zeros((3, *g))
+    for d in range(3):
+        k = rng.integers(1, 3, size=3)
+        ph = rng.uniform(0, 2 * np.pi, 3)
+        u[d] = amp * np.sin(2 * np.pi * k[0] * x[0] / g[0] + ph[0]) * np.cos(2 * np.pi * k[1] * x[1] / g[1] + ph[1]) \
+            * np.cos(2 * np.pi * k[2] * x[2] / g[2] + ph[2])
+    rho = 1.0 + 0.01 * np.sin(2 * np.pi * x[0] / g[0])
+    return rho, u
+
+
+@pytest.mark.parametrize("q", [15, 19, 27])
+@pytest.mark.parametrize("closure", [0, 1, 2])
+def test_oracle_matches_numpy_periodic(oracle_mod, q, closure):
+    size = (6, 5, 4)
+    g = tuple(s + 2 for s in size)
+    rho, u = _smooth_field(g, 7 + q + closure)
+    nu = 0.02
+    o = oracle_mod.Oracle(size, q, 8, nu, flags=8 | 16 | 32)
+    o.set_closure(closure, 0.3)
+    o.set_body_force((1e-3, -2e-3, 5e-4))
+    o.init_f_fields(rho, u)
+    ref = NumpyLBGK(size, q, nu, periodic=(True, True, True))
+    ref.closure, ref.cs = closure, 0.3
+    ref.g = np.array([1e-3, -2e-3, 5e-4])
+    ref.init_f(rho, u)
+    for _ in range(3):
+        o.step(1)
+        ref.step()
+    I = (slice(None), slice(1, -1), slice(1, -1), slice(1, -1))
+    assert np.allclose(o.get_f()[I], ref.f[I], rtol=0, atol=1e-13)
+    assert np.allclose(o.get_u()[I], ref.u[I], rtol=0, atol=1e-13)
+
+
+def test_oracle_coriolis_incompressible(oracle_mod):
+    size = (5, 4, 6)
+    g = tuple(s + 2 for s in size)
+    rho, u = _smooth_field(g, 3)
+    o = oracle_mod.Oracle(size, 19, 8, 0.05, flags=4 | 8 | 16 | 32)
+    o.set_omega((0.01, -0.02, 0.03))
+    o.init_f_fields(rho, u)
+    ref = NumpyLBGK(size, 19, 0.05, periodic=(True, True, True), compressible=False)
+    ref.Om = np.array([0.01, -0.02, 0.03])
+    ref.init_f(rho, u)
+    for _ in range(2):
+        o.step(1)
+        ref.step()
+    I = (slice(None), slice(1, -1), slice(1, -1), slice(1, -1))
+    assert np.allclose(o.get_f()[I], ref.f[I], rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("q", [15, 19, 27])
+def test_oracle_matches_numpy_boundaries(oracle_mod, q):
+    size = (7, 5, 6)
+    g = tuple(s + 2 for s in size)
+    rho, u = _smooth_field(g, 11 + q, amp=0.02)
+    pos = np.stack(np.meshgrid(*[np.arange(n) - 1.0 for n in g], indexing="ij"))
+    sphere = np.clip((np.sqrt(((pos - np.array([3.0, 2.0, 2.5]).reshape(3, 1, 1, 1)) ** 2).sum(0)) - 1.6) / 1.8,
+                     -1, 1).astype(np.float32)
+    vmap = np.clip((np.sqrt(((pos - np.array([5.5, 3.0, 4.0]).reshape(3, 1, 1, 1)) ** 2).sum(0)) - 1.2) / 1.8,
+                   -1, 1).astype(np.float32)
+    plan = [("slice", "velocity", ("X0",), 0.0, (0.03, 0.01, 0.0)),
+            ("slice", "pressure", ("XE",), 1.01, (0, 0, 0)),
+            ("slice", "noslip", ("Y0", "YE"), 0.0, (0, 0, 0)),
+            ("slice", "pressure_velocity", ("Z0", "ZE"), 0.99, (0.01, 0.0, -0.02)),
+            ("map", "noslip", sphere, 0.0, (0, 0, 0)),
+            ("map", "velocity", vmap, 0.0, (0.0, 0.02, 0.01)),
+            ("map", "pressure_velocity", vmap, 1.02, (0.01, 0.0, 0.0))]
+    o = oracle_mod.Oracle(size, q, 8, 0.03)
+    o.init_f_fields(rho, u)
+    ref = NumpyLBGK(size, q, 0.03)
+    ref.init_f(rho, u)
+    ids = []
+    for kind, name, where, p, uu in plan:
+        if kind == "slice":
+            ids.append(o.bc_slice(SLICE[name], sum(WALLS[w] for w in where), p, uu))
+        else:
+            ids.append(o.bc_map(MAPK[name], where, p, uu))
+    for _ in range(3):
+        o.step(1)
+        ref.step()
+        for bid, (kind, name, where, p, uu) in zip(ids, plan):
+            o.bc_execute(bid)
+            if kind == "slice":
+                ref.apply_slice(name, where, p, uu)
+            else:
+                ref.apply_map(name, where, p, uu)
+    f_o = o.get_f()
+    assert np.allclose(f_o, ref.f, rtol=0, atol=1e-13)
+    out, fld = o.force(sphere, r0=(3.0, 2.0, 2.5), field=True)
+    ref_out, ref_fld = ref.force(sphere, r0=(3.0, 2.0, 2.5))
+    assert np.allclose(fld, ref_fld, atol=1e-6)
+    assert np.allclose(out, ref_out, rtol=1e-10, atol=1e-12)
+
+
+def test_force_at_rest_is_zero(oracle_mod):
+    size = (10, 8, 8)
+    g = tuple(s + 2 for s in size)
+    pos = np.stack(np.meshgrid(*[np.arange(n) - 1.0 for n in g], indexing="ij"))
+    m = np.clip((np.sqrt(((pos - 4.0) ** 2).sum(0)) - 2.5) / 1.8, -1, 1).astype(np.float32)
+    o = oracle_mod.Oracle(size, 19, 8, 0.05)
+    o.init_f(1.0, (0, 0, 0))
+    assert np.all(o.force(m) == 0.0)  # every link term is 1 + 1 - 2
+    bid = o.bc_map(10, m)
+    o.step(5)
+    o.bc_execute(bid)
+    assert np.abs(o.force(m)).max() < 1e-12
+
+
+def test_mass_conserved_in_closed_box(oracle_mod):
+    size = (8, 7, 6)
+    g = tuple(s + 2 for s in size)
+    rho, u = _smooth_field(g, 5, amp=0.03)
+    o = oracle_mod.Oracle(size, 19, 8, 0.02)
+    o.init_f_fields(rho, u)
+    bid = o.bc_slice(0, 63)
+    c, w, _ = oracle_mod.lattice(19)
+
+    def mass():
+        f = o.get_f()[:, 1:-1, 1:-1, 1:-1]
+        return float((w[:, None, None, None] * f).sum())
+
+    o.bc_execute(bid)
+    m0 = mass()
+    for _ in range(30):
+        o.step(1)
+        o.bc_execute(bid)
+    assert abs(mass() - m0) < 1e-11 * m0
+
+
+def test_poiseuille_profile(oracle_mod):
+    # Body-force channel between no-slip walls at y = 1/2 and y = ny + 1/2
+    # (halfway bounce-back), periodic in x and z: u(y) = g/(2 nu) (y-1/2)(ny+1/2-y).
+    ny, nu, gx = 16, 0.1, 1e-5
+    o = oracle_mod.Oracle((4, ny, 3), 19, 8, nu, flags=8 | 32)
+    o.set_body_force((gx, 0, 0))
+    o.init_f(1.0, (0, 0, 0))
+    bid = o.bc_slice(0, 4 | 8)
+    for _ in range(4000):
+        o.step(1)
+        o.bc_execute(bid)
+    ux = o.get_u()[0, 2, 1:-1, 2]
+    y = np.arange(1, ny + 1)
+    ana = gx / (2 * nu) * (y - 0.5) * (ny + 0.5 - y)
+    assert np.max(np.abs(ux - ana)) < 0.01 * ana.max()
+
+
+def test_couette_profile(oracle_mod):
+    # Wall YE moves with uw along x (ConstantVelocity BC), Y0 at rest.
+    ny, nu, uw = 12, 0.1667, 0.01
+    o = oracle_mod.Oracle((3, ny, 3), 19, 8, nu, flags=8 | 32)
+    o.init_f(1.0, (0, 0, 0))
+    b0 = o.bc_slice(0, 4)
+    b1 = o.bc_slice(1, 8, 0.0, (uw, 0, 0))
+    for _ in range(3000):
+        o.step(1)
+        o.bc_execute(b0)
+        o.bc_execute(b1)
+    ux = o.get_u()[0, 2, 1:-1, 2]
+    y = np.arange(1, ny + 1)
+    ana = uw * (y - 0.5) / ny
+    assert np.max(np.abs(ux - ana)) < 2e-3 * uw
+
+
+def test_single_cell_collide_by_hand(oracle_mod):
+    # One periodic cell: streaming is the identity, so one step is one collision.
+    q, nu = 19, 0.1
+    c, w, _ = oracle_mod.lattice(q)
+    rng = np.random.default_rng(1)
+    f0 = 1.0 + 0.05 * rng.standard_normal(q)
+    o = oracle_mod.Oracle((1, 1, 1), q, 8, nu, flags=8 | 16 | 32)
+    f = np.ones((q, 3, 3, 3))
+    f[:, 1, 1, 1] = f0
+    o.set_f(f)
+    o.step(1)
+    got = o.get_f()[:, 1, 1, 1]
+    rho = sum(w[i] * f0[i] for i in range(q))
+    m = [sum(w[i] * c[i][d] * f0[i] for i in range(q)) for d in range(3)]
+    mm = sum(a * a for a in m)
+    om = 1.0 / (3 * nu + 0.5)
+    for i in range(q):
+        cm = sum(c[i][d] * m[d] for d in range(3))
+        feq = rho + 3 * cm + 4.5 * cm * cm / rho - 1.5 * mm / rho
+        assert abs(got[i] - ((1 - om) * f0[i] + om * feq)) < 1e-14
