@@ -54,13 +54,20 @@ struct aslb_lbgk {
   int graph_parity = -1;
   long long graph_version = -1;
   long long version = 0;  // bumped by every parameter change
+  // fused no-slip maps
+  std::vector<uint32_t> mask_host;
+  uint32_t* mask_dev = nullptr;
 };
 
 struct aslb_bc {
   aslb_lbgk* h = nullptr;
-  int4* anchors = nullptr;
+  int4* anchors = nullptr;  // anchor form: (x, y, z, direction mask)
   int n = 0;
+  int* dlinks = nullptr;    // direction-sorted form: anchor storage index per link
+  int nd = 0;
+  LinkSet ls{};
   long long links = 0;
+  bool fused = false;  // folded into the stream-collide kernel (execute is a no-op)
   BcParams bp{};
 };
 
@@ -99,7 +106,10 @@ int do_step(aslb_lbgk* h) {
 
 int do_bc(aslb_bc* bc) {
   aslb_lbgk* h = bc->h;
-  cudaError_t e = launch_bc(h->d, bc->anchors, bc->n, bc->bp, h->parity, h->stream);
+  if (bc->fused) return ASLB_OK;
+  cudaError_t e = cudaSuccess;
+  if (bc->nd) e = launch_bc_links(h->d, bc->dlinks, bc->nd, bc->ls, bc->bp, h->parity, h->stream);
+  if (e == cudaSuccess && bc->n) e = launch_bc(h->d, bc->anchors, bc->n, bc->bp, h->parity, h->stream);
   if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("boundary launch: ") + cudaGetErrorString(e));
   return ASLB_OK;
 }
@@ -140,6 +150,117 @@ bool interior(const GridDesc& g, int x, int y, int z) {
 float map_at(const GridDesc& g, const float* map, int x, int y, int z) {
   if (x < 0 || y < 0 || z < 0 || x >= g.gx || y >= g.gy || z >= g.gz) return -0.9f;  // generateDCFullSafe(map, -.9)
   return map[aidx(g, x, y, z)];
+}
+
+
+// Split candidate links (anchor a, direction k) into the direction-sorted form
+// (fluid end at anchor + storage offset of c_k) and the anchor form (links
+// that wrap across a periodic face, and every link of a velocity map, which
+// needs all links of its anchor together).
+struct Cand {
+  int x, y, z, k;
+};
+
+int finalize_links(aslb_lbgk* h, aslb_bc* bc, const std::vector<Cand>& cand, bool anchor_form_only) {
+  const GridDesc& g = h->d.g;
+  const int q = h->d.q;
+  std::vector<std::vector<int>> per_dir(q);
+  std::vector<std::pair<long long, int>> rest;  // (ghosted linear index, k)
+  for (const Cand& c : cand) {
+    const long long wa = sidx(g, wrapc(h, c.x, 0), wrapc(h, c.y, 1), wrapc(h, c.z, 2));
+    const long long wq = sidx(g, wrapc(h, c.x + lattice_c(q, c.k, 0), 0), wrapc(h, c.y + lattice_c(q, c.k, 1), 1),
+                              wrapc(h, c.z + lattice_c(q, c.k, 2), 2));
+    const long long off = lattice_c(q, c.k, 0) * g.plane + lattice_c(q, c.k, 1) * (long long)g.pitch + lattice_c(q, c.k, 2);
+    if (!anchor_form_only && wq == wa + off)
+      per_dir[c.k].push_back((int)wa);
+    else
+      rest.emplace_back(aidx(g, c.x, c.y, c.z), c.k);
+  }
+  std::vector<int> flat;
+  bc->ls.seg[0] = 0;
+  bc->ls.seg[1] = 0;
+  for (int k = 1; k < 27; ++k) {
+    if (k < q) {
+      auto& v = per_dir[k];
+      std::sort(v.begin(), v.end());
+      v.erase(std::unique(v.begin(), v.end()), v.end());
+      flat.insert(flat.end(), v.begin(), v.end());
+    }
+    bc->ls.seg[k + 1] = (int)flat.size();
+  }
+  for (int k = 0; k < 27; ++k) {
+    bc->ls.off[k] = k < q ? int(lattice_c(q, k, 0) * g.plane + lattice_c(q, k, 1) * (long long)g.pitch +
+                                lattice_c(q, k, 2))
+                          : 0;
+    bc->ls.inv[k] = k < q ? lattice_inv(q, k) : 0;
+  }
+  std::sort(rest.begin(), rest.end());
+  std::vector<int4> anchors;
+  for (size_t i = 0; i < rest.size();) {
+    const long long a = rest[i].first;
+    unsigned mask = 0;
+    while (i < rest.size() && rest[i].first == a) mask |= 1u << rest[i++].second;
+    const int z = int(a % g.gz);
+    const int y = int((a / g.gz) % g.gy);
+    const int x = int(a / ((long long)g.gz * g.gy));
+    anchors.push_back(make_int4(x, y, z, (int)mask));
+  }
+  bc->nd = (int)flat.size();
+  bc->n = (int)anchors.size();
+  bc->links = (long long)flat.size();
+  for (auto& a : anchors) bc->links += __builtin_popcount((unsigned)a.w);
+  int r = upload(&bc->dlinks, flat);
+  if (!r) r = upload(&bc->anchors, anchors);
+  return r;
+}
+
+// Per-direction constants of a condition, evaluated in the arithmetic of the
+// storage (float for FP32/FP16, double for FP64) like the per-link kernels.
+void fill_link_values(aslb_lbgk* h, aslb_bc* bc) {
+  const int q = h->d.q;
+  const BcParams& bp = bc->bp;
+  for (int k = 0; k < 27; ++k) {
+    if (k >= q) {
+      bc->ls.val[k] = 0.f;
+      bc->ls.vald[k] = 0.0;
+      continue;
+    }
+    const int c0 = lattice_c(q, k, 0), c1 = lattice_c(q, k, 1), c2 = lattice_c(q, k, 2);
+    {
+      const float u0 = (float)bp.u[0], u1 = (float)bp.u[1], u2 = (float)bp.u[2], P = (float)bp.p;
+      const float cu = u0 * (float)c0 + u1 * (float)c1 + u2 * (float)c2;
+      const float vv = u0 * u0 + u1 * u1 + u2 * u2;
+      float v = 0.f;
+      switch (bp.kind) {
+        case BCK_VELOCITY: v = 6.0f * cu; break;
+        case BCK_PRESSURE: v = P; break;
+        case BCK_PRESSURE_VELOCITY: v = P + 3.0f * cu; break;
+        case BCK_MAP_PRESSURE_VELOCITY:
+          v = bp.compressible ? P + 3.0f * P * cu + 4.5f * P * cu * cu - 1.5f * P * vv
+                              : P + 3.0f * cu + 4.5f * cu * cu - 1.5f * vv;
+          break;
+        default: break;
+      }
+      bc->ls.val[k] = v;
+    }
+    {
+      const double u0 = bp.u[0], u1 = bp.u[1], u2 = bp.u[2], P = bp.p;
+      const double cu = u0 * c0 + u1 * c1 + u2 * c2;
+      const double vv = u0 * u0 + u1 * u1 + u2 * u2;
+      double v = 0.0;
+      switch (bp.kind) {
+        case BCK_VELOCITY: v = 6.0 * cu; break;
+        case BCK_PRESSURE: v = P; break;
+        case BCK_PRESSURE_VELOCITY: v = P + 3.0 * cu; break;
+        case BCK_MAP_PRESSURE_VELOCITY:
+          v = bp.compressible ? P + 3.0 * P * cu + 4.5 * P * cu * cu - 1.5 * P * vv
+                              : P + 3.0 * cu + 4.5 * cu * cu - 1.5 * vv;
+          break;
+        default: break;
+      }
+      bc->ls.vald[k] = v;
+    }
+  }
 }
 
 }  // namespace
@@ -228,6 +349,7 @@ int aslb_lbgk_destroy(aslb_lbgk* h) {
   cudaFree(h->d.rho);
   cudaFree(h->d.u);
   cudaFree(h->mlp_dev);
+  cudaFree(h->mask_dev);
   cudaFree(h->red_partials);
   cudaFree(h->red_out);
   if (h->host_out) cudaFreeHost(h->host_out);
@@ -563,11 +685,13 @@ int aslb_bc_slice_create(aslb_lbgk* h, int kind, unsigned wallmask, double p, co
   if (wallmask == 0 || wallmask > 63u) return fail(ASLB_ERR_ARG, "aslb_bc_slice_create: bad wall mask");
   const GridDesc& g = h->d.g;
   const int q = h->d.q;
-  // Walls X0, XE, Y0, YE, Z0, ZE with inward normals c_1, c_4, c_2, c_5, c_3, c_6
+  // Walls X0, XE, Y0, YE, Z0, ZE with inward normals c_1, c_4, c_2, c_5, c_3, c_6;
+  // every direction k with c_k . n > 0 and every point a of the first interior
+  // layer (tangential coordinates 1 .. N'-2) gives the ghost point a - c_k
   // (src/num/aslBCond.cxx:373-493).
   static const int normal_dir[6] = {1, 4, 2, 5, 3, 6};
   const int G[3] = {g.gx, g.gy, g.gz};
-  std::vector<std::pair<long long, int>> links;
+  std::vector<Cand> cand;
   for (int w = 0; w < 6; ++w) {
     if (!(wallmask >> w & 1u)) continue;
     const int ax = w / 2;
@@ -585,35 +709,22 @@ int aslb_bc_slice_create(aslb_lbgk* h, int kind, unsigned wallmask, double p, co
           a[ax] = layer;
           a[t1] = i;
           a[t2] = j;
-          const int px = a[0] - lattice_c(q, k, 0), py = a[1] - lattice_c(q, k, 1), pz = a[2] - lattice_c(q, k, 2);
-          links.emplace_back(aidx(g, px, py, pz), k);
+          cand.push_back({a[0] - lattice_c(q, k, 0), a[1] - lattice_c(q, k, 1), a[2] - lattice_c(q, k, 2), k});
         }
     }
   }
-  std::sort(links.begin(), links.end());
-  std::vector<int4> anchors;
-  for (size_t i = 0; i < links.size();) {
-    const long long a = links[i].first;
-    unsigned mask = 0;
-    while (i < links.size() && links[i].first == a) mask |= 1u << links[i++].second;
-    const int z = int(a % g.gz);
-    const int y = int((a / g.gz) % g.gy);
-    const int x = int(a / ((long long)g.gz * g.gy));
-    anchors.push_back(make_int4(x, y, z, (int)mask));
-  }
   auto* bc = new aslb_bc();
   bc->h = h;
-  bc->n = (int)anchors.size();
-  for (auto& a : anchors) bc->links += __builtin_popcount((unsigned)a.w);
   bc->bp.kind = kind;
   bc->bp.compressible = h->p.compressible;
   bc->bp.p = p;
   for (int d = 0; d < 3; ++d) bc->bp.u[d] = u ? u[d] : 0.0;
   bc->bp.scale = h->p.scale;
   bc->bp.inv_scale = h->p.inv_scale;
-  int r = upload(&bc->anchors, anchors);
+  fill_link_values(h, bc);
+  int r = finalize_links(h, bc, cand, false);
   if (r) {
-    delete bc;
+    aslb_bc_destroy(bc);
     return r;
   }
   *out = bc;
@@ -629,8 +740,7 @@ int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const
     return fail(ASLB_ERR_ARG, "aslb_bc_map_create: unknown map kind");
   const GridDesc& g = h->d.g;
   const int q = h->d.q;
-  std::vector<int4> anchors;
-  long long links = 0;
+  std::vector<Cand> cand;
   // Cell x is processed iff -0.9999 < map(x) <= 0; link k iff map(x + c_k) > 0
   // (src/num/aslLBGKBC.cxx:235-251), counted when x + c_k is an interior cell.
   for (int x = 0; x < g.gx; ++x)
@@ -639,23 +749,16 @@ int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const
         if (on_periodic_ghost(h, x, y, z)) continue;
         const float m0 = map[aidx(g, x, y, z)];
         if (!(m0 <= 0.f && m0 > -0.9999f)) continue;
-        unsigned mask = 0;
         for (int k = 1; k < q; ++k) {
           const int qx = wrapc(h, x + lattice_c(q, k, 0), 0), qy = wrapc(h, y + lattice_c(q, k, 1), 1),
                     qz = wrapc(h, z + lattice_c(q, k, 2), 2);
           if (!interior(g, qx, qy, qz)) continue;
-          if (map_at(g, map, qx, qy, qz) > 0.f) mask |= 1u << k;
-        }
-        if (mask) {
-          anchors.push_back(make_int4(x, y, z, (int)mask));
-          links += __builtin_popcount(mask);
+          if (map_at(g, map, qx, qy, qz) > 0.f) cand.push_back({x, y, z, k});
         }
       }
-  if (anchors.size() >= (size_t)(1u << 31)) return fail(ASLB_ERR_ARG, "aslb_bc_map_create: too many boundary cells");
+  if (cand.size() >= (size_t)(1u << 31)) return fail(ASLB_ERR_ARG, "aslb_bc_map_create: too many boundary links");
   auto* bc = new aslb_bc();
   bc->h = h;
-  bc->n = (int)anchors.size();
-  bc->links = links;
   bc->bp.kind = kind;
   bc->bp.compressible = h->p.compressible;
   bc->bp.p = p;
@@ -668,14 +771,62 @@ int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const
   bc->bp.dx = h->dx;
   bc->bp.scale = h->p.scale;
   bc->bp.inv_scale = h->p.inv_scale;
-  int r = upload(&bc->anchors, anchors);
+  fill_link_values(h, bc);
+  const bool velocity_map = kind == ASLB_BC_MAP_VELOCITY || kind == ASLB_BC_MAP_VELOCITY_ROTATION;
+  int r = finalize_links(h, bc, cand, velocity_map);
   if (r) {
-    delete bc;
+    aslb_bc_destroy(bc);
     return r;
   }
   *out = bc;
   return ASLB_OK;
 }
+
+int aslb_bc_fuse(aslb_bc* bc, const float* map) {
+  if (!bc || !map) return fail(ASLB_ERR_ARG, "aslb_bc_fuse: null argument");
+  if (bc->bp.kind != ASLB_BC_MAP_NOSLIP) return fail(ASLB_ERR_ARG, "aslb_bc_fuse: only no-slip maps can be fused");
+  if (bc->fused) return ASLB_OK;
+  aslb_lbgk* h = bc->h;
+  const GridDesc& g = h->d.g;
+  const int q = h->d.q;
+  std::vector<uint32_t> m = h->mask_host.empty() ? std::vector<uint32_t>((size_t)g.dstride, 0u) : h->mask_host;
+  for (int x = 0; x < g.gx; ++x)
+    for (int y = 0; y < g.gy; ++y)
+      for (int z = 0; z < g.gz; ++z) {
+        if (on_periodic_ghost(h, x, y, z)) continue;
+        if (map[aidx(g, x, y, z)] <= 0.f) m[sidx(g, x, y, z)] |= kSolidBit;
+      }
+  for (int x = 1; x <= g.nx; ++x)
+    for (int y = 1; y <= g.ny; ++y)
+      for (int z = 1; z <= g.nz; ++z) {
+        if (map[aidx(g, x, y, z)] <= 0.f) continue;
+        uint32_t bits = 0;
+        for (int k = 1; k < q; ++k) {
+          const int sx = wrapc(h, x - lattice_c(q, k, 0), 0), sy = wrapc(h, y - lattice_c(q, k, 1), 1),
+                    sz = wrapc(h, z - lattice_c(q, k, 2), 2);
+          const float ms = map_at(g, map, sx, sy, sz);
+          if (ms > 0.f) continue;
+          // The map condition skips solid cells at or below -0.9999: their links
+          // would pull a collided solid population, which fused mode cannot give.
+          if (!(ms > -0.9999f))
+            return fail(ASLB_ERR_ARG, "aslb_bc_fuse: a fluid cell borders a solid cell beyond the map guard "
+                                      "(-0.9999); normalise the map or keep the condition unfused");
+          bits |= 1u << k;
+        }
+        m[sidx(g, x, y, z)] |= bits;
+      }
+  if (!h->mask_dev) ASLB_CUDA(cudaMalloc((void**)&h->mask_dev, (size_t)g.dstride * sizeof(uint32_t)));
+  ASLB_CUDA(cudaStreamSynchronize(h->stream));
+  ASLB_CUDA(cudaMemcpy(h->mask_dev, m.data(), m.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  h->mask_host.swap(m);
+  h->p.mask = h->mask_dev;
+  bc->fused = true;
+  h->version++;
+  drop_graph(h);
+  return ASLB_OK;
+}
+
+int aslb_bc_is_fused(aslb_bc* bc) { return bc && bc->fused ? 1 : 0; }
 
 int aslb_bc_execute(aslb_bc* bc) {
   if (!bc) return fail(ASLB_ERR_ARG, "aslb_bc_execute: null handle");
@@ -689,11 +840,14 @@ int aslb_bc_destroy(aslb_bc* bc) {
     drop_graph(bc->h);
   }
   cudaFree(bc->anchors);
+  cudaFree(bc->dlinks);
   delete bc;
   return ASLB_OK;
 }
 
 long long aslb_bc_num_links(aslb_bc* bc) { return bc ? bc->links : -1; }
+
+int aslb_bc_kernels(aslb_bc* bc) { return !bc || bc->fused ? 0 : (bc->nd > 0) + (bc->n > 0); }
 
 // ---- surface force ---------------------------------------------------------
 
@@ -756,7 +910,7 @@ int aslb_force_compute(aslb_force* fc, const double r0[3], float* field_host, do
   aslb_lbgk* h = fc->h;
   const double zero[3] = {0, 0, 0};
   cudaError_t e = launch_force(h->d, fc->cells, fc->mask_in, fc->n, fc->field, r0 ? r0 : zero, h->pos0, h->dx,
-                               h->p.inv_scale, fc->partials, fc->out, h->stream);
+                               h->p.inv_scale, h->mask_dev, h->parity, fc->partials, fc->out, h->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(fc->host_out, fc->out, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess && field_host)

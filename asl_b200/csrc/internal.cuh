@@ -63,7 +63,13 @@ struct StepParams {
   int write_rho, write_vel;
   float scale, inv_scale;  // FP16 storage: d = (f - 1) * scale
   const void* mlp;         // closure network (device), CL == 3
+  // Fused no-slip maps (null when none): per storage cell, bit 31 marks a
+  // solid cell that is not advanced, bit k that population k enters this
+  // fluid cell from such a solid cell and is taken by bounce-back instead.
+  const uint32_t* mask;
 };
+
+constexpr uint32_t kSolidBit = 0x80000000u;
 
 // ---- storage formats -------------------------------------------------------
 template <class S>
@@ -134,6 +140,19 @@ struct BcParams {
   double pos0[3];
   double dx;
   float scale, inv_scale;
+};
+
+// Direction-sorted boundary links: links [seg[k], seg[k+1]) have direction k,
+// each stored as the storage index of its anchor; the fluid end is
+// anchor + off[k] (links that wrap across a periodic face go to the anchor
+// form instead). val[k] is the per-direction constant of the condition:
+// 6 c_k.u (velocity), p (pressure), p + 3 c_k.u, or f_eq,k(p, u).
+struct LinkSet {
+  int seg[28];
+  int off[27];
+  int inv[27];
+  float val[27];
+  double vald[27];
 };
 
 }  // namespace aslb

@@ -287,6 +287,58 @@ cudaError_t launch_bc(const DomainDev& d, const int4* anchors, int n, const BcPa
   ASLB_DISPATCH(d, bc_impl, d, anchors, n, bp, parity, st)
 }
 
+// Direction-sorted links: thread t handles link t, whose direction k comes from
+// the segment table (warp-uniform except at segment ends). IN and OUT slots as
+// above; the fluid end is anchor + off[k].
+template <int Q, class S>
+__global__ void __launch_bounds__(256) k_bc_links(S* __restrict__ F, const GridDesc g, const int* __restrict__ links,
+                                                  int n, const LinkSet ls, const BcParams bp, int parity) {
+  using C = typename Store<S>::C;
+  using A = BcArith<S>;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int k = 1;
+  while (t >= ls.seg[k + 1]) ++k;
+  const int wa = links[t];
+  const int wq = wa + ls.off[k];
+  const int kb = ls.inv[k];
+  S* in;
+  S* out;
+  if (parity == 0) {
+    in = F + (size_t)k * g.dstride + wa;
+    out = F + (size_t)kb * g.dstride + wq;
+  } else {
+    in = F + (size_t)kb * g.dstride + wq;
+    out = F + (size_t)k * g.dstride + wa;
+  }
+  const C v = std::is_same<C, double>::value ? C(ls.vald[k]) : C(ls.val[k]);
+  switch (bp.kind) {
+    case BCK_NOSLIP:
+    case BCK_MAP_NOSLIP:
+      *in = *out;
+      break;
+    case BCK_VELOCITY:
+      A::put(in, A::get(out, bp) + v, bp);
+      break;
+    default:  // pressure, pressure + velocity, equilibrium: a constant per direction
+      A::put(in, A::rep(v), bp);
+      break;
+  }
+}
+
+template <int Q, class S>
+static cudaError_t bc_links_impl(const DomainDev& d, const int* links, int n, const LinkSet& ls, const BcParams& bp,
+                                 int parity, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_bc_links<Q, S><<<(n + 255) / 256, 256, 0, st>>>((S*)d.F, d.g, links, n, ls, bp, parity);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bc_links(const DomainDev& d, const int* links, int n, const LinkSet& ls, const BcParams& bp,
+                            int parity, cudaStream_t st) {
+  ASLB_DISPATCH(d, bc_links_impl, d, links, n, ls, bp, parity, st)
+}
+
 // ---------------------------------------------------------------------------
 // Reductions: warp shuffle, then one row of partial sums per block.
 template <int W>
@@ -323,9 +375,10 @@ __global__ void __launch_bounds__(kForceThreads)
     k_force(const S* __restrict__ F, const GridDesc g, const int4* __restrict__ cells,
             const uint32_t* __restrict__ mask_in, int n, float* __restrict__ field, double r00, double r01,
             double r02, double p00, double p01, double p02, double dx, float inv_scale,
-            double* __restrict__ partials) {
+            const uint32_t* __restrict__ fused, int parity, double* __restrict__ partials) {
   using Lt = Lattice<Q>;
   using C = typename Store<S>::C;
+  constexpr bool kDev = std::is_same<S, __half>::value;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   double v[6] = {0, 0, 0, 0, 0, 0};
   if (t < n) {
@@ -333,6 +386,7 @@ __global__ void __launch_bounds__(kForceThreads)
     const unsigned m0 = (unsigned)an.w, mi = mask_in[t];
     const bool px = g.periodic & 1, py = g.periodic & 2, pz = g.periodic & 4;
     const long long sa = sidx(g, an.x, an.y, an.z);
+    const bool a_solid_fused = fused && (fused[sa] & kSolidBit);
     C Fx = C(0), Fy = C(0), Fz = C(0);
 #pragma unroll
     for (int k = 1; k < Q; ++k) {
@@ -340,13 +394,23 @@ __global__ void __launch_bounds__(kForceThreads)
       if (!(b0 || bi)) continue;
       const long long sq = sidx(g, wrap_axis(an.x + Lt::c(k, 0), g.nx, px), wrap_axis(an.y + Lt::c(k, 1), g.ny, py),
                                 wrap_axis(an.z + Lt::c(k, 2), g.nz, pz));
+      const S* pa = F + (size_t)k * g.dstride + sa;           // f_k(x) in representation A
+      const S* pq = F + (size_t)Lt::inv(k) * g.dstride + sq;  // f_inv(k)(x + c_k) in representation A
+      // With a fused no-slip map the solid end's incoming slot is not written:
+      // bounce-back makes it equal to the fluid end's outgoing population.
+      const bool solid_fused = b0 ? a_solid_fused : (fused && (fused[sq] & kSolidBit));
       C a;
-      if (std::is_same<S, __half>::value)
-        a = Store<S>::dev(F + (size_t)k * g.dstride + sa, inv_scale) +
-            Store<S>::dev(F + (size_t)Lt::inv(k) * g.dstride + sq, inv_scale);
-      else
-        a = Store<S>::val(F + (size_t)k * g.dstride + sa, inv_scale) +
-            Store<S>::val(F + (size_t)Lt::inv(k) * g.dstride + sq, inv_scale) - C(2);
+      if (solid_fused) {
+        // outgoing slot of the fluid end: the anchor's neighbour q for mask0
+        // links, the anchor itself for mask_in links; representation B holds
+        // it in the other slot of the pair.
+        const S* out = (b0 != (parity != 0)) ? pq : pa;
+        a = kDev ? C(2) * Store<S>::dev(out, inv_scale) : C(2) * Store<S>::val(out, inv_scale) - C(2);
+      } else if (kDev) {
+        a = Store<S>::dev(pa, inv_scale) + Store<S>::dev(pq, inv_scale);
+      } else {
+        a = Store<S>::val(pa, inv_scale) + Store<S>::val(pq, inv_scale) - C(2);
+      }
       if (bi) a = -a;
       const C wa = a * C(Lt::w(k));
       if (Lt::c(k, 0)) Fx += Lt::c(k, 0) > 0 ? wa : -wa;
@@ -396,20 +460,20 @@ cudaError_t launch_reduce_rows(const double* partials, int nblocks, int width, d
 
 template <int Q, class S>
 static cudaError_t force_impl(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,
-                              const double* r0, const double* pos0, double dx, float inv_scale, double* partials,
-                              double* out6, cudaStream_t st) {
+                              const double* r0, const double* pos0, double dx, float inv_scale,
+                              const uint32_t* fused, int parity, double* partials, double* out6, cudaStream_t st) {
   const int nb = force_blocks(n);
   k_force<Q, S><<<nb, kForceThreads, 0, st>>>((const S*)d.F, d.g, cells, mask_in, n, field, r0[0], r0[1], r0[2],
-                                              pos0[0], pos0[1], pos0[2], dx, inv_scale, partials);
+                                              pos0[0], pos0[1], pos0[2], dx, inv_scale, fused, parity, partials);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return launch_reduce_rows(partials, nb, 6, out6, st);
 }
 
 cudaError_t launch_force(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,
-                         const double* r0, const double* pos0, double dx, float inv_scale, double* partials,
-                         double* out6, cudaStream_t st) {
-  ASLB_DISPATCH(d, force_impl, d, cells, mask_in, n, field, r0, pos0, dx, inv_scale, partials, out6, st)
+                         const double* r0, const double* pos0, double dx, float inv_scale, const uint32_t* fused,
+                         int parity, double* partials, double* out6, cudaStream_t st) {
+  ASLB_DISPATCH(d, force_impl, d, cells, mask_in, n, field, r0, pos0, dx, inv_scale, fused, parity, partials, out6, st)
 }
 
 // ---------------------------------------------------------------------------
@@ -435,6 +499,7 @@ __global__ void __launch_bounds__(kMomentThreads)
     const long long r = c / g.nz;
     const int y = int(r % g.ny) + 1;
     const int x = int(r / g.ny) + 1;
+    if (p.mask && (p.mask[sidx(g, x, y, z)] & kSolidBit)) continue;  // not advanced in fused mode
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
       long long s;

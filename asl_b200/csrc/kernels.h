@@ -34,13 +34,18 @@ cudaError_t launch_import_f(const DomainDev& d, const StepParams& p, const void*
 // Boundary links: anchors (x, y, z, direction mask) in ghosted coordinates.
 cudaError_t launch_bc(const DomainDev& d, const int4* anchors, int n, const BcParams& bp, int parity,
                       cudaStream_t st);
+// Direction-sorted links (one thread per link), the common case of every
+// condition except the velocity maps.
+cudaError_t launch_bc_links(const DomainDev& d, const int* links, int n, const LinkSet& ls, const BcParams& bp,
+                            int parity, cudaStream_t st);
 // Surface force: per-cell field (ASL layout, optional) and per-block FP64
 // partial sums of (F, (r - r0) x F), then a fixed-order final sum into out6.
 int force_blocks(int n);
 cudaError_t launch_force(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,
-                         const double* r0, const double* pos0, double dx, float inv_scale, double* partials,
-                         double* out6, cudaStream_t st);
-// Global diagnostics over interior cells: (mass, momentum x, y, z) in FP64.
+                         const double* r0, const double* pos0, double dx, float inv_scale, const uint32_t* fused,
+                         int parity, double* partials, double* out6, cudaStream_t st);
+// Global diagnostics over interior cells (fluid cells in fused mode): (mass,
+// momentum x, y, z) in FP64.
 int moments_blocks(const GridDesc& g);
 cudaError_t launch_moments(const DomainDev& d, const StepParams& p, int parity, double* partials, double* out4,
                            cudaStream_t st);

@@ -54,17 +54,26 @@ __global__ void __launch_bounds__(256) k_stream_collide(S* __restrict__ F, const
   const int x = blockIdx.z + 1;
   if (z > g.nz || y > g.ny) return;
   const int s = (int)sidx(g, x, y, z);
+  uint32_t bb = 0;
+  if (p.mask) {
+    bb = p.mask[s];
+    if (bb & kSolidBit) return;  // solid cell of a fused no-slip map: not advanced
+  }
   int ox[3], oy[3], oz[3];
-  if (ODD) nb_offsets(g, x, y, z, ox, oy, oz);
+  nb_offsets(g, x, y, z, ox, oy, oz);
   C f[Q];
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
+    // Pulled from the upstream neighbour, or, where that neighbour is a fused
+    // solid cell, bounced back from this cell's own outgoing population: the
+    // two slots swap roles between the representations.
+    const int up = s + ox[1 - Lt::c(i, 0)] + oy[1 - Lt::c(i, 1)] + oz[1 - Lt::c(i, 2)];
+    const bool b = (bb >> i) & 1u;
     const S* src;
     if (ODD)
-      src = F + (size_t)i * g.dstride +
-            (s + ox[1 - Lt::c(i, 0)] + oy[1 - Lt::c(i, 1)] + oz[1 - Lt::c(i, 2)]);
+      src = b ? F + (size_t)Lt::inv(i) * g.dstride + s : F + (size_t)i * g.dstride + up;
     else
-      src = F + (size_t)Lt::inv(i) * g.dstride + s;
+      src = b ? F + (size_t)i * g.dstride + up : F + (size_t)Lt::inv(i) * g.dstride + s;
     f[i] = Store<S>::load(src, p);
   }
   C rho, u[3];

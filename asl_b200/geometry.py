@@ -167,54 +167,20 @@ def pack_spheres(size, rmin: float, rmax: float, solid_fraction: float, seed: in
                  attempts: int = 400) -> SpherePack:
     """Random sequential addition of non-overlapping spheres, radii U[rmin, rmax],
     placed largest first until the sphere volume reaches ``solid_fraction`` of
-    the box. Spheres stay inside y/z; x is periodic when ``periodic_x``."""
+    the box. Spheres stay inside y/z; x is periodic when ``periodic_x``.
+    Runs in the library's host code (aslb_geom_pack_spheres)."""
+    import ctypes as C
+    from . import _lib as L
     nx, ny, nz = size
-    rng = np.random.default_rng(seed)
-    target = solid_fraction * nx * ny * nz
-    radii = []
-    vol = 0.0
-    while vol < target * 1.25:
-        r = float(rng.uniform(rmin, rmax))
-        radii.append(r)
-        vol += 4.0 / 3.0 * math.pi * r ** 3
-    radii.sort(reverse=True)
-    bucket = 2.0 * rmax
-    nbx, nby, nbz = (int(math.ceil(n / bucket)) for n in size)
-    grid: dict = {}
-    centers, placed = [], []
-    placed_vol = 0.0
-    for r in radii:
-        if placed_vol >= target:
-            break
-        for _ in range(attempts):
-            c = np.array([rng.uniform(0, nx) if periodic_x else rng.uniform(r, nx - 1 - r),
-                          rng.uniform(r, ny - 1 - r), rng.uniform(r, nz - 1 - r)])
-            bx, by, bz = int(c[0] // bucket), int(c[1] // bucket), int(c[2] // bucket)
-            ok = True
-            for ix in (bx - 1, bx, bx + 1):
-                jx = ix % nbx if periodic_x else ix
-                for iy in (by - 1, by, by + 1):
-                    for iz in (bz - 1, bz, bz + 1):
-                        for k in grid.get((jx, iy, iz), ()):
-                            d = centers[k] - c
-                            if periodic_x:
-                                d[0] -= nx * round(d[0] / nx)
-                            if d @ d < (placed[k] + r) ** 2:
-                                ok = False
-                                break
-                        if not ok:
-                            break
-                    if not ok:
-                        break
-                if not ok:
-                    break
-            if ok:
-                grid.setdefault((bx % nbx if periodic_x else bx, by, bz), []).append(len(centers))
-                centers.append(c)
-                placed.append(r)
-                placed_vol += 4.0 / 3.0 * math.pi * r ** 3
-                break
-    return SpherePack(np.array(centers).reshape(-1, 3), np.array(placed))
+    cap = int(solid_fraction * nx * ny * nz / (4.0 / 3.0 * math.pi * rmin ** 3)) + 16
+    centers = np.zeros((cap, 3))
+    radii = np.zeros(cap)
+    n = C.c_int(0)
+    L.check(L.load().aslb_geom_pack_spheres(int(nx), int(ny), int(nz), float(rmin), float(rmax), float(solid_fraction),
+                                            int(seed), int(bool(periodic_x)), int(attempts), cap,
+                                            centers.ctypes.data_as(L._pd), radii.ctypes.data_as(L._pd), C.byref(n)),
+            "pack_spheres")
+    return SpherePack(centers[:n.value].copy(), radii[:n.value].copy())
 
 
 def rasterize_spheres(block, pack: SpherePack, periodic_x: bool = True, margin: float = 2.0) -> np.ndarray:

@@ -307,6 +307,21 @@ class BC:
     def num_links(self) -> int:
         return int(self.num.lib.aslb_bc_num_links(self.h))
 
+    @property
+    def kernels(self) -> int:
+        """Kernel launches per execute()."""
+        return int(self.num.lib.aslb_bc_kernels(self.h))
+
+    def fuse(self, m: np.ndarray):
+        """Fold this no-slip map condition into the stream-collide kernel
+        (extension): solid cells are skipped, bounce-back happens inline."""
+        arr = _map_array(self.num, m)
+        L.check(self.num.lib.aslb_bc_fuse(self.h, arr.ctypes.data_as(L._pf)), "BCNoSlipMap::fuse")
+
+    @property
+    def fused(self) -> bool:
+        return bool(self.num.lib.aslb_bc_is_fused(self.h))
+
     def __del__(self):
         try:
             if self.h:

@@ -81,8 +81,10 @@ def porous_channel(size=(512, 256, 256), rmin=4.0, rmax=12.0, solid_fraction=0.4
                     info={"spheres": int(len(pack.radii)), "solid_fraction": solid, "seed": seed, "tau": tau})
 
 
-def build_lbgk(w: Workload, storage="f32", compVel=True, compRho=True, closure_cls=None):
-    """Instantiate the workload on the GPU through the ASL-style API."""
+def build_lbgk(w: Workload, storage="f32", compVel=True, compRho=True, closure_cls=None, fuse=False):
+    """Instantiate the workload on the GPU through the ASL-style API. With
+    ``fuse`` the no-slip map condition (last in every workload's order) is
+    folded into the stream-collide kernel."""
     from . import lbgk as A
     vt = {15: A.d3q15(), 19: A.d3q19(), 27: A.d3q27()}[w.q]
     cls = closure_cls or A.LBGK
@@ -103,7 +105,10 @@ def build_lbgk(w: Workload, storage="f32", compVel=True, compRho=True, closure_c
         elif s.kind == "pressure_velocity":
             bcs.append(A.generateBCConstantPressureVelocity(lb, s.p, s.u, walls))
         elif s.kind == "map_noslip":
-            bcs.append(A.generateBCNoSlip(lb, w.map))
+            bc = A.generateBCNoSlip(lb, w.map)
+            if fuse:
+                bc.fuse(w.map)
+            bcs.append(bc)
         else:
             raise ValueError(s.kind)
     A.initAll(bcs)

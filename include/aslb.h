@@ -176,11 +176,23 @@ int aslb_bc_slice_create(aslb_lbgk* h, int kind, unsigned wallmask, double p, co
  * generateBCConstantPressureVelocity(map) (src/num/aslLBGKBC.cxx:205-438). */
 int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const double u[3], const double omega[3],
                        const double center[3], aslb_bc** out);
+/* Extension (no ASL analogue): fold a no-slip map condition into the
+ * stream-collide kernel. Solid cells of `map` (the same map the condition was
+ * made from) are no longer advanced and fluid cells take bounce-back
+ * populations inline; fluid results are bit-identical to the separate
+ * condition, provided the fused condition is the last one to write its links
+ * each step (later writers win in ASL). Rejects maps where a fluid cell
+ * borders a solid cell at or below the -0.9999 guard. Solid-cell populations
+ * are not meaningful afterwards. */
+int aslb_bc_fuse(aslb_bc* bc, const float* map);
+int aslb_bc_is_fused(aslb_bc* bc);
 /* BCond::execute() (src/num/aslLBGKBC.cxx:80-83, 257-260). */
 int aslb_bc_execute(aslb_bc* bc);
 int aslb_bc_destroy(aslb_bc* bc);
 /* Number of boundary links (direction slots written per execute). */
 long long aslb_bc_num_links(aslb_bc* bc);
+/* Kernel launches one execute makes (0 for a fused condition). */
+int aslb_bc_kernels(aslb_bc* bc);
 
 /* ---- surface force ------------------------------------------------------- */
 
@@ -192,6 +204,18 @@ int aslb_force_create(aslb_lbgk* h, const float* map, aslb_force** out);
  * receives the per-cell force field. Synchronises. */
 int aslb_force_compute(aslb_force* fc, const double r0[3], float* field_host, double out6[6]);
 int aslb_force_destroy(aslb_force* fc);
+
+/* ---- workload geometry (host) ----------------------------------------- */
+
+/* Extension (no ASL analogue; ASL builds such media from user distance
+ * functions): seeded random sequential addition of non-overlapping spheres in
+ * an nx x ny x nz box, radii uniform in [rmin, rmax] placed largest first until
+ * their volume reaches solid_fraction of the box. Spheres stay inside y and z;
+ * x wraps when periodic_x. centers (3 * max_spheres doubles, interior-cell
+ * coordinates) and radii (max_spheres) receive *count spheres. */
+int aslb_geom_pack_spheres(int nx, int ny, int nz, double rmin, double rmax, double solid_fraction,
+                           unsigned long long seed, int periodic_x, int attempts, int max_spheres, double* centers,
+                           double* radii, int* count);
 
 #ifdef __cplusplus
 }

@@ -1,8 +1,9 @@
 """GPU parity: the CUDA path (through libaslb.so's C ABI) against the CPU oracle.
 
 Tolerances: FP64 storage must match the FP64 oracle to 1e-12 (rounding
-only); FP32 storage the FP32 oracle to 2e-6 absolute on populations for a few
-steps (fused multiply-add contraction differs); the canonical cylinder
+only); FP32 storage the FP32 oracle to 1e-5 absolute on populations of order 1
+over a few steps (the GPU contracts multiply-adds, the oracle does not: about
+20 ulp after 7 steps); the canonical cylinder
 channel to relative L2 <= 1e-4 on rho and u over interior fluid cells and
 <= 1e-4 on the drag after 1000 steps.
 """
@@ -42,7 +43,7 @@ def sphere_map(g, center, r):
 
 @pytest.mark.parametrize("q", [15, 19, 27])
 @pytest.mark.parametrize("closure", [0, 1, 2])
-@pytest.mark.parametrize("storage,prec,tol", [("f64", 8, 1e-12), ("f32", 4, 2e-6)])
+@pytest.mark.parametrize("storage,prec,tol", [("f64", 8, 1e-12), ("f32", 4, 1e-5)])
 def test_periodic_steps_match_oracle(gpu, oracle_mod, q, closure, storage, prec, tol):
     size = (10, 9, 8)
     g = tuple(s + 2 for s in size)
@@ -80,7 +81,7 @@ def test_coriolis_incompressible_match_oracle(gpu, oracle_mod):
 
 
 @pytest.mark.parametrize("q", [15, 19, 27])
-@pytest.mark.parametrize("storage,prec,tol", [("f64", 8, 1e-12), ("f32", 4, 3e-6)])
+@pytest.mark.parametrize("storage,prec,tol", [("f64", 8, 1e-12), ("f32", 4, 2e-5)])
 def test_boundaries_and_force_match_oracle(gpu, oracle_mod, q, storage, prec, tol):
     size = (11, 9, 10)
     g = tuple(s + 2 for s in size)
@@ -252,3 +253,36 @@ def test_channel_cylinder_parity_1000_steps(gpu, oracle_mod):
     got = force.execute(r0=(32.0, 32.0, 31.5))
     want = o.force(w.map, r0=(32.0, 32.0, 31.5))
     assert abs(got[0] - want[0]) <= 1e-4 * abs(want[0])
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
+@pytest.mark.parametrize("case", ["porous", "cylinder"])
+def test_fused_noslip_bitwise_equals_separate_condition(gpu, storage, case):
+    """Folding the no-slip map into the stream-collide kernel leaves every
+    fluid population, density, velocity and the surface force bit-identical."""
+    if case == "porous":
+        w = W.porous_channel(size=(64, 32, 32), rmin=2.0, rmax=5.0, solid_fraction=0.35, steps=0)
+    else:
+        w = W.channel_cylinder(size=(48, 24, 20), radius=5.0, center=(14.0, 12.0), steps=0)
+    a, abcs = W.build_lbgk(w, storage=storage)
+    b, bbcs = W.build_lbgk(w, storage=storage, fuse=True)
+    assert bbcs[-1].fused and not abcs[-1].fused
+    fluid = w.map[1:-1, 1:-1, 1:-1] > 0
+    for n in (13, 12):
+        a.run(n, abcs)
+        b.run(n, bbcs)
+        assert np.array_equal(a.getF()[I4][:, fluid], b.getF()[I4][:, fluid])
+        assert np.array_equal(a.getVelocity()[I4][:, fluid], b.getVelocity()[I4][:, fluid])
+        fa = A.generateComputeSurfaceForce(a, w.map).execute(r0=(1.0, 2.0, 3.0))
+        fb = A.generateComputeSurfaceForce(b, w.map).execute(r0=(1.0, 2.0, 3.0))
+        assert np.array_equal(fa, fb)
+
+
+def test_fuse_rejects_unguarded_map(gpu):
+    lb = A.LBGK(A.Block((12, 10, 8)), 0.1, A.d3q19())
+    g = lb.block.ghosted
+    pos = np.stack(np.meshgrid(*[np.arange(n) - 1.0 for n in g], indexing="ij"))
+    raw = (np.sqrt(((pos - 5.0) ** 2).sum(0)) - 3.0).astype(np.float32)  # not normalised: reaches -3
+    bc = A.generateBCNoSlip(lb, raw)
+    with pytest.raises(A.L.ASLError):
+        bc.fuse(raw)
