@@ -65,7 +65,7 @@ PROTOTYPES = {
     "aslb_lbgk_moments": (C.c_int, [_vp, _pd]),
     "aslb_bc_slice_create": (C.c_int, [_vp, C.c_int, C.c_uint, C.c_double, _pd, C.POINTER(_vp)]),
     "aslb_bc_map_create": (C.c_int, [_vp, C.c_int, _pf, C.c_double, _pd, _pd, _pd, C.POINTER(_vp)]),
-    "aslb_bc_fuse": (C.c_int, [_vp, _pf]),
+    "aslb_bc_fuse": (C.c_int, [_vp]),
     "aslb_bc_is_fused": (C.c_int, [_vp]),
     "aslb_bc_execute": (C.c_int, [_vp]),
     "aslb_bc_destroy": (C.c_int, [_vp]),

@@ -69,6 +69,8 @@ struct aslb_bc {
   long long links = 0;
   bool fused = false;  // folded into the stream-collide kernel (execute is a no-op)
   BcParams bp{};
+  std::vector<int> host_links;     // host copies, kept for fusing
+  std::vector<int4> host_anchors;
 };
 
 struct aslb_force {
@@ -211,6 +213,8 @@ int finalize_links(aslb_lbgk* h, aslb_bc* bc, const std::vector<Cand>& cand, boo
   for (auto& a : anchors) bc->links += __builtin_popcount((unsigned)a.w);
   int r = upload(&bc->dlinks, flat);
   if (!r) r = upload(&bc->anchors, anchors);
+  bc->host_links.swap(flat);
+  bc->host_anchors.swap(anchors);
   return r;
 }
 
@@ -294,14 +298,18 @@ int aslb_lbgk_create(int nx, int ny, int nz, int q, int storage, double nu, unsi
   GridDesc& g = h->d.g;
   g.nx = nx; g.ny = ny; g.nz = nz;
   g.gx = nx + 2; g.gy = ny + 2; g.gz = nz + 2;
-  g.pitch = ((g.gz + kZOff + 7) / 8) * 8;
+  // Rows aligned to 128 bytes: the first interior cell (z = 1) of every row at
+  // a multiple of `align` elements.
+  const int align = int(128 / storage_bytes(storage));
+  g.zoff = align - 1;
+  g.pitch = ((g.gz + g.zoff + align - 1) / align) * align;
   g.periodic = int((flags >> 3) & 7u);
   g.plane = (long long)g.gy * g.pitch;
-  g.dstride = (((long long)g.gx * g.plane + 63) / 64) * 64;
+  g.dstride = (((long long)g.gx * g.plane + align - 1) / align) * align;
   g.L = (long long)g.gx * g.gy * g.gz;
-  if (g.dstride >= (1ll << 31)) {
+  if ((long long)q * g.dstride >= (1ll << 32) || g.plane >= (1ll << 30)) {
     delete h;
-    return fail(ASLB_ERR_ARG, "aslb_lbgk_create: domain too large for 32-bit per-direction indexing");
+    return fail(ASLB_ERR_ARG, "aslb_lbgk_create: domain too large for 32-bit element indexing on one GPU");
   }
   h->d.q = q;
   h->d.storage = storage;
@@ -514,6 +522,11 @@ int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int us
   if (nsteps < 0 || nbc < 0 || (nbc > 0 && !bcs)) return fail(ASLB_ERR_ARG, "aslb_lbgk_run: bad arguments");
   for (int b = 0; b < nbc; ++b)
     if (!bcs[b] || bcs[b]->h != h) return fail(ASLB_ERR_ARG, "aslb_lbgk_run: boundary of another domain");
+  // A fused condition takes effect inside the next step, after every separate
+  // condition of this step: it must be the last writer of its links.
+  for (int b = 1; b < nbc; ++b)
+    if (bcs[b - 1]->fused && !bcs[b]->fused)
+      return fail(ASLB_ERR_ARG, "aslb_lbgk_run: fused conditions must come after all separate ones");
   auto eager = [&](int n) -> int {
     for (int i = 0; i < n; ++i) {
       int r = do_step(h);
@@ -525,7 +538,7 @@ int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int us
     }
     return ASLB_OK;
   };
-  if (!use_graph || h->stream == nullptr || nsteps < 4) return eager(nsteps);
+  if (!use_graph || h->stream == nullptr || nsteps < 2) return eager(nsteps);
   int done = 0;
   if (h->macro_once) {
     int r = eager(1);
@@ -782,39 +795,49 @@ int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const
   return ASLB_OK;
 }
 
-int aslb_bc_fuse(aslb_bc* bc, const float* map) {
-  if (!bc || !map) return fail(ASLB_ERR_ARG, "aslb_bc_fuse: null argument");
-  if (bc->bp.kind != ASLB_BC_MAP_NOSLIP) return fail(ASLB_ERR_ARG, "aslb_bc_fuse: only no-slip maps can be fused");
+int aslb_bc_fuse(aslb_bc* bc) {
+  if (!bc) return fail(ASLB_ERR_ARG, "aslb_bc_fuse: null argument");
+  if (bc->bp.kind != ASLB_BC_MAP_NOSLIP && bc->bp.kind != ASLB_BC_NOSLIP)
+    return fail(ASLB_ERR_ARG, "aslb_bc_fuse: only no-slip conditions can be fused");
   if (bc->fused) return ASLB_OK;
   aslb_lbgk* h = bc->h;
   const GridDesc& g = h->d.g;
   const int q = h->d.q;
   std::vector<uint32_t> m = h->mask_host.empty() ? std::vector<uint32_t>((size_t)g.dstride, 0u) : h->mask_host;
-  for (int x = 0; x < g.gx; ++x)
-    for (int y = 0; y < g.gy; ++y)
-      for (int z = 0; z < g.gz; ++z) {
-        if (on_periodic_ghost(h, x, y, z)) continue;
-        if (map[aidx(g, x, y, z)] <= 0.f) m[sidx(g, x, y, z)] |= kSolidBit;
-      }
-  for (int x = 1; x <= g.nx; ++x)
-    for (int y = 1; y <= g.ny; ++y)
-      for (int z = 1; z <= g.nz; ++z) {
-        if (map[aidx(g, x, y, z)] <= 0.f) continue;
-        uint32_t bits = 0;
-        for (int k = 1; k < q; ++k) {
-          const int sx = wrapc(h, x - lattice_c(q, k, 0), 0), sy = wrapc(h, y - lattice_c(q, k, 1), 1),
-                    sz = wrapc(h, z - lattice_c(q, k, 2), 2);
-          const float ms = map_at(g, map, sx, sy, sz);
-          if (ms > 0.f) continue;
-          // The map condition skips solid cells at or below -0.9999: their links
-          // would pull a collided solid population, which fused mode cannot give.
-          if (!(ms > -0.9999f))
-            return fail(ASLB_ERR_ARG, "aslb_bc_fuse: a fluid cell borders a solid cell beyond the map guard "
-                                      "(-0.9999); normalise the map or keep the condition unfused");
-          bits |= 1u << k;
-        }
-        m[sidx(g, x, y, z)] |= bits;
-      }
+  // Link (anchor a, direction k) enters fluid cell f = a + c_k: f reads it by
+  // bounce-back (bit k), and an interior anchor, which the stream-collide
+  // kernel advances, skips its write of direction k (bit k + solid bit).
+  auto add = [&](long long sa, bool anchor_interior, long long sf, int k) -> int {
+    if (m[sf] & kSolidBit)
+      return fail(ASLB_ERR_ARG, "aslb_bc_fuse: a cell is fluid for this condition and solid for a fused one");
+    m[sf] |= 1u << k;
+    if (anchor_interior) {
+      if (m[sa] && !(m[sa] & kSolidBit))
+        return fail(ASLB_ERR_ARG, "aslb_bc_fuse: a cell is solid for this condition and fluid for a fused one");
+      m[sa] |= kSolidBit | (1u << k);
+    }
+    return ASLB_OK;
+  };
+  for (int k = 1; k < q; ++k)
+    for (int t = bc->ls.seg[k]; t < bc->ls.seg[k + 1]; ++t) {
+      const long long sa = bc->host_links[t];
+      const long long local = sa % ((long long)g.gx * g.plane);
+      const int z = int(local % g.pitch) - g.zoff;
+      const int y = int((local / g.pitch) % g.gy);
+      const int x = int(local / g.plane);
+      int r = add(sa, interior(g, x, y, z), sa + bc->ls.off[k], k);
+      if (r) return r;
+    }
+  for (const int4& an : bc->host_anchors)
+    for (int k = 1; k < q; ++k) {
+      if (!((unsigned)an.w >> k & 1u)) continue;
+      const int ax = wrapc(h, an.x, 0), ay = wrapc(h, an.y, 1), az = wrapc(h, an.z, 2);
+      const long long sa = sidx(g, ax, ay, az);
+      const long long sf = sidx(g, wrapc(h, an.x + lattice_c(q, k, 0), 0), wrapc(h, an.y + lattice_c(q, k, 1), 1),
+                                wrapc(h, an.z + lattice_c(q, k, 2), 2));
+      int r = add(sa, interior(g, ax, ay, az), sf, k);
+      if (r) return r;
+    }
   if (!h->mask_dev) ASLB_CUDA(cudaMalloc((void**)&h->mask_dev, (size_t)g.dstride * sizeof(uint32_t)));
   ASLB_CUDA(cudaStreamSynchronize(h->stream));
   ASLB_CUDA(cudaMemcpy(h->mask_dev, m.data(), m.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));

@@ -5,10 +5,12 @@
 // like ASL's DataWithGhostNodes (src/data/aslDataWithGhostNodes.h:97-145),
 // one ghost layer: ghosted coordinates x in [0, Nx+1] etc. Direction i of the
 // populations is one array; inside it cell (x, y, z) sits at
-//     ((x * Gy + y) * pitch) + kZOff + z
-// with pitch a multiple of 8 elements and kZOff = 7, so the first interior
-// cell of every z-row (z = 1) starts on a 32-byte boundary. All Q arrays live
-// in one allocation, `dstride` elements apart.
+//     ((x * Gy + y) * pitch) + zoff + z
+// with pitch a multiple of 128 bytes and zoff = 128 B / element - 1, so the
+// first interior cell of every z-row (z = 1) starts on a 128-byte boundary
+// (HBM is read in 64-byte pieces: a 32-byte aligned row would drag one extra
+// piece per row). All Q arrays live in one allocation, `dstride` elements
+// apart; Q * dstride < 2^32 so element indices are 32-bit.
 //
 // Streaming is the AA pattern: the populations are stored in one of two
 // representations that alternate every step (parity 0 = "A", 1 = "B"):
@@ -25,12 +27,11 @@
 
 namespace aslb {
 
-constexpr int kZOff = 7;
-
 struct GridDesc {
   int nx, ny, nz;     // interior cells
   int gx, gy, gz;     // ghosted sizes (n + 2)
   int pitch;          // elements per z-row in storage
+  int zoff;           // storage position of ghost z = 0 within a row
   int periodic;       // bit0 x, bit1 y, bit2 z
   long long plane;    // gy * pitch
   long long dstride;  // elements between direction arrays
@@ -38,7 +39,7 @@ struct GridDesc {
 };
 
 __host__ __device__ inline long long sidx(const GridDesc& g, int x, int y, int z) {
-  return ((long long)x * g.gy + y) * g.pitch + kZOff + z;
+  return ((long long)x * g.gy + y) * g.pitch + g.zoff + z;
 }
 // ASL's flattening of the ghosted block, z fastest (src/data/aslBlocks.h:118-130).
 __host__ __device__ inline long long aidx(const GridDesc& g, int x, int y, int z) {
@@ -63,9 +64,11 @@ struct StepParams {
   int write_rho, write_vel;
   float scale, inv_scale;  // FP16 storage: d = (f - 1) * scale
   const void* mlp;         // closure network (device), CL == 3
-  // Fused no-slip maps (null when none): per storage cell, bit 31 marks a
-  // solid cell that is not advanced, bit k that population k enters this
-  // fluid cell from such a solid cell and is taken by bounce-back instead.
+  // Fused no-slip conditions (null when none), one word per storage cell.
+  // Fluid cell: bit k = population k enters through a no-slip link, so it is
+  // read by bounce-back from this cell's own outgoing population. Solid cell
+  // (bit 31 set): bit k = its outgoing population k lands in such a link's
+  // incoming slot, which the condition overwrites, so the write is skipped.
   const uint32_t* mask;
 };
 

@@ -37,6 +37,38 @@ cudaError_t launch_step(const DomainDev& d, const StepParams& p, int closure, in
   }
 
 // ---------------------------------------------------------------------------
+// Storage index of f*_i(x), the post-collision population of cell x in
+// direction i, for either representation. With fused no-slip links the
+// incoming slot of a link is never written; its value is the fluid end's
+// outgoing population, held by the other slot of the pair. Returns -1 where
+// representation B would need a cell outside the block (ghost cells only).
+template <int Q>
+__device__ __forceinline__ long long fstar_index(const GridDesc& g, const uint32_t* __restrict__ mask, int parity,
+                                                 int x, int y, int z, int i) {
+  using Lt = Lattice<Q>;
+  const bool inter = x >= 1 && x <= g.nx && y >= 1 && y <= g.ny && z >= 1 && z <= g.nz;
+  int tx = x + Lt::c(i, 0), ty = y + Lt::c(i, 1), tz = z + Lt::c(i, 2);
+  if (inter) {
+    tx = wrap_axis(tx, g.nx, g.periodic & 1);
+    ty = wrap_axis(ty, g.ny, g.periodic & 2);
+    tz = wrap_axis(tz, g.nz, g.periodic & 4);
+  }
+  const bool tin = tx >= 0 && ty >= 0 && tz >= 0 && tx < g.gx && ty < g.gy && tz < g.gz;
+  const long long sx = sidx(g, wrap_axis(x, g.nx, g.periodic & 1), wrap_axis(y, g.ny, g.periodic & 2),
+                            wrap_axis(z, g.nz, g.periodic & 4));
+  const long long sq = tin ? sidx(g, tx, ty, tz) : -1;
+  bool fused = false;
+  if (mask && tin && tx >= 1 && tx <= g.nx && ty >= 1 && ty <= g.ny && tz >= 1 && tz <= g.nz) {
+    const uint32_t m = mask[sq];
+    fused = !(m & kSolidBit) && ((m >> i) & 1u);
+  }
+  const bool in_own = (parity == 0) != fused;  // slot F[i][x] (else F[inv i][x + c_i])
+  if (in_own) return (long long)i * g.dstride + sx;
+  if (!tin) return -1;
+  return (long long)Lt::inv(i) * g.dstride + sq;
+}
+
+// ---------------------------------------------------------------------------
 // initF: f_i = rho (1 + 3 c.u + 4.5 (c.u)^2 - 1.5 u.u) on every ghosted cell
 // (src/num/aslLBGK.cxx:262-280), representation A.
 template <int Q, class S>
@@ -90,32 +122,16 @@ cudaError_t launch_init_f(const DomainDev& d, const StepParams& p, double rho0, 
 template <int Q, class S>
 __global__ void k_export_f(const S* __restrict__ F, const GridDesc g, const StepParams p, int parity,
                            typename MacroT<S>::T* __restrict__ out) {
-  using Lt = Lattice<Q>;
   using M = typename MacroT<S>::T;
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
   const int x = blockIdx.z;
   if (z >= g.gz) return;
   const long long a = aidx(g, x, y, z);
-  const bool inter = x >= 1 && x <= g.nx && y >= 1 && y <= g.ny && z >= 1 && z <= g.nz;
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
-    M v;
-    if (parity == 0) {
-      v = M(Store<S>::val(F + (size_t)i * g.dstride + sidx(g, x, y, z), p.inv_scale));
-    } else {
-      int tx = x + Lt::c(i, 0), ty = y + Lt::c(i, 1), tz = z + Lt::c(i, 2);
-      if (inter) {
-        tx = wrap_axis(tx, g.nx, g.periodic & 1);
-        ty = wrap_axis(ty, g.ny, g.periodic & 2);
-        tz = wrap_axis(tz, g.nz, g.periodic & 4);
-      }
-      if (tx < 0 || ty < 0 || tz < 0 || tx >= g.gx || ty >= g.gy || tz >= g.gz)
-        v = M(NAN);
-      else
-        v = M(Store<S>::val(F + (size_t)Lt::inv(i) * g.dstride + sidx(g, tx, ty, tz), p.inv_scale));
-    }
-    out[(long long)i * g.L + a] = v;
+    const long long k = fstar_index<Q>(g, p.mask, parity, x, y, z, i);
+    out[(long long)i * g.L + a] = k < 0 ? M(NAN) : M(Store<S>::val(F + k, p.inv_scale));
   }
 }
 
@@ -386,7 +402,6 @@ __global__ void __launch_bounds__(kForceThreads)
     const unsigned m0 = (unsigned)an.w, mi = mask_in[t];
     const bool px = g.periodic & 1, py = g.periodic & 2, pz = g.periodic & 4;
     const long long sa = sidx(g, an.x, an.y, an.z);
-    const bool a_solid_fused = fused && (fused[sa] & kSolidBit);
     C Fx = C(0), Fy = C(0), Fz = C(0);
 #pragma unroll
     for (int k = 1; k < Q; ++k) {
@@ -396,9 +411,15 @@ __global__ void __launch_bounds__(kForceThreads)
                                 wrap_axis(an.z + Lt::c(k, 2), g.nz, pz));
       const S* pa = F + (size_t)k * g.dstride + sa;           // f_k(x) in representation A
       const S* pq = F + (size_t)Lt::inv(k) * g.dstride + sq;  // f_inv(k)(x + c_k) in representation A
-      // With a fused no-slip map the solid end's incoming slot is not written:
-      // bounce-back makes it equal to the fluid end's outgoing population.
-      const bool solid_fused = b0 ? a_solid_fused : (fused && (fused[sq] & kSolidBit));
+      // A fused no-slip link never writes the solid end's incoming slot:
+      // bounce-back makes it equal to the fluid end's outgoing population. The
+      // fluid end carries the link's bit (direction k into q for mask0 links,
+      // direction inv(k) into the anchor for mask_in links).
+      bool solid_fused = false;
+      if (fused) {
+        const uint32_t mf = b0 ? fused[sq] : fused[sa];
+        solid_fused = !(mf & kSolidBit) && ((mf >> (b0 ? k : Lt::inv(k))) & 1u);
+      }
       C a;
       if (solid_fused) {
         // outgoing slot of the fluid end: the anchor's neighbour q for mask0
@@ -499,20 +520,9 @@ __global__ void __launch_bounds__(kMomentThreads)
     const long long r = c / g.nz;
     const int y = int(r % g.ny) + 1;
     const int x = int(r / g.ny) + 1;
-    if (p.mask && (p.mask[sidx(g, x, y, z)] & kSolidBit)) continue;  // not advanced in fused mode
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-      long long s;
-      int dir;
-      if (parity == 0) {
-        s = sidx(g, x, y, z);
-        dir = i;
-      } else {
-        s = sidx(g, wrap_axis(x + Lt::c(i, 0), g.nx, g.periodic & 1), wrap_axis(y + Lt::c(i, 1), g.ny, g.periodic & 2),
-                 wrap_axis(z + Lt::c(i, 2), g.nz, g.periodic & 4));
-        dir = Lt::inv(i);
-      }
-      const double fi = double(Store<S>::val(F + (size_t)dir * g.dstride + s, p.inv_scale));
+      const double fi = double(Store<S>::val(F + fstar_index<Q>(g, p.mask, parity, x, y, z, i), p.inv_scale));
       const double wf = Lt::w(i) * fi;
       v[0] += wf;
       v[1] += Lt::c(i, 0) * wf;

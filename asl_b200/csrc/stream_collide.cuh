@@ -39,42 +39,55 @@ __device__ __forceinline__ void nb_offsets(const GridDesc& g, int x, int y, int 
   }
 }
 
+// Resident blocks of 256 threads per SM the register budget aims for: four
+// (64 registers) for the plain FP32/FP16 kernels, which must keep enough
+// loads in flight to saturate HBM; two for FP64 and the closures.
+template <class S, int CL>
+struct StepOccupancy {
+  static constexpr int blocks = (CL == CL_NONE && !std::is_same<S, double>::value) ? 4 : 2;
+};
+
 // ---------------------------------------------------------------------------
 // Stream + collide, one interior cell per thread. ODD: representation A -> B
 // (reads F[i][x - c_i], writes F[inv i][x + c_i]); EVEN: B -> A (reads
-// F[inv i][x], writes F[i][x]).
+// F[inv i][x], writes F[i][x]). Element indices are 32-bit (Q * dstride < 2^32).
 template <int Q, class S, int CL, bool ODD>
-__global__ void __launch_bounds__(256) k_stream_collide(S* __restrict__ F, const GridDesc g, const StepParams p,
-                                                        typename MacroT<S>::T* __restrict__ rho_out,
-                                                        typename MacroT<S>::T* __restrict__ u_out) {
+__global__ void __launch_bounds__(256, StepOccupancy<S, CL>::blocks)
+    k_stream_collide(S* __restrict__ F, const GridDesc g, const StepParams p,
+                     typename MacroT<S>::T* __restrict__ rho_out, typename MacroT<S>::T* __restrict__ u_out) {
   using Lt = Lattice<Q>;
   using C = typename Store<S>::C;
   const int z = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int x = blockIdx.z + 1;
   if (z > g.nz || y > g.ny) return;
-  const int s = (int)sidx(g, x, y, z);
-  uint32_t bb = 0;
+  const unsigned s = (unsigned)sidx(g, x, y, z);
+  const unsigned ds = (unsigned)g.dstride;
+  // Fused no-slip links: a fluid cell reads bounce-back populations, a solid
+  // cell skips the writes the condition would overwrite.
+  uint32_t bounce = 0, elide = 0;
   if (p.mask) {
-    bb = p.mask[s];
-    if (bb & kSolidBit) return;  // solid cell of a fused no-slip map: not advanced
+    const uint32_t m = p.mask[s];
+    if (m & kSolidBit)
+      elide = m;
+    else
+      bounce = m;
   }
   int ox[3], oy[3], oz[3];
   nb_offsets(g, x, y, z, ox, oy, oz);
   C f[Q];
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
-    // Pulled from the upstream neighbour, or, where that neighbour is a fused
-    // solid cell, bounced back from this cell's own outgoing population: the
-    // two slots swap roles between the representations.
-    const int up = s + ox[1 - Lt::c(i, 0)] + oy[1 - Lt::c(i, 1)] + oz[1 - Lt::c(i, 2)];
-    const bool b = (bb >> i) & 1u;
-    const S* src;
+    // Upstream neighbour slot, or for a bounce-back link this cell's own
+    // outgoing population: the two slots swap roles between representations.
+    const unsigned up = s + (unsigned)(ox[1 - Lt::c(i, 0)] + oy[1 - Lt::c(i, 1)] + oz[1 - Lt::c(i, 2)]);
+    const bool b = (bounce >> i) & 1u;
+    unsigned idx;
     if (ODD)
-      src = b ? F + (size_t)Lt::inv(i) * g.dstride + s : F + (size_t)i * g.dstride + up;
+      idx = b ? (unsigned)Lt::inv(i) * ds + s : (unsigned)i * ds + up;
     else
-      src = b ? F + (size_t)i * g.dstride + up : F + (size_t)Lt::inv(i) * g.dstride + s;
-    f[i] = Store<S>::load(src, p);
+      idx = b ? (unsigned)i * ds + up : (unsigned)Lt::inv(i) * ds + s;
+    f[i] = Store<S>::load(F + idx, p);
   }
   C rho, u[3];
   collide_cell<Q, C, CL>(f, p, rho, u);
@@ -89,13 +102,13 @@ __global__ void __launch_bounds__(256) k_stream_collide(S* __restrict__ F, const
   }
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
-    S* dst;
+    if ((elide >> i) & 1u) continue;
+    unsigned idx;
     if (ODD)
-      dst = F + (size_t)Lt::inv(i) * g.dstride +
-            (s + ox[1 + Lt::c(i, 0)] + oy[1 + Lt::c(i, 1)] + oz[1 + Lt::c(i, 2)]);
+      idx = (unsigned)Lt::inv(i) * ds + s + (unsigned)(ox[1 + Lt::c(i, 0)] + oy[1 + Lt::c(i, 1)] + oz[1 + Lt::c(i, 2)]);
     else
-      dst = F + (size_t)i * g.dstride + s;
-    Store<S>::store(dst, f[i], p);
+      idx = (unsigned)i * ds + s;
+    Store<S>::store(F + idx, f[i], p);
   }
 }
 

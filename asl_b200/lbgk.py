@@ -312,11 +312,10 @@ class BC:
         """Kernel launches per execute()."""
         return int(self.num.lib.aslb_bc_kernels(self.h))
 
-    def fuse(self, m: np.ndarray):
-        """Fold this no-slip map condition into the stream-collide kernel
-        (extension): solid cells are skipped, bounce-back happens inline."""
-        arr = _map_array(self.num, m)
-        L.check(self.num.lib.aslb_bc_fuse(self.h, arr.ctypes.data_as(L._pf)), "BCNoSlipMap::fuse")
+    def fuse(self):
+        """Fold this no-slip condition into the stream-collide kernel
+        (extension): bounce-back happens inline, results are unchanged."""
+        L.check(self.num.lib.aslb_bc_fuse(self.h), "BCNoSlip::fuse")
 
     @property
     def fused(self) -> bool:

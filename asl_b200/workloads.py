@@ -83,8 +83,9 @@ def porous_channel(size=(512, 256, 256), rmin=4.0, rmax=12.0, solid_fraction=0.4
 
 def build_lbgk(w: Workload, storage="f32", compVel=True, compRho=True, closure_cls=None, fuse=False):
     """Instantiate the workload on the GPU through the ASL-style API. With
-    ``fuse`` the no-slip map condition (last in every workload's order) is
-    folded into the stream-collide kernel."""
+    ``fuse`` the trailing no-slip conditions (walls and map, which every
+    workload lists after its other conditions) are folded into the
+    stream-collide kernel."""
     from . import lbgk as A
     vt = {15: A.d3q15(), 19: A.d3q19(), 27: A.d3q27()}[w.q]
     cls = closure_cls or A.LBGK
@@ -97,7 +98,10 @@ def build_lbgk(w: Workload, storage="f32", compVel=True, compRho=True, closure_c
     for s in w.bcs:
         walls = [getattr(A, n) for n in s.walls]
         if s.kind == "noslip":
-            bcs.append(A.generateBCNoSlip(lb, walls))
+            bc = A.generateBCNoSlip(lb, walls)
+            if fuse:
+                bc.fuse()
+            bcs.append(bc)
         elif s.kind == "velocity":
             bcs.append(A.generateBCConstantVelocity(lb, s.u, walls))
         elif s.kind == "pressure":
@@ -107,7 +111,7 @@ def build_lbgk(w: Workload, storage="f32", compVel=True, compRho=True, closure_c
         elif s.kind == "map_noslip":
             bc = A.generateBCNoSlip(lb, w.map)
             if fuse:
-                bc.fuse(w.map)
+                bc.fuse()
             bcs.append(bc)
         else:
             raise ValueError(s.kind)

@@ -176,15 +176,14 @@ int aslb_bc_slice_create(aslb_lbgk* h, int kind, unsigned wallmask, double p, co
  * generateBCConstantPressureVelocity(map) (src/num/aslLBGKBC.cxx:205-438). */
 int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const double u[3], const double omega[3],
                        const double center[3], aslb_bc** out);
-/* Extension (no ASL analogue): fold a no-slip map condition into the
- * stream-collide kernel. Solid cells of `map` (the same map the condition was
- * made from) are no longer advanced and fluid cells take bounce-back
- * populations inline; fluid results are bit-identical to the separate
- * condition, provided the fused condition is the last one to write its links
- * each step (later writers win in ASL). Rejects maps where a fluid cell
- * borders a solid cell at or below the -0.9999 guard. Solid-cell populations
- * are not meaningful afterwards. */
-int aslb_bc_fuse(aslb_bc* bc, const float* map);
+/* Extension (no ASL analogue): fold a no-slip condition (walls or map) into
+ * the stream-collide kernel, removing its separate launch. Fluid cells read
+ * bounce-back populations inline and solid cells skip the writes the
+ * condition would overwrite; every cell evolves exactly as with the separate
+ * condition (populations read back through aslb_lbgk_read are identical),
+ * provided no condition executed after it writes the same links (ASL: later
+ * writers win). aslb_lbgk_run enforces that fused conditions come last. */
+int aslb_bc_fuse(aslb_bc* bc);
 int aslb_bc_is_fused(aslb_bc* bc);
 /* BCond::execute() (src/num/aslLBGKBC.cxx:80-83, 257-260). */
 int aslb_bc_execute(aslb_bc* bc);

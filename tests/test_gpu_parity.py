@@ -258,31 +258,57 @@ def test_channel_cylinder_parity_1000_steps(gpu, oracle_mod):
 @pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
 @pytest.mark.parametrize("case", ["porous", "cylinder"])
 def test_fused_noslip_bitwise_equals_separate_condition(gpu, storage, case):
-    """Folding the no-slip map into the stream-collide kernel leaves every
-    fluid population, density, velocity and the surface force bit-identical."""
+    """Folding the no-slip conditions (walls and map) into the stream-collide
+    kernel leaves every population (solid and ghost cells included), the
+    density, velocity, mass and surface force bit-identical."""
     if case == "porous":
         w = W.porous_channel(size=(64, 32, 32), rmin=2.0, rmax=5.0, solid_fraction=0.35, steps=0)
     else:
         w = W.channel_cylinder(size=(48, 24, 20), radius=5.0, center=(14.0, 12.0), steps=0)
     a, abcs = W.build_lbgk(w, storage=storage)
     b, bbcs = W.build_lbgk(w, storage=storage, fuse=True)
-    assert bbcs[-1].fused and not abcs[-1].fused
-    fluid = w.map[1:-1, 1:-1, 1:-1] > 0
+    assert bbcs[-1].fused and bbcs[-2].fused and not abcs[-1].fused
+    assert sum(x.kernels for x in bbcs) < sum(x.kernels for x in abcs)
     for n in (13, 12):
         a.run(n, abcs)
         b.run(n, bbcs)
-        assert np.array_equal(a.getF()[I4][:, fluid], b.getF()[I4][:, fluid])
-        assert np.array_equal(a.getVelocity()[I4][:, fluid], b.getVelocity()[I4][:, fluid])
+        assert np.array_equal(a.getF(), b.getF(), equal_nan=True)
+        assert np.array_equal(a.getVelocity(), b.getVelocity())
+        assert np.array_equal(a.getRho(), b.getRho())
+        assert np.array_equal(a.moments(), b.moments())
         fa = A.generateComputeSurfaceForce(a, w.map).execute(r0=(1.0, 2.0, 3.0))
         fb = A.generateComputeSurfaceForce(b, w.map).execute(r0=(1.0, 2.0, 3.0))
         assert np.array_equal(fa, fb)
 
 
-def test_fuse_rejects_unguarded_map(gpu):
-    lb = A.LBGK(A.Block((12, 10, 8)), 0.1, A.d3q19())
-    g = lb.block.ghosted
+def test_fused_unnormalised_map_matches_oracle(gpu, oracle_mod):
+    """A raw (unnormalised) distance map leaves solid cells below the -0.9999
+    guard next to fluid; those links are not bounce-back and stream collided
+    solid populations, in fused mode exactly as in the oracle."""
+    size = (20, 14, 12)
+    g = tuple(s + 2 for s in size)
     pos = np.stack(np.meshgrid(*[np.arange(n) - 1.0 for n in g], indexing="ij"))
-    raw = (np.sqrt(((pos - 5.0) ** 2).sum(0)) - 3.0).astype(np.float32)  # not normalised: reaches -3
-    bc = A.generateBCNoSlip(lb, raw)
+    raw = (np.sqrt(((pos - np.array([8.0, 6.5, 5.5]).reshape(3, 1, 1, 1)) ** 2).sum(0)) - 3.5).astype(np.float32)
+    lb = A.LBGK(A.Block(size), 0.05, A.d3q19(), storage="f64")
+    A.LBGKUtilities(lb).initF((0.02, 0.0, 0.0))
+    bcs = [A.generateBCConstantVelocity(lb, (0.02, 0, 0), [A.X0]), A.generateBCConstantPressure(lb, 1.0, [A.XE]),
+           A.generateBCNoSlip(lb, [A.Y0, A.YE, A.Z0, A.ZE]), A.generateBCNoSlip(lb, raw)]
+    bcs[2].fuse()
+    bcs[3].fuse()
+    o = oracle_mod.Oracle(size, 19, 8, 0.05)
+    o.init_f(1.0, (0.02, 0, 0))
+    ids = [o.bc_slice(1, 1, 0, (0.02, 0, 0)), o.bc_slice(2, 2, 1.0), o.bc_slice(0, 4 | 8 | 16 | 32), o.bc_map(10, raw)]
+    lb.run(15, bcs)
+    for _ in range(15):
+        o.step(1)
+        for i in ids:
+            o.bc_execute(i)
+    assert np.abs(lb.getF()[I4] - o.get_f()[I4]).max() < 1e-12
+
+
+def test_fused_condition_must_come_last(gpu):
+    w = W.channel_cylinder(size=(24, 16, 12), radius=3.0, center=(8.0, 8.0), steps=0)
+    lb, bcs = W.build_lbgk(w)
+    bcs[-1].fuse()
     with pytest.raises(A.L.ASLError):
-        bc.fuse(raw)
+        lb.run(4, [bcs[-1]] + bcs[:-1])
