@@ -55,8 +55,12 @@ struct aslb_lbgk {
   long long graph_version = -1;
   long long version = 0;  // bumped by every parameter change
   // fused no-slip maps
-  std::vector<uint32_t> mask_host;
-  uint32_t* mask_dev = nullptr;
+  std::vector<uint2> mask_host;
+  uint2* mask_dev = nullptr;
+  // conditions and force objects made on this domain; destroying the domain
+  // releases their device memory and detaches them (any destruction order)
+  std::vector<aslb_bc*> bcs;
+  std::vector<aslb_force*> forces;
 };
 
 struct aslb_bc {
@@ -353,6 +357,28 @@ int aslb_lbgk_destroy(aslb_lbgk* h) {
   if (!h) return ASLB_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
   drop_graph(h);
+  for (aslb_bc* bc : h->bcs) {
+    cudaFree(bc->anchors);
+    cudaFree(bc->dlinks);
+    bc->anchors = nullptr;
+    bc->dlinks = nullptr;
+    bc->h = nullptr;
+  }
+  for (aslb_force* fc : h->forces) {
+    cudaFree(fc->cells);
+    cudaFree(fc->mask_in);
+    cudaFree(fc->field);
+    cudaFree(fc->partials);
+    cudaFree(fc->out);
+    if (fc->host_out) cudaFreeHost(fc->host_out);
+    fc->cells = nullptr;
+    fc->mask_in = nullptr;
+    fc->field = nullptr;
+    fc->partials = nullptr;
+    fc->out = nullptr;
+    fc->host_out = nullptr;
+    fc->h = nullptr;
+  }
   cudaFree(h->d.F);
   cudaFree(h->d.rho);
   cudaFree(h->d.u);
@@ -740,6 +766,7 @@ int aslb_bc_slice_create(aslb_lbgk* h, int kind, unsigned wallmask, double p, co
     aslb_bc_destroy(bc);
     return r;
   }
+  h->bcs.push_back(bc);
   *out = bc;
   return ASLB_OK;
 }
@@ -791,32 +818,28 @@ int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const
     aslb_bc_destroy(bc);
     return r;
   }
+  h->bcs.push_back(bc);
   *out = bc;
   return ASLB_OK;
 }
 
 int aslb_bc_fuse(aslb_bc* bc) {
   if (!bc) return fail(ASLB_ERR_ARG, "aslb_bc_fuse: null argument");
+  if (!bc->h) return fail(ASLB_ERR_STATE, "aslb_bc_fuse: its domain was destroyed");
   if (bc->bp.kind != ASLB_BC_MAP_NOSLIP && bc->bp.kind != ASLB_BC_NOSLIP)
     return fail(ASLB_ERR_ARG, "aslb_bc_fuse: only no-slip conditions can be fused");
   if (bc->fused) return ASLB_OK;
   aslb_lbgk* h = bc->h;
   const GridDesc& g = h->d.g;
   const int q = h->d.q;
-  std::vector<uint32_t> m = h->mask_host.empty() ? std::vector<uint32_t>((size_t)g.dstride, 0u) : h->mask_host;
+  std::vector<uint2> m = h->mask_host.empty() ? std::vector<uint2>((size_t)g.dstride, make_uint2(0u, 0u))
+                                               : h->mask_host;
   // Link (anchor a, direction k) enters fluid cell f = a + c_k: f reads it by
-  // bounce-back (bit k), and an interior anchor, which the stream-collide
-  // kernel advances, skips its write of direction k (bit k + solid bit).
-  auto add = [&](long long sa, bool anchor_interior, long long sf, int k) -> int {
-    if (m[sf] & kSolidBit)
-      return fail(ASLB_ERR_ARG, "aslb_bc_fuse: a cell is fluid for this condition and solid for a fused one");
-    m[sf] |= 1u << k;
-    if (anchor_interior) {
-      if (m[sa] && !(m[sa] & kSolidBit))
-        return fail(ASLB_ERR_ARG, "aslb_bc_fuse: a cell is solid for this condition and fluid for a fused one");
-      m[sa] |= kSolidBit | (1u << k);
-    }
-    return ASLB_OK;
+  // bounce-back (bounce bit k), and an interior anchor, which the
+  // stream-collide kernel advances, skips its write of direction k (elide bit k).
+  auto add = [&](long long sa, bool anchor_interior, long long sf, int k) {
+    m[sf].x |= 1u << k;
+    if (anchor_interior) m[sa].y |= 1u << k;
   };
   for (int k = 1; k < q; ++k)
     for (int t = bc->ls.seg[k]; t < bc->ls.seg[k + 1]; ++t) {
@@ -825,8 +848,7 @@ int aslb_bc_fuse(aslb_bc* bc) {
       const int z = int(local % g.pitch) - g.zoff;
       const int y = int((local / g.pitch) % g.gy);
       const int x = int(local / g.plane);
-      int r = add(sa, interior(g, x, y, z), sa + bc->ls.off[k], k);
-      if (r) return r;
+      add(sa, interior(g, x, y, z), sa + bc->ls.off[k], k);
     }
   for (const int4& an : bc->host_anchors)
     for (int k = 1; k < q; ++k) {
@@ -835,12 +857,11 @@ int aslb_bc_fuse(aslb_bc* bc) {
       const long long sa = sidx(g, ax, ay, az);
       const long long sf = sidx(g, wrapc(h, an.x + lattice_c(q, k, 0), 0), wrapc(h, an.y + lattice_c(q, k, 1), 1),
                                 wrapc(h, an.z + lattice_c(q, k, 2), 2));
-      int r = add(sa, interior(g, ax, ay, az), sf, k);
-      if (r) return r;
+      add(sa, interior(g, ax, ay, az), sf, k);
     }
-  if (!h->mask_dev) ASLB_CUDA(cudaMalloc((void**)&h->mask_dev, (size_t)g.dstride * sizeof(uint32_t)));
+  if (!h->mask_dev) ASLB_CUDA(cudaMalloc((void**)&h->mask_dev, (size_t)g.dstride * sizeof(uint2)));
   ASLB_CUDA(cudaStreamSynchronize(h->stream));
-  ASLB_CUDA(cudaMemcpy(h->mask_dev, m.data(), m.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  ASLB_CUDA(cudaMemcpy(h->mask_dev, m.data(), m.size() * sizeof(uint2), cudaMemcpyHostToDevice));
   h->mask_host.swap(m);
   h->p.mask = h->mask_dev;
   bc->fused = true;
@@ -853,6 +874,7 @@ int aslb_bc_is_fused(aslb_bc* bc) { return bc && bc->fused ? 1 : 0; }
 
 int aslb_bc_execute(aslb_bc* bc) {
   if (!bc) return fail(ASLB_ERR_ARG, "aslb_bc_execute: null handle");
+  if (!bc->h) return fail(ASLB_ERR_STATE, "aslb_bc_execute: its domain was destroyed");
   return do_bc(bc);
 }
 
@@ -861,6 +883,8 @@ int aslb_bc_destroy(aslb_bc* bc) {
   if (bc->h) {
     cudaStreamSynchronize(bc->h->stream);
     drop_graph(bc->h);
+    auto& v = bc->h->bcs;
+    v.erase(std::remove(v.begin(), v.end(), bc), v.end());
   }
   cudaFree(bc->anchors);
   cudaFree(bc->dlinks);
@@ -924,12 +948,14 @@ int aslb_force_create(aslb_lbgk* h, const float* map, aslb_force** out) {
     aslb_force_destroy(fc);
     return fail(ASLB_ERR_CUDA, std::string("aslb_force_create: ") + cudaGetErrorString(e));
   }
+  h->forces.push_back(fc);
   *out = fc;
   return ASLB_OK;
 }
 
 int aslb_force_compute(aslb_force* fc, const double r0[3], float* field_host, double out6[6]) {
   if (!fc || !out6) return fail(ASLB_ERR_ARG, "aslb_force_compute: null argument");
+  if (!fc->h) return fail(ASLB_ERR_STATE, "aslb_force_compute: its domain was destroyed");
   aslb_lbgk* h = fc->h;
   const double zero[3] = {0, 0, 0};
   cudaError_t e = launch_force(h->d, fc->cells, fc->mask_in, fc->n, fc->field, r0 ? r0 : zero, h->pos0, h->dx,
@@ -947,7 +973,11 @@ int aslb_force_compute(aslb_force* fc, const double r0[3], float* field_host, do
 
 int aslb_force_destroy(aslb_force* fc) {
   if (!fc) return ASLB_OK;
-  if (fc->h) cudaStreamSynchronize(fc->h->stream);
+  if (fc->h) {
+    cudaStreamSynchronize(fc->h->stream);
+    auto& v = fc->h->forces;
+    v.erase(std::remove(v.begin(), v.end(), fc), v.end());
+  }
   cudaFree(fc->cells);
   cudaFree(fc->mask_in);
   cudaFree(fc->field);

@@ -64,15 +64,13 @@ struct StepParams {
   int write_rho, write_vel;
   float scale, inv_scale;  // FP16 storage: d = (f - 1) * scale
   const void* mlp;         // closure network (device), CL == 3
-  // Fused no-slip conditions (null when none), one word per storage cell.
-  // Fluid cell: bit k = population k enters through a no-slip link, so it is
-  // read by bounce-back from this cell's own outgoing population. Solid cell
-  // (bit 31 set): bit k = its outgoing population k lands in such a link's
-  // incoming slot, which the condition overwrites, so the write is skipped.
-  const uint32_t* mask;
+  // Fused no-slip conditions (null when none), two words per storage cell.
+  // x (bounce): bit k = population k enters this cell through a fused link,
+  // so it is read by bounce-back from the cell's own outgoing population.
+  // y (elide): bit k = the cell's outgoing population k lands in the incoming
+  // slot of a fused link, which the condition would overwrite: not written.
+  const uint2* mask;
 };
-
-constexpr uint32_t kSolidBit = 0x80000000u;
 
 // ---- storage formats -------------------------------------------------------
 template <class S>

@@ -43,7 +43,7 @@ cudaError_t launch_step(const DomainDev& d, const StepParams& p, int closure, in
 // outgoing population, held by the other slot of the pair. Returns -1 where
 // representation B would need a cell outside the block (ghost cells only).
 template <int Q>
-__device__ __forceinline__ long long fstar_index(const GridDesc& g, const uint32_t* __restrict__ mask, int parity,
+__device__ __forceinline__ long long fstar_index(const GridDesc& g, const uint2* __restrict__ mask, int parity,
                                                  int x, int y, int z, int i) {
   using Lt = Lattice<Q>;
   const bool inter = x >= 1 && x <= g.nx && y >= 1 && y <= g.ny && z >= 1 && z <= g.nz;
@@ -59,8 +59,7 @@ __device__ __forceinline__ long long fstar_index(const GridDesc& g, const uint32
   const long long sq = tin ? sidx(g, tx, ty, tz) : -1;
   bool fused = false;
   if (mask && tin && tx >= 1 && tx <= g.nx && ty >= 1 && ty <= g.ny && tz >= 1 && tz <= g.nz) {
-    const uint32_t m = mask[sq];
-    fused = !(m & kSolidBit) && ((m >> i) & 1u);
+    fused = (mask[sq].x >> i) & 1u;
   }
   const bool in_own = (parity == 0) != fused;  // slot F[i][x] (else F[inv i][x + c_i])
   if (in_own) return (long long)i * g.dstride + sx;
@@ -391,7 +390,7 @@ __global__ void __launch_bounds__(kForceThreads)
     k_force(const S* __restrict__ F, const GridDesc g, const int4* __restrict__ cells,
             const uint32_t* __restrict__ mask_in, int n, float* __restrict__ field, double r00, double r01,
             double r02, double p00, double p01, double p02, double dx, float inv_scale,
-            const uint32_t* __restrict__ fused, int parity, double* __restrict__ partials) {
+            const uint2* __restrict__ fused, int parity, double* __restrict__ partials) {
   using Lt = Lattice<Q>;
   using C = typename Store<S>::C;
   constexpr bool kDev = std::is_same<S, __half>::value;
@@ -416,10 +415,7 @@ __global__ void __launch_bounds__(kForceThreads)
       // fluid end carries the link's bit (direction k into q for mask0 links,
       // direction inv(k) into the anchor for mask_in links).
       bool solid_fused = false;
-      if (fused) {
-        const uint32_t mf = b0 ? fused[sq] : fused[sa];
-        solid_fused = !(mf & kSolidBit) && ((mf >> (b0 ? k : Lt::inv(k))) & 1u);
-      }
+      if (fused) solid_fused = ((b0 ? fused[sq].x : fused[sa].x) >> (b0 ? k : Lt::inv(k))) & 1u;
       C a;
       if (solid_fused) {
         // outgoing slot of the fluid end: the anchor's neighbour q for mask0
@@ -482,7 +478,7 @@ cudaError_t launch_reduce_rows(const double* partials, int nblocks, int width, d
 template <int Q, class S>
 static cudaError_t force_impl(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,
                               const double* r0, const double* pos0, double dx, float inv_scale,
-                              const uint32_t* fused, int parity, double* partials, double* out6, cudaStream_t st) {
+                              const uint2* fused, int parity, double* partials, double* out6, cudaStream_t st) {
   const int nb = force_blocks(n);
   k_force<Q, S><<<nb, kForceThreads, 0, st>>>((const S*)d.F, d.g, cells, mask_in, n, field, r0[0], r0[1], r0[2],
                                               pos0[0], pos0[1], pos0[2], dx, inv_scale, fused, parity, partials);
@@ -492,7 +488,7 @@ static cudaError_t force_impl(const DomainDev& d, const int4* cells, const uint3
 }
 
 cudaError_t launch_force(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,
-                         const double* r0, const double* pos0, double dx, float inv_scale, const uint32_t* fused,
+                         const double* r0, const double* pos0, double dx, float inv_scale, const uint2* fused,
                          int parity, double* partials, double* out6, cudaStream_t st) {
   ASLB_DISPATCH(d, force_impl, d, cells, mask_in, n, field, r0, pos0, dx, inv_scale, fused, parity, partials, out6, st)
 }

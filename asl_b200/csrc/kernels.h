@@ -42,7 +42,7 @@ cudaError_t launch_bc_links(const DomainDev& d, const int* links, int n, const L
 // partial sums of (F, (r - r0) x F), then a fixed-order final sum into out6.
 int force_blocks(int n);
 cudaError_t launch_force(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,
-                         const double* r0, const double* pos0, double dx, float inv_scale, const uint32_t* fused,
+                         const double* r0, const double* pos0, double dx, float inv_scale, const uint2* fused,
                          int parity, double* partials, double* out6, cudaStream_t st);
 // Global diagnostics over interior cells (fluid cells in fused mode): (mass,
 // momentum x, y, z) in FP64.

@@ -67,11 +67,9 @@ __global__ void __launch_bounds__(256, StepOccupancy<S, CL>::blocks)
   // cell skips the writes the condition would overwrite.
   uint32_t bounce = 0, elide = 0;
   if (p.mask) {
-    const uint32_t m = p.mask[s];
-    if (m & kSolidBit)
-      elide = m;
-    else
-      bounce = m;
+    const uint2 m = p.mask[s];
+    bounce = m.x;
+    elide = m.y;
   }
   int ox[3], oy[3], oz[3];
   nb_offsets(g, x, y, z, ox, oy, oz);

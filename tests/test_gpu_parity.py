@@ -312,3 +312,18 @@ def test_fused_condition_must_come_last(gpu):
     bcs[-1].fuse()
     with pytest.raises(A.L.ASLError):
         lb.run(4, [bcs[-1]] + bcs[:-1])
+
+
+def test_destroy_domain_before_its_conditions(gpu):
+    """Destroying a domain detaches its conditions and force objects, which
+    may then be destroyed in any order (Python's collector picks one)."""
+    w = W.channel_cylinder(size=(24, 16, 12), radius=3.0, center=(8.0, 8.0), steps=0)
+    lb, bcs = W.build_lbgk(w)
+    force = A.generateComputeSurfaceForce(lb, w.map)
+    lb.run(3, bcs)
+    lb.close()
+    with pytest.raises(A.L.ASLError):
+        bcs[0].execute()
+    with pytest.raises(A.L.ASLError):
+        force.execute()
+    del bcs, force
