@@ -58,6 +58,8 @@ PROTOTYPES = {
     "aslb_lbgk_step": (C.c_int, [_vp, C.c_int]),
     "aslb_lbgk_run": (C.c_int, [_vp, C.c_int, C.POINTER(_vp), C.c_int, C.c_int]),
     "aslb_lbgk_sync": (C.c_int, [_vp]),
+    "aslb_lbgk_set_kernel": (C.c_int, [_vp, C.c_int]),
+    "aslb_lbgk_get_kernel": (C.c_int, [_vp]),
     "aslb_lbgk_steps": (C.c_longlong, [_vp]),
     "aslb_lbgk_read": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "aslb_lbgk_write": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),

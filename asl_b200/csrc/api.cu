@@ -48,6 +48,7 @@ struct aslb_lbgk {
   double* red_partials = nullptr;  // moments scratch
   double* red_out = nullptr;
   double* host_out = nullptr;      // pinned
+  int* host_err = nullptr;         // pinned copy of the device error word
   // time-loop graph cache
   cudaGraphExec_t graph = nullptr;
   std::vector<aslb_bc*> graph_bcs;
@@ -324,12 +325,16 @@ int aslb_lbgk_create(int nx, int ny, int nz, int q, int storage, double nu, unsi
   h->p.scale = 1024.0f;
   h->p.inv_scale = 1.0f / 1024.0f;
   h->p.cs = 0.17;
-  const size_t fbytes = (size_t)q * g.dstride * storage_bytes(storage);
+  // slack after the last direction: staged copies of a row segment may read a
+  // little past the end of the final row
+  const size_t fbytes = ((size_t)q * g.dstride + 4096) * storage_bytes(storage);
   const size_t mb = macro_bytes(storage);
   cudaError_t e = cudaMalloc(&h->d.F, fbytes);
   if (e == cudaSuccess) e = cudaMalloc(&h->d.rho, (size_t)g.L * mb);
   if (e == cudaSuccess) e = cudaMalloc(&h->d.u, 3 * (size_t)g.L * mb);
   if (e == cudaSuccess) e = cudaMalloc((void**)&h->red_out, 8 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&h->d.err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&h->host_err, sizeof(int));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&h->host_out, 8 * sizeof(double));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
@@ -338,7 +343,9 @@ int aslb_lbgk_create(int nx, int ny, int nz, int q, int storage, double nu, unsi
     return fail(e == cudaErrorMemoryAllocation ? ASLB_ERR_NOMEM : ASLB_ERR_CUDA, msg);
   }
   h->stream = h->own_stream;
+  h->d.variant = 1;  // TMA-staged stream-collide by default
   e = cudaMemsetAsync(h->d.F, 0, fbytes, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->d.err, 0, sizeof(int), h->stream);
   if (e == cudaSuccess) {
     const double u0[3] = {0, 0, 0};
     e = launch_init_f(h->d, h->p, 1.0, u0, nullptr, nullptr, h->stream);
@@ -386,7 +393,9 @@ int aslb_lbgk_destroy(aslb_lbgk* h) {
   cudaFree(h->mask_dev);
   cudaFree(h->red_partials);
   cudaFree(h->red_out);
+  cudaFree(h->d.err);
   if (h->host_out) cudaFreeHost(h->host_out);
+  if (h->host_err) cudaFreeHost(h->host_err);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
   return ASLB_OK;
@@ -612,9 +621,22 @@ int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int us
 
 int aslb_lbgk_sync(aslb_lbgk* h) {
   ASLB_CHECK_HANDLE(h);
+  ASLB_CUDA(cudaMemcpyAsync(h->host_err, h->d.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   ASLB_CUDA(cudaStreamSynchronize(h->stream));
+  if (*h->host_err)
+    return fail(ASLB_ERR_STATE, "aslb_lbgk_sync: a bounded device wait gave up (asynchronous copy never completed)");
   return ASLB_OK;
 }
+
+int aslb_lbgk_set_kernel(aslb_lbgk* h, int variant) {
+  ASLB_CHECK_HANDLE(h);
+  if (variant != 0 && variant != 1) return fail(ASLB_ERR_ARG, "aslb_lbgk_set_kernel: variant must be 0 or 1");
+  h->d.variant = variant;
+  h->version++;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_get_kernel(aslb_lbgk* h) { return h ? h->d.variant : -1; }
 
 long long aslb_lbgk_steps(aslb_lbgk* h) { return h ? h->steps : -1; }
 
@@ -859,7 +881,7 @@ int aslb_bc_fuse(aslb_bc* bc) {
                                 wrapc(h, an.z + lattice_c(q, k, 2), 2));
       add(sa, interior(g, ax, ay, az), sf, k);
     }
-  if (!h->mask_dev) ASLB_CUDA(cudaMalloc((void**)&h->mask_dev, (size_t)g.dstride * sizeof(uint2)));
+  if (!h->mask_dev) ASLB_CUDA(cudaMalloc((void**)&h->mask_dev, ((size_t)g.dstride + 4096) * sizeof(uint2)));
   ASLB_CUDA(cudaStreamSynchronize(h->stream));
   ASLB_CUDA(cudaMemcpy(h->mask_dev, m.data(), m.size() * sizeof(uint2), cudaMemcpyHostToDevice));
   h->mask_host.swap(m);

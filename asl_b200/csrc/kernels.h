@@ -15,6 +15,8 @@ struct DomainDev {
   void* F;     // populations (Q direction arrays)
   void* rho;   // density, ASL ghosted layout (float, or double for ST_F64)
   void* u;     // velocity, 3 components of L each
+  int variant; // stream-collide kernel: 0 plain, 1 TMA-staged
+  int* err;    // device error word (bounded waits that gave up)
 };
 
 inline size_t storage_bytes(int st) { return st == ST_F16 ? 2 : (st == ST_F64 ? 8 : 4); }

@@ -118,8 +118,13 @@ inline void step_launch_shape(const GridDesc& g, dim3& grid, dim3& block) {
   grid = dim3((g.nz + tz - 1) / tz, (g.ny + ty - 1) / ty, g.nx);
 }
 
+// Launch of the TMA-staged variant (stream_collide_tma.cuh).
+template <int Q, class S, int CL>
+cudaError_t step_tma(const DomainDev& d, const StepParams& p, int parity_in, cudaStream_t st);
+
 template <int Q, class S, int CL>
 cudaError_t step_q_s_cl(const DomainDev& d, const StepParams& p, int parity_in, cudaStream_t st) {
+  if (d.variant == 1) return step_tma<Q, S, CL>(d, p, parity_in, st);
   dim3 grid, block;
   step_launch_shape(d.g, grid, block);
   using M = typename MacroT<S>::T;

@@ -166,6 +166,14 @@ class LBGK:
     def sync(self):
         L.check(self.lib.aslb_lbgk_sync(self.h), "LBGK::sync")
 
+    def setKernel(self, variant: int):
+        """1: TMA-staged persistent stream-collide (default), 0: direct loads."""
+        L.check(self.lib.aslb_lbgk_set_kernel(self.h, int(variant)), "LBGK::setKernel")
+
+    @property
+    def kernel(self) -> int:
+        return int(self.lib.aslb_lbgk_get_kernel(self.h))
+
     @property
     def steps(self) -> int:
         return int(self.lib.aslb_lbgk_steps(self.h))

@@ -146,8 +146,15 @@ int aslb_lbgk_step(aslb_lbgk* h, int nsteps);
  * (examples/flow/flow.cc:124-134) as one call. use_graph != 0 records two
  * steps into a CUDA graph once and replays it. */
 int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int use_graph);
-/* Wait for all work of the domain. */
+/* Wait for all work of the domain; fails with ASLB_ERR_STATE if a kernel's
+ * bounded wait gave up. */
 int aslb_lbgk_sync(aslb_lbgk* h);
+/* Stream-collide kernel variant: 1 (default) stages every tile's population
+ * rows in shared memory with asynchronous bulk copies (TMA) in a persistent,
+ * pipelined kernel; 0 is the one-cell-per-thread kernel with direct loads.
+ * Both give identical results. */
+int aslb_lbgk_set_kernel(aslb_lbgk* h, int variant);
+int aslb_lbgk_get_kernel(aslb_lbgk* h);
 /* Steps taken so far. */
 long long aslb_lbgk_steps(aslb_lbgk* h);
 

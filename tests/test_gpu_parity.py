@@ -327,3 +327,39 @@ def test_destroy_domain_before_its_conditions(gpu):
     with pytest.raises(A.L.ASLError):
         force.execute()
     del bcs, force
+
+
+@pytest.mark.parametrize("q", [15, 19, 27])
+@pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
+@pytest.mark.parametrize("shape,periodic", [((6, 5, 300), (True, True, True)),    # two z segments, z wrap
+                                            ((9, 7, 40), (False, True, True)),    # 4 rows per tile, partial group
+                                            ((5, 3, 17), (True, False, False))])  # short rows
+def test_tma_kernel_bitwise_equals_direct_kernel(gpu, q, storage, shape, periodic):
+    g = tuple(s + 2 for s in shape)
+    rho, u = smooth_field(g, 3 + q)
+    lbs = []
+    for variant in (0, 1):
+        lb = A.LBGK(A.Block(shape), 0.03, VT[q], storage=storage, periodic=periodic, body_force=(1e-4, 0, 0))
+        lb.setKernel(variant)
+        A.LBGKUtilities(lb).initF(rho, u)
+        walls = [w for a, w in ((0, (A.X0, A.XE)), (1, (A.Y0, A.YE)), (2, (A.Z0, A.ZE))) if not periodic[a] for w in w]
+        bcs = [A.generateBCNoSlip(lb, walls)] if walls else []
+        lbs.append((lb, bcs))
+    for lb, bcs in lbs:
+        lb.run(7, bcs)
+        lb.sync()
+    assert lbs[1][0].kernel == 1 and lbs[0][0].kernel == 0
+    assert np.array_equal(lbs[0][0].getF(), lbs[1][0].getF(), equal_nan=True)
+    assert np.array_equal(lbs[0][0].getVelocity(), lbs[1][0].getVelocity())
+
+
+def test_tma_kernel_fused_porous_bitwise(gpu):
+    w = W.porous_channel(size=(80, 40, 36), rmin=2.0, rmax=5.0, solid_fraction=0.35, steps=0)
+    out = []
+    for variant in (0, 1):
+        lb, bcs = W.build_lbgk(w, fuse=True)
+        lb.setKernel(variant)
+        lb.run(9, bcs)
+        lb.sync()
+        out.append(lb.getF())
+    assert np.array_equal(out[0], out[1], equal_nan=True)
