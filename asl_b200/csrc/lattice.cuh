@@ -35,6 +35,10 @@ struct Lattice {
                      : (norm2(i) == 0 ? 8. / 27.
                                       : (norm2(i) == 1 ? 2. / 27. : (norm2(i) == 2 ? 1. / 54. : 1. / 216.)));
   }
+  // Runtime-index lookups (device code whose loop the compiler does not
+  // unroll) read the constant-memory tables below.
+  __device__ static int c_rt(int i, int d);
+  __device__ static int inv_rt(int i);
   // Opposite direction (ASL's invertVectors).
   __host__ __device__ static constexpr int inv(int i) {
     int r = 0;
@@ -43,6 +47,30 @@ struct Lattice {
     return r;
   }
 };
+
+// Constant-memory copies of the velocity sets for runtime indexing in device
+// code: [lattice: 0 = D3Q15, 1 = D3Q19/D3Q27 order][direction][axis], and the
+// opposite-direction tables.
+static __constant__ int kLatC[2][27][3] = {
+    {{0, 0, 0},  {1, 0, 0},  {0, 1, 0},   {0, 0, 1},   {-1, 0, 0}, {0, -1, 0}, {0, 0, -1}, {1, 1, 1},   {1, 1, -1},
+     {1, -1, 1}, {1, -1, -1}, {-1, 1, 1}, {-1, 1, -1}, {-1, -1, 1}, {-1, -1, -1}},
+    {{0, 0, 0},  {1, 0, 0},   {0, 1, 0},   {0, 0, 1},   {-1, 0, 0},  {0, -1, 0},  {0, 0, -1},
+     {1, 1, 0},  {1, -1, 0},  {-1, -1, 0}, {-1, 1, 0},  {0, 1, 1},   {0, 1, -1},  {0, -1, -1},
+     {0, -1, 1}, {1, 0, 1},   {1, 0, -1},  {-1, 0, -1}, {-1, 0, 1},  {1, 1, 1},   {1, 1, -1},
+     {1, -1, 1}, {1, -1, -1}, {-1, 1, 1},  {-1, 1, -1}, {-1, -1, 1}, {-1, -1, -1}}};
+static __constant__ int kLatInv[3][27] = {
+    {0, 4, 5, 6, 1, 2, 3, 14, 13, 12, 11, 10, 9, 8, 7},
+    {0, 4, 5, 6, 1, 2, 3, 9, 10, 7, 8, 13, 14, 11, 12, 17, 18, 15, 16},
+    {0, 4, 5, 6, 1, 2, 3, 9, 10, 7, 8, 13, 14, 11, 12, 17, 18, 15, 16, 26, 25, 24, 23, 22, 21, 20, 19}};
+
+template <int Q>
+__device__ inline int Lattice<Q>::c_rt(int i, int d) {
+  return kLatC[Q == 15 ? 0 : 1][i][d];
+}
+template <int Q>
+__device__ inline int Lattice<Q>::inv_rt(int i) {
+  return kLatInv[Q == 15 ? 0 : (Q == 19 ? 1 : 2)][i];
+}
 
 // Runtime lookups for host code and for kernels that loop over a bitmask.
 inline int lattice_c(int q, int i, int d) { return q == 15 ? lat_c15(i, d) : lat_c27(i, d); }

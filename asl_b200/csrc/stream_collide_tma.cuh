@@ -40,35 +40,40 @@ __device__ __forceinline__ uint2* stage_mask(unsigned char* smem, const TmaShape
   return reinterpret_cast<uint2*>(smem + (size_t)st * sh.stage_bytes + (size_t)sh.rows * q * sh.span * sizeof(S));
 }
 
-// Issue the copies of tile `tile` into stage `st` (one thread).
+// Issue the copies of tile `tile` into stage `st`: the 32 lanes of the
+// producer warp split the (row, direction) copies; lane 0 first arms the
+// stage's barrier with the transaction byte count.
 template <int Q, class S, bool ODD>
 __device__ __forceinline__ void tma_issue_tile(const S* F, const GridDesc& g, const StepParams& p,
                                                const TmaShape& sh, unsigned char* smem, uint64_t* bar, int st,
-                                               int tile) {
+                                               int tile, int lane) {
   using Lt = Lattice<Q>;
   const int rg = tile / sh.nseg, seg = tile % sh.nseg;
-  const int nrows_total = g.nx * g.ny;
   const int r0 = rg * sh.rows;
-  const int nr = min(sh.rows, nrows_total - r0);
+  const int nr = min(sh.rows, g.nx * g.ny - r0);
   const uint32_t row_bytes = (uint32_t)(sh.span * sizeof(S));
   const uint32_t mask_bytes = sh.fused ? (uint32_t)(sh.tz * sizeof(uint2)) : 0u;
-  mbar_arrive_expect_tx(bar, (uint32_t)nr * (Q * row_bytes + mask_bytes));
-  for (int r = 0; r < nr; ++r) {
+  if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)nr * (Q * row_bytes + mask_bytes));
+  __syncwarp();
+  const int per_row = Q + sh.fused;
+  for (int c = lane; c < nr * per_row; c += 32) {
+    const int r = c / per_row, i = c % per_row;
     const int row = r0 + r;
     const int x = row / g.ny + 1, y = row % g.ny + 1;
     const long long s0 = sidx(g, x, y, 1 + seg * sh.tz);
-    int ox[3], oy[3], oz[3];
-    nb_offsets(g, x, y, 2, ox, oy, oz);  // z = 2: no z wrap in the row offsets
-#pragma unroll
-    for (int i = 0; i < Q; ++i) {
-      long long src;
-      if (ODD)
-        src = (long long)i * g.dstride + s0 + ox[1 - Lt::c(i, 0)] + oy[1 - Lt::c(i, 1)] - sh.pad;
-      else
-        src = (long long)Lt::inv(i) * g.dstride + s0 - sh.pad;
-      bulk_g2s(stage_pop<S>(smem, sh, st, r, i, Q), F + src, row_bytes, bar);
+    if (i == Q) {
+      bulk_g2s(stage_mask<S>(smem, sh, st, Q) + (size_t)r * sh.tz, p.mask + s0, mask_bytes, bar);
+      continue;
     }
-    if (sh.fused) bulk_g2s(stage_mask<S>(smem, sh, st, Q) + (size_t)r * sh.tz, p.mask + s0, mask_bytes, bar);
+    long long src;
+    if (ODD) {
+      int ox[3], oy[3], oz[3];
+      nb_offsets(g, x, y, 2, ox, oy, oz);  // z = 2: no z wrap in the row offsets
+      src = (long long)i * g.dstride + s0 + ox[1 - Lt::c_rt(i, 0)] + oy[1 - Lt::c_rt(i, 1)] - sh.pad;
+    } else {
+      src = (long long)Lt::inv_rt(i) * g.dstride + s0 - sh.pad;
+    }
+    bulk_g2s(stage_pop<S>(smem, sh, st, r, i, Q), F + src, row_bytes, bar);
   }
 }
 
@@ -77,44 +82,67 @@ struct TmaOccupancy {
   static constexpr int blocks = (CL == CL_NONE && !std::is_same<S, double>::value) ? 3 : 2;
 };
 
+constexpr int kConsumerWarps = 8;
+constexpr int kTmaThreads = (kConsumerWarps + 1) * 32;
+
+// Warp-specialised persistent kernel: warps 0-7 compute one cell per thread,
+// warp 8 produces. full[st] completes when a stage's copies have landed;
+// empty[st] when all consumer warps have read it.
 template <int Q, class S, int CL, bool ODD>
-__global__ void __launch_bounds__(256, TmaOccupancy<S, CL>::blocks)
+__global__ void __launch_bounds__(kTmaThreads, TmaOccupancy<S, CL>::blocks)
     k_stream_collide_tma(S* __restrict__ F, const GridDesc g, const StepParams p,
                          typename MacroT<S>::T* __restrict__ rho_out, typename MacroT<S>::T* __restrict__ u_out,
                          const TmaShape sh, int* __restrict__ err) {
   using Lt = Lattice<Q>;
   using C = typename Store<S>::C;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bars[4];
+  __shared__ __align__(8) uint64_t full[4], empty[4];
   const int tid = threadIdx.x;
-  const int lr = tid / sh.tz, lz = tid % sh.tz;  // row within tile, cell within segment
+  const int warp = tid >> 5, lane = tid & 31;
   const unsigned ds = (unsigned)g.dstride;
 
   if (tid == 0) {
-    for (int st = 0; st < sh.stages; ++st) mbar_init(&bars[st], 1);
+    for (int st = 0; st < sh.stages; ++st) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], kConsumerWarps);
+    }
     fence_mbar_init();
   }
   __syncthreads();
-  // Copies issued / consumed per stage (thread 0), for the failure-path drain.
-  int issued[4] = {0, 0, 0, 0};
-  if (tid == 0) {
+
+  if (warp == kConsumerWarps) {
+    // ---- producer ----
     int k = 0;
-    for (int tile = blockIdx.x; tile < sh.ntiles && k < sh.stages; tile += gridDim.x, ++k) {
-      tma_issue_tile<Q, S, ODD>(F, g, p, sh, smem, &bars[k], k, tile);
-      issued[k] = 1;
+    for (int tile = blockIdx.x; tile < sh.ntiles; tile += gridDim.x, ++k) {
+      const int st = k % sh.stages;
+      if (k >= sh.stages) {
+        int ok = 1;
+        if (lane == 0) ok = mbar_wait(&empty[st], (uint32_t)(((k / sh.stages) - 1) & 1));
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) {
+          if (lane == 0) atomicExch(err, 1);
+          break;
+        }
+        fence_proxy_async_smem();
+      }
+      tma_issue_tile<Q, S, ODD>(F, g, p, sh, smem, &full[st], st, tile, lane);
     }
+    return;
   }
 
+  // ---- consumers ----
+  const int lr = tid / sh.tz, lz = tid % sh.tz;  // row within tile, cell within segment
   int k = 0;
   for (int tile = blockIdx.x; tile < sh.ntiles; tile += gridDim.x, ++k) {
     const int st = k % sh.stages;
-    const uint32_t phase = (uint32_t)((k / sh.stages) & 1);
-    const bool ok = mbar_wait(&bars[st], phase);
-
+    if (!mbar_wait(&full[st], (uint32_t)((k / sh.stages) & 1))) {
+      if (lane == 0) atomicExch(err, 1);
+      return;
+    }
     const int rg = tile / sh.nseg, seg = tile % sh.nseg;
     const int row = rg * sh.rows + lr;
     const int z = 1 + seg * sh.tz + lz;
-    const bool valid = ok && row < g.nx * g.ny && z <= g.nz;
+    const bool valid = row < g.nx * g.ny && z <= g.nz;
     const int x = valid ? row / g.ny + 1 : 1, y = valid ? row % g.ny + 1 : 1;
 
     C f[Q];
@@ -151,29 +179,8 @@ __global__ void __launch_bounds__(256, TmaOccupancy<S, CL>::blocks)
         }
       }
     }
-    // All reads of this stage are done (and a timeout anywhere stops everyone).
-    const int bad = __syncthreads_or(!ok);
-    if (bad) {
-      if (tid == 0) {
-        atomicExch(err, 1);
-        // Let copies still in flight land (bounded) before the CTA's shared
-        // memory is released: stage j has issued[j] copies, the first
-        // consumed[j] of which completed.
-        for (int j = 0; j < sh.stages; ++j) {
-          const int consumed = (k - j + sh.stages - 1) / sh.stages;
-          for (int c = consumed; c < issued[j]; ++c) mbar_wait(&bars[j], (uint32_t)(c & 1));
-        }
-      }
-      return;
-    }
-    if (tid == 0) {
-      const int next = tile + sh.stages * gridDim.x;
-      if (next < sh.ntiles) {
-        fence_proxy_async_smem();
-        tma_issue_tile<Q, S, ODD>(F, g, p, sh, smem, &bars[st], st, next);
-        issued[st] += 1;
-      }
-    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[st]);  // this warp is done with the stage
     if (!valid) continue;
 
     C rho, u[3];
@@ -242,11 +249,11 @@ cudaError_t step_tma(const DomainDev& d, const StepParams& p, int parity_in, cud
     configured[parity_in] = true;
   }
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTmaThreads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   const int grid = std::min(sh.ntiles, sm_count * per_sm);
-  kern<<<grid, 256, smem, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u, sh, d.err);
+  kern<<<grid, kTmaThreads, smem, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u, sh, d.err);
   return cudaGetLastError();
 }
 

@@ -281,29 +281,37 @@ def test_fused_noslip_bitwise_equals_separate_condition(gpu, storage, case):
         assert np.array_equal(fa, fb)
 
 
-def test_fused_unnormalised_map_matches_oracle(gpu, oracle_mod):
+@pytest.mark.parametrize("fuse", ["none", "walls", "map", "both"])
+@pytest.mark.parametrize("variant", [0, 1])
+def test_unnormalised_map_matches_oracle(gpu, oracle_mod, fuse, variant):
     """A raw (unnormalised) distance map leaves solid cells below the -0.9999
     guard next to fluid; those links are not bounce-back and stream collided
-    solid populations, in fused mode exactly as in the oracle."""
+    solid populations, with or without fusing, exactly as in the oracle."""
     size = (20, 14, 12)
     g = tuple(s + 2 for s in size)
     pos = np.stack(np.meshgrid(*[np.arange(n) - 1.0 for n in g], indexing="ij"))
     raw = (np.sqrt(((pos - np.array([8.0, 6.5, 5.5]).reshape(3, 1, 1, 1)) ** 2).sum(0)) - 3.5).astype(np.float32)
     lb = A.LBGK(A.Block(size), 0.05, A.d3q19(), storage="f64")
+    lb.setKernel(variant)
     A.LBGKUtilities(lb).initF((0.02, 0.0, 0.0))
     bcs = [A.generateBCConstantVelocity(lb, (0.02, 0, 0), [A.X0]), A.generateBCConstantPressure(lb, 1.0, [A.XE]),
            A.generateBCNoSlip(lb, [A.Y0, A.YE, A.Z0, A.ZE]), A.generateBCNoSlip(lb, raw)]
-    bcs[2].fuse()
-    bcs[3].fuse()
+    if fuse in ("walls", "both"):
+        bcs[2].fuse()
+    if fuse in ("map", "both"):
+        bcs[3].fuse()
+    if fuse == "walls":
+        bcs = bcs[:2] + [bcs[3], bcs[2]]  # fused conditions go last (both no-slip: order-free)
     o = oracle_mod.Oracle(size, 19, 8, 0.05)
     o.init_f(1.0, (0.02, 0, 0))
     ids = [o.bc_slice(1, 1, 0, (0.02, 0, 0)), o.bc_slice(2, 2, 1.0), o.bc_slice(0, 4 | 8 | 16 | 32), o.bc_map(10, raw)]
-    lb.run(15, bcs)
-    for _ in range(15):
+    for n in range(1, 16):
+        lb.run(1, bcs)
         o.step(1)
         for i in ids:
             o.bc_execute(i)
-    assert np.abs(lb.getF()[I4] - o.get_f()[I4]).max() < 1e-12
+        err = np.abs(lb.getF()[I4] - o.get_f()[I4]).max()
+        assert err < 1e-12, (n, err)
 
 
 def test_fused_condition_must_come_last(gpu):
