@@ -55,7 +55,11 @@ struct aslb_lbgk {
   int graph_parity = -1;
   long long graph_version = -1;
   long long version = 0;  // bumped by every parameter change
-  // fused no-slip maps
+  // fused no-slip conditions
+  // fresh: populations were (re)initialised and no fused condition has run
+  // since, so incoming slots still hold their initial values and the next
+  // step must read them as they are (no bounce-back, no skipped writes).
+  bool fresh = true;
   std::vector<uint2> mask_host;
   uint2* mask_dev = nullptr;
   // conditions and force objects made on this domain; destroying the domain
@@ -96,6 +100,7 @@ void prepare_params(aslb_lbgk* h) {
   h->p.write_vel = (h->comp_vel || h->macro_once) ? 1 : 0;
   h->p.write_macro = h->p.write_rho | h->p.write_vel;
   h->p.mlp = h->mlp_dev;
+  h->p.mask = h->fresh ? nullptr : h->mask_dev;
 }
 
 int do_step(aslb_lbgk* h) {
@@ -113,7 +118,14 @@ int do_step(aslb_lbgk* h) {
 
 int do_bc(aslb_bc* bc) {
   aslb_lbgk* h = bc->h;
-  if (bc->fused) return ASLB_OK;
+  if (bc->fused) {
+    // The condition takes effect inside the next steps (bounce-back reads).
+    if (h->fresh) {
+      h->fresh = false;
+      h->version++;
+    }
+    return ASLB_OK;
+  }
   cudaError_t e = cudaSuccess;
   if (bc->nd) e = launch_bc_links(h->d, bc->dlinks, bc->nd, bc->ls, bc->bp, h->parity, h->stream);
   if (e == cudaSuccess && bc->n) e = launch_bc(h->d, bc->anchors, bc->n, bc->bp, h->parity, h->stream);
@@ -517,6 +529,8 @@ int aslb_lbgk_init_f(aslb_lbgk* h, double rho, const double u[3]) {
   cudaError_t e = launch_init_f(h->d, h->p, rho, u ? u : z, nullptr, nullptr, h->stream);
   if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_init_f: ") + cudaGetErrorString(e));
   h->parity = 0;
+  h->fresh = true;
+  h->version++;
   return ASLB_OK;
 }
 
@@ -539,6 +553,8 @@ int aslb_lbgk_init_f_fields(aslb_lbgk* h, const double* rho, const double* u) {
   if (e != cudaSuccess || e2 != cudaSuccess)
     return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_init_f_fields: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
   h->parity = 0;
+  h->fresh = true;
+  h->version++;
   return ASLB_OK;
 }
 
@@ -575,7 +591,7 @@ int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int us
   };
   if (!use_graph || h->stream == nullptr || nsteps < 2) return eager(nsteps);
   int done = 0;
-  if (h->macro_once) {
+  if (h->macro_once || h->fresh) {
     int r = eager(1);
     if (r) return r;
     done = 1;
@@ -659,6 +675,7 @@ int aslb_lbgk_read(aslb_lbgk* h, int field, int dtype, void* host_out) {
     count = (size_t)h->d.q * L;
     ASLB_CUDA(cudaMalloc(&dev, count * mb));
     own = true;
+    prepare_params(h);
     cudaError_t e = launch_export_f(h->d, h->p, h->parity, dev, h->stream);
     if (e != cudaSuccess) {
       cudaFree(dev);
@@ -711,6 +728,8 @@ int aslb_lbgk_write(aslb_lbgk* h, int field, int dtype, const void* host_in) {
   cudaFree(dev);
   if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_write: ") + cudaGetErrorString(e));
   h->parity = 0;
+  h->fresh = true;
+  h->version++;
   return ASLB_OK;
 }
 
@@ -726,6 +745,7 @@ int aslb_lbgk_moments(aslb_lbgk* h, double out[4]) {
   if (!out) return fail(ASLB_ERR_ARG, "aslb_lbgk_moments: null output");
   const int nb = moments_blocks(h->d.g);
   if (!h->red_partials) ASLB_CUDA(cudaMalloc((void**)&h->red_partials, (size_t)nb * 4 * sizeof(double)));
+  prepare_params(h);
   cudaError_t e = launch_moments(h->d, h->p, h->parity, h->red_partials, h->red_out, h->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(h->host_out, h->red_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
@@ -885,7 +905,6 @@ int aslb_bc_fuse(aslb_bc* bc) {
   ASLB_CUDA(cudaStreamSynchronize(h->stream));
   ASLB_CUDA(cudaMemcpy(h->mask_dev, m.data(), m.size() * sizeof(uint2), cudaMemcpyHostToDevice));
   h->mask_host.swap(m);
-  h->p.mask = h->mask_dev;
   bc->fused = true;
   h->version++;
   drop_graph(h);
@@ -981,7 +1000,8 @@ int aslb_force_compute(aslb_force* fc, const double r0[3], float* field_host, do
   aslb_lbgk* h = fc->h;
   const double zero[3] = {0, 0, 0};
   cudaError_t e = launch_force(h->d, fc->cells, fc->mask_in, fc->n, fc->field, r0 ? r0 : zero, h->pos0, h->dx,
-                               h->p.inv_scale, h->mask_dev, h->parity, fc->partials, fc->out, h->stream);
+                               h->p.inv_scale, h->fresh ? nullptr : h->mask_dev, h->parity, fc->partials,
+                               fc->out, h->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(fc->host_out, fc->out, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess && field_host)

@@ -189,7 +189,10 @@ int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const
  * condition would overwrite; every cell evolves exactly as with the separate
  * condition (populations read back through aslb_lbgk_read are identical),
  * provided no condition executed after it writes the same links (ASL: later
- * writers win). aslb_lbgk_run enforces that fused conditions come last. */
+ * writers win). aslb_lbgk_run enforces that fused conditions come last.
+ * Like any condition it must be executed after every step (aslb_bc_execute
+ * or aslb_lbgk_run): after initF or a population write, the steps read the
+ * initial values until a fused condition has been executed, as in ASL. */
 int aslb_bc_fuse(aslb_bc* bc);
 int aslb_bc_is_fused(aslb_bc* bc);
 /* BCond::execute() (src/num/aslLBGKBC.cxx:80-83, 257-260). */
