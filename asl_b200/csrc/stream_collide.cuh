@@ -78,13 +78,16 @@ __global__ void __launch_bounds__(256, StepOccupancy<S, CL>::blocks)
   for (int i = 0; i < Q; ++i) {
     // Upstream neighbour slot, or for a bounce-back link this cell's own
     // outgoing population: the two slots swap roles between representations.
-    const unsigned up = s + (unsigned)(ox[1 - Lt::c(i, 0)] + oy[1 - Lt::c(i, 1)] + oz[1 - Lt::c(i, 2)]);
     const bool b = (bounce >> i) & 1u;
     unsigned idx;
-    if (ODD)
-      idx = b ? (unsigned)Lt::inv(i) * ds + s : (unsigned)i * ds + up;
-    else
-      idx = b ? (unsigned)i * ds + up : (unsigned)Lt::inv(i) * ds + s;
+    if (ODD) {
+      idx = b ? (unsigned)Lt::inv(i) * ds + s
+              : (unsigned)i * ds + s + (unsigned)(ox[1 - Lt::c(i, 0)] + oy[1 - Lt::c(i, 1)] + oz[1 - Lt::c(i, 2)]);
+    } else if (b) {
+      idx = (unsigned)i * ds + s + (unsigned)(ox[1 - Lt::c(i, 0)] + oy[1 - Lt::c(i, 1)] + oz[1 - Lt::c(i, 2)]);
+    } else {
+      idx = (unsigned)Lt::inv(i) * ds + s;
+    }
     f[i] = Store<S>::load(F + idx, p);
   }
   C rho, u[3];

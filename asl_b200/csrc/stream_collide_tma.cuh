@@ -8,9 +8,11 @@
 // memory (the AA pattern writes the same slots it read).
 //
 // Alignment: a row's first interior cell is 128-byte aligned and x/y
-// neighbour offsets are whole rows, so every copy starts on a 16-byte
-// boundary once it is widened by `pad` = 16 B of elements on both sides; the
-// +-1 z shift of a direction is absorbed by indexing inside the buffer.
+// neighbour offsets are whole rows, so every copy is exactly the 128-byte
+// aligned row segment (widening it to reach the +-1 z neighbours makes the
+// copy engine fetch whole extra lines for every row). A direction's +-1 z
+// shift is absorbed by indexing inside the buffer; the one lane per row whose
+// upstream cell falls outside the segment reads it from global memory.
 #pragma once
 #include "stream_collide.cuh"
 #include "tma.cuh"
@@ -24,8 +26,7 @@ struct TmaShape {
   int nseg;     // segments per row
   int ntiles;   // row groups * nseg
   int stages;   // pipeline depth
-  int pad;      // elements of 16 bytes
-  int span;     // tz + 2 * pad
+  int span;     // staged elements per row (= tz)
   int stage_bytes;
   int fused;    // masks staged too
 };
@@ -69,9 +70,9 @@ __device__ __forceinline__ void tma_issue_tile(const S* F, const GridDesc& g, co
     if (ODD) {
       int ox[3], oy[3], oz[3];
       nb_offsets(g, x, y, 2, ox, oy, oz);  // z = 2: no z wrap in the row offsets
-      src = (long long)i * g.dstride + s0 + ox[1 - Lt::c_rt(i, 0)] + oy[1 - Lt::c_rt(i, 1)] - sh.pad;
+      src = (long long)i * g.dstride + s0 + ox[1 - Lt::c_rt(i, 0)] + oy[1 - Lt::c_rt(i, 1)];
     } else {
-      src = (long long)Lt::inv_rt(i) * g.dstride + s0 - sh.pad;
+      src = (long long)Lt::inv_rt(i) * g.dstride + s0;
     }
     bulk_g2s(stage_pop<S>(smem, sh, st, r, i, Q), F + src, row_bytes, bar);
   }
@@ -167,15 +168,15 @@ __global__ void __launch_bounds__(kTmaThreads, TmaOccupancy<S, CL>::blocks)
           f[i] = Store<S>::load(F + idx, p);
         } else if (ODD) {
           // upstream cell z - c_z (wrapped on a periodic z axis) inside the staged row
-          const int pos = z + oz[1 - Lt::c(i, 2)] - (1 + seg * sh.tz) + sh.pad;
+          const int pos = z + oz[1 - Lt::c(i, 2)] - (1 + seg * sh.tz);
           if (pos >= 0 && pos < sh.span) {
             f[i] = Store<S>::load(stage_pop<S>(smem, sh, st, lr, i, Q) + pos, p);
-          } else {  // periodic wrap into another segment of a long row
+          } else {  // ghost z, or a periodic wrap into another segment of a long row
             const unsigned up = s + (unsigned)(ox[1 - Lt::c(i, 0)] + oy[1 - Lt::c(i, 1)] + oz[1 - Lt::c(i, 2)]);
             f[i] = Store<S>::load(F + (unsigned)i * ds + up, p);
           }
         } else {
-          f[i] = Store<S>::load(stage_pop<S>(smem, sh, st, lr, i, Q) + sh.pad + lz, p);
+          f[i] = Store<S>::load(stage_pop<S>(smem, sh, st, lr, i, Q) + lz, p);
         }
       }
     }
@@ -219,8 +220,7 @@ inline TmaShape tma_shape(const GridDesc& g, bool fused, int blocks_per_sm) {
   sh.nseg = (g.nz + tz - 1) / tz;
   const int rgroups = (g.nx * g.ny + sh.rows - 1) / sh.rows;
   sh.ntiles = rgroups * sh.nseg;
-  sh.pad = 16 / (int)sizeof(S);
-  sh.span = tz + 2 * sh.pad;
+  sh.span = tz;
   sh.fused = fused ? 1 : 0;
   int bytes = sh.rows * Q * sh.span * (int)sizeof(S) + (fused ? sh.rows * tz * (int)sizeof(uint2) : 0);
   sh.stage_bytes = ((bytes + 127) / 128) * 128;
