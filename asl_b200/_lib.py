@@ -76,6 +76,7 @@ PROTOTYPES = {
     "aslb_force_create": (C.c_int, [_vp, _pf, C.POINTER(_vp)]),
     "aslb_force_compute": (C.c_int, [_vp, _pd, _pf, _pd]),
     "aslb_force_destroy": (C.c_int, [_vp]),
+    "aslb_force_compute_noalloc": (C.c_int, [_vp, _pd, _pd]),
     "aslb_geom_pack_spheres": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                          C.c_ulonglong, C.c_int, C.c_int, C.c_int, _pd, _pd, C.POINTER(C.c_int)]),
 }

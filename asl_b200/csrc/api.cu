@@ -1030,4 +1030,60 @@ int aslb_force_destroy(aslb_force* fc) {
   return ASLB_OK;
 }
 
+// ---- surface force without any allocation ---------------------------------
+//
+// For callers that cannot allocate device memory at the moment they need a
+// force: code running inside a stream capture or under an allocator that
+// forbids new device allocations, or an embedding runtime that hands out all
+// memory up front. aslb_force_compute allocates nothing per call either, but
+// its scratch rows come from cudaMalloc at aslb_force_create; this variant
+// takes the per-block partial sums and the final sums from one fixed array in
+// the library's own device memory instead.
+
 }  // extern "C"
+
+namespace {
+// Up to kNoAllocForceBlocks blocks of 256 listed force cells (1,048,576
+// cells), six partial sums each, plus the six final sums: 196,672 bytes that
+// every device which loads the library keeps until the process exits.
+constexpr int kNoAllocForceBlocks = 4096;
+constexpr int kNoAllocForceCells = kNoAllocForceBlocks * 256;
+constexpr int kNoAllocScratch = kNoAllocForceBlocks * 6 + 8;
+static __device__ __align__(256) double g_force_scratch[kNoAllocScratch];
+// Device address of g_force_scratch per device (the name is only a host-side
+// stand-in in host code), looked up on the first call on each device.
+double* g_force_scratch_dev[64] = {nullptr};
+}  // namespace
+
+extern "C" int aslb_force_compute_noalloc(aslb_force* fc, const double r0[3], double out6[6]) {
+  if (!fc || !out6) return fail(ASLB_ERR_ARG, "aslb_force_compute_noalloc: null argument");
+  if (!fc->h) return fail(ASLB_ERR_STATE, "aslb_force_compute_noalloc: its domain was destroyed");
+  aslb_lbgk* h = fc->h;
+  if (force_blocks(fc->n) > kNoAllocForceBlocks)
+    return fail(ASLB_ERR_ARG, "aslb_force_compute_noalloc: " + std::to_string(fc->n) +
+                                  " force cells exceed the fixed scratch limit of " +
+                                  std::to_string(kNoAllocForceCells) + "; use aslb_force_compute");
+  int dev = -1;
+  ASLB_CUDA(cudaGetDevice(&dev));
+  if (dev != h->device)
+    return fail(ASLB_ERR_STATE, "aslb_force_compute_noalloc: make the domain's device current first");
+  if (dev < 0 || dev >= 64) return fail(ASLB_ERR_ARG, "aslb_force_compute_noalloc: device index out of range");
+  if (!g_force_scratch_dev[dev]) {
+    double* p = nullptr;
+    ASLB_CUDA(cudaGetSymbolAddress((void**)&p, g_force_scratch));
+    g_force_scratch_dev[dev] = p;
+  }
+  double* partials = g_force_scratch_dev[dev];
+  double* sums = partials + (size_t)kNoAllocForceBlocks * 6;
+  // Every block writes its whole row of partial sums and the final kernel
+  // overwrites the six sums, so nothing left by an earlier call is read.
+  const double zero[3] = {0, 0, 0};
+  cudaError_t e = launch_force(h->d, fc->cells, fc->mask_in, fc->n, nullptr, r0 ? r0 : zero, h->pos0, h->dx,
+                               h->p.inv_scale, h->fresh ? nullptr : h->mask_dev, h->parity, partials, sums,
+                               h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out6, sums, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess)
+    return fail(ASLB_ERR_CUDA, std::string("aslb_force_compute_noalloc: ") + cudaGetErrorString(e));
+  return ASLB_OK;
+}

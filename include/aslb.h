@@ -213,6 +213,17 @@ int aslb_force_create(aslb_lbgk* h, const float* map, aslb_force** out);
  * receives the per-cell force field. Synchronises. */
 int aslb_force_compute(aslb_force* fc, const double r0[3], float* field_host, double out6[6]);
 int aslb_force_destroy(aslb_force* fc);
+/* No counterpart in the reference. The same totals as aslb_force_compute
+ * (without the per-cell field) for callers that cannot allocate device memory
+ * when they need them, e.g. inside a stream capture or under an allocator
+ * that forbids new allocations: it calls no cudaMalloc or cudaFree and keeps
+ * its partial sums in a fixed array of the library's device memory (196,672
+ * bytes per device, held until exit). Lists of more than 1,048,576 force
+ * cells are rejected with ASLB_ERR_ARG. The domain's device must be current;
+ * the first call on each device looks up the array's address, so make that
+ * first call before any stream capture. All calls share the array: calls
+ * whose work overlaps on the GPU (different streams) race. Synchronises. */
+int aslb_force_compute_noalloc(aslb_force* fc, const double r0[3], double out6[6]);
 
 /* ---- workload geometry (host) ----------------------------------------- */
 
