@@ -7,10 +7,25 @@
 // plus the optional Coriolis term (component-sequential like ASL's generated
 // code), Guo forcing for a body force, and the closures that replace omega.
 #pragma once
+#include <type_traits>
 #include "internal.cuh"
 #include "mlp.cuh"
 
 namespace aslb {
+
+// c_i . v with the lattice vector known at compile time: only the nonzero
+// components are added (0 * v cannot be dropped by the compiler under IEEE
+// rules), the same value as the full dot product for finite v.
+template <int Q, class C>
+__device__ __forceinline__ C cdot(int i, C v0, C v1, C v2) {
+  using Lt = Lattice<Q>;
+  C r = C(0);
+  bool first = true;
+  if (Lt::c(i, 0)) { r = Lt::c(i, 0) > 0 ? v0 : -v0; first = false; }
+  if (Lt::c(i, 1)) { r = first ? (Lt::c(i, 1) > 0 ? v1 : -v1) : (Lt::c(i, 1) > 0 ? r + v1 : r - v1); first = false; }
+  if (Lt::c(i, 2)) { r = first ? (Lt::c(i, 2) > 0 ? v2 : -v2) : (Lt::c(i, 2) > 0 ? r + v2 : r - v2); }
+  return r;
+}
 
 template <int Q, class C, int CL>
 __device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, C& rho_out, C (&u_out)[3]) {
@@ -27,7 +42,8 @@ __device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, C& 
     if (Lt::c(i, 2) > 0) m2 += wf;
     if (Lt::c(i, 2) < 0) m2 -= wf;
   }
-  const C om0 = C(1) / (C(3) * C(p.nu) + C(0.5));
+  // omega = 1 / (3 nu + 1/2), evaluated on the host in the storage's arithmetic
+  const C om0 = std::is_same<C, double>::value ? C(p.om0d) : C(p.om0f);
   C om = om0;
   if (p.has_coriolis) {
     const C k = C(2) / om;
@@ -62,7 +78,7 @@ __device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, C& 
     C P00 = C(0), P11 = C(0), P22 = C(0), P01 = C(0), P12 = C(0), P02 = C(0);
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-      const C cm = C(Lt::c(i, 0)) * m0 + C(Lt::c(i, 1)) * m1 + C(Lt::c(i, 2)) * m2;
+      const C cm = cdot<Q, C>(i, m0, m1, m2);
       const C feq = a0 + C(3) * cm + a2 * (cm * cm);
       const C d = f[i] - feq;
       if (CL == CL_ASL_INTENT) {
@@ -98,28 +114,31 @@ __device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, C& 
     }
   }
 
+  // Relaxation folded into three multiply-adds per direction:
+  //   (1 - om) f + om f_eq = (1 - om) f + om a0 + cm (3 om + om a2 cm)
   const C one_m = C(1) - om;
-  C fx = C(0), fy = C(0), fz = C(0), ux = C(0), uy = C(0), uz = C(0), cgu = C(0), half_src = C(0);
+  const C oa0 = om * a0, o3 = C(3) * om, oa2 = om * a2;
+  // Guo source (1 - om/2) rho [3 (c - u).g + 9 (c.u)(c.g)] with u = m / rho:
+  //   hs3 c.g + hs9 (c.m / rho)(c.g) - hs3 u.g
+  C gx = C(0), gy = C(0), gz = C(0), hs3 = C(0), hs9 = C(0), sA = C(0);
   if (p.has_force) {
-    fx = C(p.g[0]);
-    fy = C(p.g[1]);
-    fz = C(p.g[2]);
-    ux = m0 * inv_rho;
-    uy = m1 * inv_rho;
-    uz = m2 * inv_rho;
-    cgu = ux * fx + uy * fy + uz * fz;
-    half_src = (C(1) - C(0.5) * om) * rho;
+    gx = C(p.g[0]);
+    gy = C(p.g[1]);
+    gz = C(p.g[2]);
+    const C hs = (C(1) - C(0.5) * om) * rho;
+    hs3 = C(3) * hs;
+    hs9 = C(9) * hs * inv_rho;
+    sA = -hs3 * ((m0 * gx + m1 * gy + m2 * gz) * inv_rho);
   }
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
-    const C cm = C(Lt::c(i, 0)) * m0 + C(Lt::c(i, 1)) * m1 + C(Lt::c(i, 2)) * m2;
-    const C feq = a0 + C(3) * cm + a2 * (cm * cm);
-    C fn = f[i] * one_m + om * feq;
+    const C cm = cdot<Q, C>(i, m0, m1, m2);
+    C t = oa2 * cm + o3;
+    t = t * cm + oa0;
+    C fn = one_m * f[i] + t;
     if (p.has_force) {
-      // Guo source in ASL units: (1 - om/2) rho [3 (c - u).g + 9 (c.u)(c.g)]
-      const C cu = C(Lt::c(i, 0)) * ux + C(Lt::c(i, 1)) * uy + C(Lt::c(i, 2)) * uz;
-      const C cg = C(Lt::c(i, 0)) * fx + C(Lt::c(i, 1)) * fy + C(Lt::c(i, 2)) * fz;
-      fn += half_src * (C(3) * (cg - cgu) + C(9) * cu * cg);
+      const C cg = cdot<Q, C>(i, gx, gy, gz);
+      fn += cg * (hs3 + hs9 * cm) + sA;
     }
     f[i] = fn;
   }

@@ -54,6 +54,8 @@ __host__ __device__ inline int wrap_axis(int v, int n, bool periodic) {
 
 struct StepParams {
   double nu;
+  float om0f;   // 1 / (3 nu + 1/2) in FP32 (ASL's LBGK::init0 expression order)
+  double om0d;  // the same in FP64
   double g[3];
   double Om[3];
   double cs;         // Smagorinsky constant

@@ -167,7 +167,7 @@ class LBGK:
         L.check(self.lib.aslb_lbgk_sync(self.h), "LBGK::sync")
 
     def setKernel(self, variant: int):
-        """1: TMA-staged persistent stream-collide (default), 0: direct loads."""
+        """0: direct-load stream-collide (default), 1: TMA-staged persistent kernel."""
         L.check(self.lib.aslb_lbgk_set_kernel(self.h, int(variant)), "LBGK::setKernel")
 
     @property

@@ -149,10 +149,10 @@ int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int us
 /* Wait for all work of the domain; fails with ASLB_ERR_STATE if a kernel's
  * bounded wait gave up. */
 int aslb_lbgk_sync(aslb_lbgk* h);
-/* Stream-collide kernel variant: 1 (default) stages every tile's population
- * rows in shared memory with asynchronous bulk copies (TMA) in a persistent,
- * pipelined kernel; 0 is the one-cell-per-thread kernel with direct loads.
- * Both give identical results. */
+/* Stream-collide kernel variant: 0 (default) is the one-cell-per-thread
+ * kernel with direct loads; 1 stages every tile's population rows in shared
+ * memory with asynchronous bulk copies (TMA) in a persistent, pipelined
+ * kernel. Both give identical results. */
 int aslb_lbgk_set_kernel(aslb_lbgk* h, int variant);
 int aslb_lbgk_get_kernel(aslb_lbgk* h);
 /* Steps taken so far. */
