@@ -47,38 +47,23 @@ struct StepOccupancy {
   static constexpr int blocks = (CL == CL_NONE && !std::is_same<S, double>::value) ? 4 : 2;
 };
 
-// ---------------------------------------------------------------------------
-// Stream + collide, one interior cell per thread. ODD: representation A -> B
-// (reads F[i][x - c_i], writes F[inv i][x + c_i]); EVEN: B -> A (reads
-// F[inv i][x], writes F[i][x]). Element indices are 32-bit (Q * dstride < 2^32).
-template <int Q, class S, int CL, bool ODD>
-__global__ void __launch_bounds__(256, StepOccupancy<S, CL>::blocks)
-    k_stream_collide(S* __restrict__ F, const GridDesc g, const StepParams p,
-                     typename MacroT<S>::T* __restrict__ rho_out, typename MacroT<S>::T* __restrict__ u_out) {
+// Load, collide and store one cell. MASKED: the cell's warp has fused no-slip
+// links (bounce bits select the bounce-back slot, elide bits skip stores).
+template <int Q, class S, int CL, bool ODD, bool MASKED>
+__device__ __forceinline__ void cell_update(S* __restrict__ F, const GridDesc& g, const StepParams& p,
+                                            typename MacroT<S>::T* __restrict__ rho_out,
+                                            typename MacroT<S>::T* __restrict__ u_out, int x, int y, int z,
+                                            unsigned s, const int (&ox)[3], const int (&oy)[3], const int (&oz)[3],
+                                            uint32_t bounce, uint32_t elide) {
   using Lt = Lattice<Q>;
   using C = typename Store<S>::C;
-  const int z = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int x = blockIdx.z + 1;
-  if (z > g.nz || y > g.ny) return;
-  const unsigned s = (unsigned)sidx(g, x, y, z);
   const unsigned ds = (unsigned)g.dstride;
-  // Fused no-slip links: a fluid cell reads bounce-back populations, a solid
-  // cell skips the writes the condition would overwrite.
-  uint32_t bounce = 0, elide = 0;
-  if (p.mask) {
-    const uint2 m = p.mask[s];
-    bounce = m.x;
-    elide = m.y;
-  }
-  int ox[3], oy[3], oz[3];
-  nb_offsets(g, x, y, z, ox, oy, oz);
   C f[Q];
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
     // Upstream neighbour slot, or for a bounce-back link this cell's own
     // outgoing population: the two slots swap roles between representations.
-    const bool b = (bounce >> i) & 1u;
+    const bool b = MASKED && ((bounce >> i) & 1u);
     unsigned idx;
     if (ODD) {
       idx = b ? (unsigned)Lt::inv(i) * ds + s
@@ -103,7 +88,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<S, CL>::blocks)
   }
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
-    if ((elide >> i) & 1u) continue;
+    if (MASKED && ((elide >> i) & 1u)) continue;
     unsigned idx;
     if (ODD)
       idx = (unsigned)Lt::inv(i) * ds + s + (unsigned)(ox[1 + Lt::c(i, 0)] + oy[1 + Lt::c(i, 1)] + oz[1 + Lt::c(i, 2)]);
@@ -111,6 +96,39 @@ __global__ void __launch_bounds__(256, StepOccupancy<S, CL>::blocks)
       idx = (unsigned)i * ds + s;
     Store<S>::store(F + idx, f[i], p);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Stream + collide, one interior cell per thread. ODD: representation A -> B
+// (reads F[i][x - c_i], writes F[inv i][x + c_i]); EVEN: B -> A (reads
+// F[inv i][x], writes F[i][x]). Element indices are 32-bit (Q * dstride < 2^32).
+template <int Q, class S, int CL, bool ODD>
+__global__ void __launch_bounds__(256, StepOccupancy<S, CL>::blocks)
+    k_stream_collide(S* __restrict__ F, const GridDesc g, const StepParams p,
+                     typename MacroT<S>::T* __restrict__ rho_out, typename MacroT<S>::T* __restrict__ u_out) {
+  using Lt = Lattice<Q>;
+  using C = typename Store<S>::C;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int x = blockIdx.z + 1;
+  if (z > g.nz || y > g.ny) return;
+  const unsigned s = (unsigned)sidx(g, x, y, z);
+  // Fused no-slip links: a fluid cell reads bounce-back populations, a solid
+  // cell skips the writes the condition would overwrite.
+  uint32_t bounce = 0, elide = 0;
+  if (p.mask) {
+    const uint2 m = p.mask[s];
+    bounce = m.x;
+    elide = m.y;
+  }
+  int ox[3], oy[3], oz[3];
+  nb_offsets(g, x, y, z, ox, oy, oz);
+  // Warps without any fused link take the unmasked path (no per-direction
+  // selects or predicated stores); the branch is uniform across the warp.
+  if (__any_sync(__activemask(), (bounce | elide) != 0u))
+    cell_update<Q, S, CL, ODD, true>(F, g, p, rho_out, u_out, x, y, z, s, ox, oy, oz, bounce, elide);
+  else
+    cell_update<Q, S, CL, ODD, false>(F, g, p, rho_out, u_out, x, y, z, s, ox, oy, oz, 0u, 0u);
 }
 
 inline void step_launch_shape(const GridDesc& g, dim3& grid, dim3& block) {
