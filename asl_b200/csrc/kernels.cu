@@ -8,15 +8,27 @@
 
 namespace aslb {
 
-cudaError_t step_q15(const DomainDev&, const StepParams&, int, int, cudaStream_t);
-cudaError_t step_q19(const DomainDev&, const StepParams&, int, int, cudaStream_t);
-cudaError_t step_q27(const DomainDev&, const StepParams&, int, int, cudaStream_t);
+cudaError_t step_q15_f32(const DomainDev&, const StepParams&, int, int, cudaStream_t);
+cudaError_t step_q15_f16(const DomainDev&, const StepParams&, int, int, cudaStream_t);
+cudaError_t step_q15_f64(const DomainDev&, const StepParams&, int, int, cudaStream_t);
+cudaError_t step_q19_f32(const DomainDev&, const StepParams&, int, int, cudaStream_t);
+cudaError_t step_q19_f16(const DomainDev&, const StepParams&, int, int, cudaStream_t);
+cudaError_t step_q19_f64(const DomainDev&, const StepParams&, int, int, cudaStream_t);
+cudaError_t step_q27_f32(const DomainDev&, const StepParams&, int, int, cudaStream_t);
+cudaError_t step_q27_f16(const DomainDev&, const StepParams&, int, int, cudaStream_t);
+cudaError_t step_q27_f64(const DomainDev&, const StepParams&, int, int, cudaStream_t);
 
 cudaError_t launch_step(const DomainDev& d, const StepParams& p, int closure, int parity_in, cudaStream_t st) {
-  switch (d.q) {
-    case 15: return step_q15(d, p, closure, parity_in, st);
-    case 19: return step_q19(d, p, closure, parity_in, st);
-    case 27: return step_q27(d, p, closure, parity_in, st);
+  switch (d.q * 8 + d.storage) {
+    case 15 * 8 + ST_F32: return step_q15_f32(d, p, closure, parity_in, st);
+    case 15 * 8 + ST_F16: return step_q15_f16(d, p, closure, parity_in, st);
+    case 15 * 8 + ST_F64: return step_q15_f64(d, p, closure, parity_in, st);
+    case 19 * 8 + ST_F32: return step_q19_f32(d, p, closure, parity_in, st);
+    case 19 * 8 + ST_F16: return step_q19_f16(d, p, closure, parity_in, st);
+    case 19 * 8 + ST_F64: return step_q19_f64(d, p, closure, parity_in, st);
+    case 27 * 8 + ST_F32: return step_q27_f32(d, p, closure, parity_in, st);
+    case 27 * 8 + ST_F16: return step_q27_f16(d, p, closure, parity_in, st);
+    case 27 * 8 + ST_F64: return step_q27_f64(d, p, closure, parity_in, st);
   }
   return cudaErrorInvalidValue;
 }

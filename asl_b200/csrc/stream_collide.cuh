@@ -47,8 +47,8 @@ struct StepOccupancy {
   static constexpr int blocks = (CL == CL_NONE && !std::is_same<S, double>::value) ? 4 : 2;
 };
 
-// Load, collide and store one cell. MASKED: the cell's warp has fused no-slip
-// links (bounce bits select the bounce-back slot, elide bits skip stores).
+// Load, collide and store one cell. MASKED: apply the fused no-slip links
+// (bounce bits select the bounce-back slot, elide bits skip stores).
 template <int Q, class S, int CL, bool ODD, bool MASKED>
 __device__ __forceinline__ void cell_update(S* __restrict__ F, const GridDesc& g, const StepParams& p,
                                             typename MacroT<S>::T* __restrict__ rho_out,
@@ -102,7 +102,9 @@ __device__ __forceinline__ void cell_update(S* __restrict__ F, const GridDesc& g
 // Stream + collide, one interior cell per thread. ODD: representation A -> B
 // (reads F[i][x - c_i], writes F[inv i][x + c_i]); EVEN: B -> A (reads
 // F[inv i][x], writes F[i][x]). Element indices are 32-bit (Q * dstride < 2^32).
-template <int Q, class S, int CL, bool ODD>
+// FUSED: the domain has fused no-slip links (p.mask is read); chosen on the
+// host so domains without them run the unmasked code.
+template <int Q, class S, int CL, bool ODD, bool FUSED>
 __global__ void __launch_bounds__(256, StepOccupancy<S, CL>::blocks)
     k_stream_collide(S* __restrict__ F, const GridDesc g, const StepParams p,
                      typename MacroT<S>::T* __restrict__ rho_out, typename MacroT<S>::T* __restrict__ u_out) {
@@ -116,19 +118,14 @@ __global__ void __launch_bounds__(256, StepOccupancy<S, CL>::blocks)
   // Fused no-slip links: a fluid cell reads bounce-back populations, a solid
   // cell skips the writes the condition would overwrite.
   uint32_t bounce = 0, elide = 0;
-  if (p.mask) {
+  if (FUSED) {
     const uint2 m = p.mask[s];
     bounce = m.x;
     elide = m.y;
   }
   int ox[3], oy[3], oz[3];
   nb_offsets(g, x, y, z, ox, oy, oz);
-  // Warps without any fused link take the unmasked path (no per-direction
-  // selects or predicated stores); the branch is uniform across the warp.
-  if (__any_sync(__activemask(), (bounce | elide) != 0u))
-    cell_update<Q, S, CL, ODD, true>(F, g, p, rho_out, u_out, x, y, z, s, ox, oy, oz, bounce, elide);
-  else
-    cell_update<Q, S, CL, ODD, false>(F, g, p, rho_out, u_out, x, y, z, s, ox, oy, oz, 0u, 0u);
+  cell_update<Q, S, CL, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, z, s, ox, oy, oz, bounce, elide);
 }
 
 inline void step_launch_shape(const GridDesc& g, dim3& grid, dim3& block) {
@@ -149,10 +146,18 @@ cudaError_t step_q_s_cl(const DomainDev& d, const StepParams& p, int parity_in, 
   dim3 grid, block;
   step_launch_shape(d.g, grid, block);
   using M = typename MacroT<S>::T;
-  if (parity_in == 0)
-    k_stream_collide<Q, S, CL, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
-  else
-    k_stream_collide<Q, S, CL, false><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+  const bool fused = p.mask != nullptr;
+  if (parity_in == 0) {
+    if (fused)
+      k_stream_collide<Q, S, CL, true, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+    else
+      k_stream_collide<Q, S, CL, true, false><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+  } else {
+    if (fused)
+      k_stream_collide<Q, S, CL, false, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+    else
+      k_stream_collide<Q, S, CL, false, false><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+  }
   return cudaGetLastError();
 }
 
