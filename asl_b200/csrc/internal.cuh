@@ -70,7 +70,9 @@ struct StepParams {
   // x (bounce): bit k = population k enters this cell through a fused link,
   // so it is read by bounce-back from the cell's own outgoing population.
   // y (elide): bit k = the cell's outgoing population k lands in the incoming
-  // slot of a fused link, which the condition would overwrite: not written.
+  // slot of a fused link, which the condition would overwrite: the slot keeps
+  // its bits (FP32/FP64 skip the store; FP16 stores back what it holds, so
+  // that warps write whole sectors).
   const uint2* mask;
 };
 
@@ -83,6 +85,7 @@ struct Store<float> {
   using C = float;
   __device__ static __forceinline__ C load(const float* p, const StepParams&) { return *p; }
   __device__ static __forceinline__ void store(float* p, C v, const StepParams&) { *p = v; }
+  __device__ static __forceinline__ float encode(C v, const StepParams&) { return v; }
   // deviation from rest (f - 1)
   __device__ static __forceinline__ C dev(const float* p, float) { return *p - 1.0f; }
   __device__ static __forceinline__ void set_dev(float* p, C d, float) { *p = 1.0f + d; }
@@ -95,6 +98,7 @@ struct Store<double> {
   using C = double;
   __device__ static __forceinline__ C load(const double* p, const StepParams&) { return *p; }
   __device__ static __forceinline__ void store(double* p, C v, const StepParams&) { *p = v; }
+  __device__ static __forceinline__ double encode(C v, const StepParams&) { return v; }
   __device__ static __forceinline__ C dev(const double* p, float) { return *p - 1.0; }
   __device__ static __forceinline__ void set_dev(double* p, C d, float) { *p = 1.0 + d; }
   __device__ static __forceinline__ C val(const double* p, float) { return *p; }
@@ -112,6 +116,9 @@ struct Store<__half> {
   }
   __device__ static __forceinline__ void store(__half* p, C v, const StepParams& sp) {
     *p = __float2half_rn((v - 1.0f) * sp.scale);
+  }
+  __device__ static __forceinline__ __half encode(C v, const StepParams& sp) {
+    return __float2half_rn((v - 1.0f) * sp.scale);
   }
   __device__ static __forceinline__ C dev(const __half* p, float inv_scale) { return __half2float(*p) * inv_scale; }
   __device__ static __forceinline__ void set_dev(__half* p, C d, float scale) { *p = __float2half_rn(d * scale); }

@@ -1,6 +1,6 @@
 // Fused AA-pattern stream-collide kernel (one interior cell per thread) and its
-// launch helpers. Instantiated per lattice in step_q15.cu / step_q19.cu /
-// step_q27.cu so the instantiations compile in parallel.
+// launch helpers. Instantiated per lattice and storage in step_q<Q>_<type>.cu
+// so the instantiations compile in parallel.
 #pragma once
 #include <type_traits>
 #include "kernels.h"
@@ -39,13 +39,33 @@ __device__ __forceinline__ void nb_offsets(const GridDesc& g, int x, int y, int 
   }
 }
 
-// Resident blocks of 256 threads per SM the register budget aims for: four
-// (64 registers) for the plain FP32/FP16 kernels, which must keep enough
-// loads in flight to saturate HBM; two for FP64 and the closures.
-template <class S, int CL>
+// Resident blocks of 256 threads per SM the register budget aims for. The
+// plain FP32/FP16 kernels must keep enough loads in flight to saturate HBM:
+// four blocks (64 registers) with fused links, whose per-direction slot
+// selects keep the schedule compact; three (80 registers) without, where the
+// compiler hoists all addresses and 64 registers would spill (two, 128
+// registers, for D3Q27). Two for FP64 and the closures.
+template <int Q, class S, int CL, bool FUSED>
 struct StepOccupancy {
-  static constexpr int blocks = (CL == CL_NONE && !std::is_same<S, double>::value) ? 4 : 2;
+  static constexpr int blocks =
+      (CL == CL_NONE && !std::is_same<S, double>::value) ? (FUSED ? 4 : (Q == 27 ? 2 : 3)) : 2;
 };
+
+// Store one outgoing population. An elided slot keeps its bits: FP32/FP64
+// skip the store; 2-byte storage writes back what the slot holds (bits no
+// other cell writes this step), so a warp's store covers whole sectors
+// instead of leaving partial ones that HBM must read to merge.
+template <class S>
+__device__ __forceinline__ void store_slot(S* __restrict__ slot, typename Store<S>::C v, bool elided,
+                                           const StepParams& p) {
+  if (sizeof(S) > 2) {
+    if (!elided) *slot = Store<S>::encode(v, p);
+  } else {
+    S out = Store<S>::encode(v, p);
+    if (elided) out = *slot;
+    *slot = out;
+  }
+}
 
 // Load, collide and store one cell. MASKED: apply the fused no-slip links
 // (bounce bits select the bounce-back slot, elide bits skip stores).
@@ -88,13 +108,12 @@ __device__ __forceinline__ void cell_update(S* __restrict__ F, const GridDesc& g
   }
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
-    if (MASKED && ((elide >> i) & 1u)) continue;
     unsigned idx;
     if (ODD)
       idx = (unsigned)Lt::inv(i) * ds + s + (unsigned)(ox[1 + Lt::c(i, 0)] + oy[1 + Lt::c(i, 1)] + oz[1 + Lt::c(i, 2)]);
     else
       idx = (unsigned)i * ds + s;
-    Store<S>::store(F + idx, f[i], p);
+    store_slot<S>(F + idx, f[i], MASKED && ((elide >> i) & 1u), p);
   }
 }
 
@@ -105,7 +124,7 @@ __device__ __forceinline__ void cell_update(S* __restrict__ F, const GridDesc& g
 // FUSED: the domain has fused no-slip links (p.mask is read); chosen on the
 // host so domains without them run the unmasked code.
 template <int Q, class S, int CL, bool ODD, bool FUSED>
-__global__ void __launch_bounds__(256, StepOccupancy<S, CL>::blocks)
+__global__ void __launch_bounds__(256, StepOccupancy<Q, S, CL, FUSED>::blocks)
     k_stream_collide(S* __restrict__ F, const GridDesc g, const StepParams p,
                      typename MacroT<S>::T* __restrict__ rho_out, typename MacroT<S>::T* __restrict__ u_out) {
   using Lt = Lattice<Q>;

@@ -1,11 +1,12 @@
-// Stream-collide with TMA staging (sm_100a). A persistent CTA of 256 threads
-// walks tiles of R z-rows x TZ cells. For every tile one elected thread issues
-// 1-D bulk copies (cp.async.bulk) of the Q population rows the tile reads,
-// plus its row of fused-link masks, into one of `stages` shared-memory
-// buffers, tracked by an mbarrier with transaction counts; the copies for the
-// next tiles are in flight while the CTA computes the current one, so HBM
-// stays busy without registers holding loads. Results go straight to global
-// memory (the AA pattern writes the same slots it read).
+// Stream-collide with TMA staging (sm_100a). A persistent, warp-specialised
+// CTA (eight compute warps and one producer warp) walks tiles of R z-rows x
+// TZ cells. For every tile the producer warp's lanes issue 1-D bulk copies
+// (cp.async.bulk) of the Q population rows the tile reads, plus its row of
+// fused-link masks, into one of `stages` shared-memory buffers, tracked by
+// full/empty mbarriers with transaction counts; the copies for the next tiles
+// are in flight while the compute warps work on the current one, so HBM stays
+// busy without registers holding loads. Results go straight to global memory
+// (the AA pattern writes the same slots it read).
 //
 // Alignment: a row's first interior cell is 128-byte aligned and x/y
 // neighbour offsets are whole rows, so every copy is exactly the 128-byte
@@ -197,13 +198,12 @@ __global__ void __launch_bounds__(kTmaThreads, TmaOccupancy<S, CL>::blocks)
     }
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-      if ((elide >> i) & 1u) continue;
       unsigned idx;
       if (ODD)
         idx = (unsigned)Lt::inv(i) * ds + s + (unsigned)(ox[1 + Lt::c(i, 0)] + oy[1 + Lt::c(i, 1)] + oz[1 + Lt::c(i, 2)]);
       else
         idx = (unsigned)i * ds + s;
-      Store<S>::store(F + idx, f[i], p);
+      store_slot<S>(F + idx, f[i], (elide >> i) & 1u, p);
     }
   }
 }
