@@ -65,14 +65,14 @@ def peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profile_traffic(name: str):
-    """DRAM bytes per launch from a committed ncu summary (line
-    'traffic_bytes_per_launch: N'), or None."""
+def profile_traffic(name: str, cells: int):
+    """DRAM bytes per launch of `cells` cells from a committed ncu summary
+    (line 'traffic_bytes_per_cell: B', measured read + write per cell), or None."""
     p = ROOT / "profiles" / name
     try:
         for line in p.read_text().splitlines():
-            if line.strip().startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].split()[0])
+            if line.strip().startswith("traffic_bytes_per_cell:"):
+                return float(line.split(":", 1)[1].split()[0]) * cells
     except OSError:
         pass
     return None
@@ -309,12 +309,12 @@ def run_ours(args):
 
     bpc = BYTES_PER_CELL[(args.storage, w.q)]
     achieved = bpc * w.cells / tk / 1e9
-    traffic = profile_traffic(f"stream_collide_d3q19_{args.storage}_porous.md")
+    traffic = profile_traffic(f"stream_collide_d3q19_{args.storage}_porous.md", w.cells)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_source": peak_kind,
             "kernel": f"k_stream_collide<19,{args.storage}> (AA pattern, odd/even launches averaged)",
             "bytes_per_cell": bpc, "cells_per_launch": w.cells, "kernel_ms": tk * 1e3,
-            "note": "algorithmic bytes: read + write of 19 populations per cell; the 4-byte fused-link "
+            "note": "algorithmic bytes: read + write of 19 populations per cell; the 8-byte fused-link "
                     "mask per cell is overhead and not counted"}
 
     cb = None
