@@ -99,6 +99,19 @@ void prepare_params(aslb_lbgk* h) {
   // omega = 1 / (3 nu + 1/2) (src/num/aslLBGK.cxx:203), once per step on the host
   h->p.om0f = 1.0f / (3.0f * (float)h->p.nu + 0.5f);
   h->p.om0d = 1.0 / (3.0 * h->p.nu + 0.5);
+  h->p.nuf = (float)h->p.nu;
+  h->p.csf = (float)h->p.cs;
+  for (int a = 0; a < 3; ++a) {
+    h->p.gf[a] = (float)h->p.g[a];
+    h->p.Omf[a] = (float)h->p.Om[a];
+  }
+  for (int i = 0; i < 27; ++i) {
+    double cg = 0.0;
+    if (i < h->d.q)
+      for (int a = 0; a < 3; ++a) cg += lattice_c(h->d.q, i, a) * h->p.g[a];
+    h->p.cgd[i] = cg;
+    h->p.cgf[i] = (float)cg;
+  }
   h->p.write_rho = (h->comp_rho || h->macro_once) ? 1 : 0;
   h->p.write_vel = (h->comp_vel || h->macro_once) ? 1 : 0;
   h->p.write_macro = h->p.write_rho | h->p.write_vel;

@@ -6,8 +6,25 @@
 //   f_i   <- (1 - omega) f_i + omega f_eq,i,  omega = 1 / (3 nu + 1/2)
 // plus the optional Coriolis term (component-sequential like ASL's generated
 // code), Guo forcing for a body force, and the closures that replace omega.
+//
+// Evaluation. Opposite directions i, i' = inv(i) share |c|^2 and weight, and
+// c_i.v = -c_i'.v, so the kernel works on pairs:
+//   moments   s = f_i + f_i', d = f_i - f_i', summed per weight class first
+//             (rho = w_0 f_0 + sum_k w_k S_k, m = sum_k w_k M_k),
+//   update    f_i  <- (1 - om) f_i  + (P + A)
+//             f_i' <- (1 - om) f_i' + (P - A)
+//   with the even part P = om (a0 + a2 cm^2) + Guo's even part and the odd
+//   part A = 3 om cm + Guo's odd part (cm = c_i.m). The result is the same
+//   expression as ASL's, evaluated in another order (rounding differences only).
+//
+// Collision representation. FP32/FP64 storage hands the collision f itself.
+// FP16 storage holds D = (f - 1) * sigma and the collision works on D
+// directly: with V = sum w D = sigma (rho - 1) and M = sum w c D = sigma m,
+//   sigma (f_eq,i - 1) = V + 3 c.M + 4.5 (c.M)^2 / (sigma rho) - 1.5 M.M / (sigma rho)
+// i.e. the same update with a0, a2 rescaled, and rho = 1 + V / sigma.
 #pragma once
 #include <type_traits>
+#include <utility>
 #include "internal.cuh"
 #include "mlp.cuh"
 
@@ -27,6 +44,42 @@ __device__ __forceinline__ double fma_(double a, double b, double c) { return __
 __device__ __forceinline__ float div_(float a, float b) { return __fdiv_rn(a, b); }
 __device__ __forceinline__ double div_(double a, double b) { return __ddiv_rn(a, b); }
 
+// Compile-time loop: f(std::integral_constant<int, I>) for I = 0 .. N-1.
+template <class F, int... I>
+__device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+// Opposite pairs of a lattice, grouped by |c|^2 (the weight class).
+template <int Q>
+struct Pairs {
+  using Lt = Lattice<Q>;
+  // i represents the pair (i, inv i)
+  __host__ __device__ static constexpr bool rep(int i) { return i > 0 && i < Lt::inv(i); }
+  __host__ __device__ static constexpr bool present(int k) {
+    for (int j = 1; j < Q; ++j)
+      if (Lt::norm2(j) == k) return true;
+    return false;
+  }
+  __host__ __device__ static constexpr int first_of(int k) {
+    for (int j = 1; j < Q; ++j)
+      if (Lt::norm2(j) == k) return j;
+    return 0;
+  }
+  // first representative of its class (with c_a != 0 when a >= 0)
+  __host__ __device__ static constexpr bool first(int i, int a) {
+    for (int j = 1; j < i; ++j)
+      if (rep(j) && Lt::norm2(j) == Lt::norm2(i) && (a < 0 || Lt::c(j, a) != 0)) return false;
+    return true;
+  }
+  // smallest class present
+  __host__ __device__ static constexpr int kmin() { return present(1) ? 1 : (present(2) ? 2 : 3); }
+};
+
 // c_i . v with the lattice vector known at compile time: only the nonzero
 // components are added (0 * v cannot be dropped by the compiler under IEEE
 // rules), the same value as the full dot product for finite v.
@@ -41,55 +94,114 @@ __device__ __forceinline__ C cdot(int i, C v0, C v1, C v2) {
   return r;
 }
 
-template <int Q, class C, int CL>
+// Step parameters in the collision's arithmetic (FP32 copies for float).
+template <class C>
+__device__ __forceinline__ C par_g(const StepParams& p, int a) {
+  if constexpr (std::is_same<C, double>::value) return p.g[a]; else return p.gf[a];
+}
+template <class C>
+__device__ __forceinline__ C par_Om(const StepParams& p, int a) {
+  if constexpr (std::is_same<C, double>::value) return p.Om[a]; else return p.Omf[a];
+}
+template <class C>
+__device__ __forceinline__ C par_cg(const StepParams& p, int i) {
+  if constexpr (std::is_same<C, double>::value) return p.cgd[i]; else return p.cgf[i];
+}
+template <class C>
+__device__ __forceinline__ C par_nu(const StepParams& p) {
+  if constexpr (std::is_same<C, double>::value) return p.nu; else return p.nuf;
+}
+template <class C>
+__device__ __forceinline__ C par_cs(const StepParams& p) {
+  if constexpr (std::is_same<C, double>::value) return p.cs; else return p.csf;
+}
+
+// f: the Q values of one cell in the collision representation (f, or
+// D = (f - 1) sigma when DEV), replaced by the post-collision values.
+// rho_out / u_out: density and velocity (ASL's compRho / compVel fields).
+template <int Q, class C, int CL, bool DEV = false>
 __device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, C& rho_out, C (&u_out)[3]) {
   using Lt = Lattice<Q>;
-  C m0 = C(0), m1 = C(0), m2 = C(0), rho = C(0);
-#pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    const C wf = mul_(C(Lt::w(i)), f[i]);
-    rho = add_(rho, wf);
-    if (Lt::c(i, 0) > 0) m0 = add_(m0, wf);
-    if (Lt::c(i, 0) < 0) m0 = sub_(m0, wf);
-    if (Lt::c(i, 1) > 0) m1 = add_(m1, wf);
-    if (Lt::c(i, 1) < 0) m1 = sub_(m1, wf);
-    if (Lt::c(i, 2) > 0) m2 = add_(m2, wf);
-    if (Lt::c(i, 2) < 0) m2 = sub_(m2, wf);
-  }
+  using Pr = Pairs<Q>;
+  // ---- moments: pair sums and differences, per weight class
+  C S[4], M[4][3];
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    if constexpr (Pr::rep(i)) {
+      constexpr int j = Lt::inv(i);
+      constexpr int k = Lt::norm2(i);
+      const C s = add_(f[i], f[j]);
+      const C d = sub_(f[i], f[j]);
+      if constexpr (Pr::first(i, -1)) S[k] = s; else S[k] = add_(S[k], s);
+      static_for<3>([&](auto ac) {
+        constexpr int a = decltype(ac)::value;
+        if constexpr (Lt::c(i, a) != 0) {
+          if constexpr (Pr::first(i, a)) M[k][a] = Lt::c(i, a) > 0 ? d : -d;
+          else M[k][a] = Lt::c(i, a) > 0 ? add_(M[k][a], d) : sub_(M[k][a], d);
+        }
+      });
+    }
+  });
+  C V = mul_(C(Lt::w(0)), f[0]);
+  C m0 = C(0), m1 = C(0), m2 = C(0);
+  static_for<4>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    if constexpr (k > 0 && Pr::present(k)) {
+      const C wk = C(Lt::w(Pr::first_of(k)));
+      V = fma_(wk, S[k], V);
+      if constexpr (k == Pr::kmin()) {
+        m0 = mul_(wk, M[k][0]);
+        m1 = mul_(wk, M[k][1]);
+        m2 = mul_(wk, M[k][2]);
+      } else {
+        m0 = fma_(wk, M[k][0], m0);
+        m1 = fma_(wk, M[k][1], m1);
+        m2 = fma_(wk, M[k][2], m2);
+      }
+    }
+  });
+  // rho; with DEV, V = sigma (rho - 1) and m = sigma * momentum
+  const C sig = DEV ? C(p.scale) : C(1);
+  const C isig = DEV ? C(p.inv_scale) : C(1);
+  const C rho = DEV ? fma_(V, isig, C(1)) : V;
+
   // omega = 1 / (3 nu + 1/2), evaluated on the host in the storage's arithmetic
   const C om0 = std::is_same<C, double>::value ? C(p.om0d) : C(p.om0f);
   C om = om0;
   if (p.has_coriolis) {
     // component-sequential, as ACL emits `momentum += (2/w) Omega x momentum`
     const C k = div_(C(2), om);
-    const C O0 = C(p.Om[0]), O1 = C(p.Om[1]), O2 = C(p.Om[2]);
+    const C O0 = par_Om<C>(p, 0), O1 = par_Om<C>(p, 1), O2 = par_Om<C>(p, 2);
     m0 = fma_(k, sub_(mul_(O1, m2), mul_(O2, m1)), m0);
     m1 = fma_(k, sub_(mul_(O2, m0), mul_(O0, m2)), m1);
     m2 = fma_(k, sub_(mul_(O0, m1), mul_(O1, m0)), m2);
   }
   if (p.has_force) {
-    const C hr = mul_(C(0.5), rho);
-    m0 = fma_(hr, C(p.g[0]), m0);
-    m1 = fma_(hr, C(p.g[1]), m1);
-    m2 = fma_(hr, C(p.g[2]), m2);
+    const C hr = DEV ? mul_(mul_(C(0.5), rho), sig) : mul_(C(0.5), rho);
+    m0 = fma_(hr, par_g<C>(p, 0), m0);
+    m1 = fma_(hr, par_g<C>(p, 1), m1);
+    m2 = fma_(hr, par_g<C>(p, 2), m2);
   }
   const C inv_rho = div_(C(1), rho);
+  // factor taking the stored momentum to velocity (u = m / rho, or m when
+  // incompressible), with the 1 / sigma of DEV folded in
+  const C ium = p.compressible ? (DEV ? mul_(isig, inv_rho) : inv_rho) : isig;
   rho_out = rho;
-  if (p.compressible) {
-    u_out[0] = mul_(m0, inv_rho);
-    u_out[1] = mul_(m1, inv_rho);
-    u_out[2] = mul_(m2, inv_rho);
+  if (DEV || p.compressible) {
+    u_out[0] = mul_(m0, ium);
+    u_out[1] = mul_(m1, ium);
+    u_out[2] = mul_(m2, ium);
   } else {
     u_out[0] = m0;
     u_out[1] = m1;
     u_out[2] = m2;
   }
   const C mm = fma_(m2, m2, fma_(m1, m1, mul_(m0, m0)));
-  const C a2 = p.compressible ? mul_(C(4.5), inv_rho) : C(4.5);
-  const C a0 = p.compressible ? sub_(rho, mul_(mul_(C(1.5), mm), inv_rho)) : sub_(rho, mul_(C(1.5), mm));
+  const C a2 = (DEV || p.compressible) ? mul_(C(4.5), ium) : C(4.5);
+  const C a0 = (DEV || p.compressible) ? sub_(V, mul_(mul_(C(1.5), mm), ium)) : sub_(V, mul_(C(1.5), mm));
 
-  if (CL == CL_ASL_INTENT || CL == CL_SMAGORINSKY || CL == CL_MLP) {
-    // Non-equilibrium quantities need f_eq first.
+  if constexpr (CL == CL_ASL_INTENT || CL == CL_SMAGORINSKY || CL == CL_MLP) {
+    // Non-equilibrium quantities need f_eq first (scaled by sigma with DEV).
     C sn = C(0), sf = C(0);
     C P00 = C(0), P11 = C(0), P22 = C(0), P01 = C(0), P12 = C(0), P02 = C(0);
 #pragma unroll
@@ -98,8 +210,9 @@ __device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, C& 
       const C feq = fma_(a2, mul_(cm, cm), fma_(C(3), cm, a0));
       const C d = sub_(f[i], feq);
       if (CL == CL_ASL_INTENT) {
+        const C fa = DEV ? fma_(f[i], isig, C(1)) : f[i];
         sn = fma_(d, d, sn);
-        sf = fma_(f[i], f[i], sf);
+        sf = fma_(fa, fa, sf);
       } else {
         const C wd = mul_(C(Lt::w(i)), d);
         if (Lt::c(i, 0) != 0) P00 += wd;
@@ -113,51 +226,66 @@ __device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, C& 
         if (Lt::c(i, 0) * Lt::c(i, 2) < 0) P02 -= wd;
       }
     }
-    if (CL == CL_ASL_INTENT) {
+    if (DEV) {
+      sn = mul_(mul_(sn, isig), isig);
+      P00 = mul_(P00, isig); P11 = mul_(P11, isig); P22 = mul_(P22, isig);
+      P01 = mul_(P01, isig); P12 = mul_(P12, isig); P02 = mul_(P02, isig);
+    }
+    if constexpr (CL == CL_ASL_INTENT) {
       // LBGKTurbulence's limiter: w = 4 |f - f_eq|^2 / |f|^2
       const C wl = mul_(C(4), div_(sn, sf));
-      if (wl > C(1)) om = div_(C(1), add_(mul_(C(3), fmin(mul_(C(p.nu), wl), C(0.5))), C(0.5)));
-    } else if (CL == CL_SMAGORINSKY) {
+      if (wl > C(1)) om = div_(C(1), add_(mul_(C(3), fmin(mul_(par_nu<C>(p), wl), C(0.5))), C(0.5)));
+    } else if constexpr (CL == CL_SMAGORINSKY) {
       // Hou, Sterling, Chen & Doolen (1996): tau = (tau0 + sqrt(tau0^2 + 18 sqrt(2) Cs^2 |Pi_neq| / rho)) / 2
       const C q2 = add_(fma_(P22, P22, fma_(P11, P11, mul_(P00, P00))),
                         mul_(C(2), fma_(P02, P02, fma_(P12, P12, mul_(P01, P01)))));
       const C tau0 = div_(C(1), om0);
-      const C cs2 = mul_(C(p.cs), C(p.cs));
+      const C cs = par_cs<C>(p);
+      const C cs2 = mul_(cs, cs);
       const C tau = mul_(C(0.5), add_(tau0, sqrt(fma_(tau0, tau0, mul_(mul_(mul_(C(25.455844122715710), cs2),
                                                                             sqrt(q2)), inv_rho)))));
       om = div_(C(1), tau);
     } else {
       // Learned closure: tau_eff from invariants of Pi_neq and the strain.
-      om = mlp_omega<C>(p.mlp, om0, rho, m0 * inv_rho, m1 * inv_rho, m2 * inv_rho, P00, P11, P22, P01, P12, P02);
+      const C iu = DEV ? mul_(isig, inv_rho) : inv_rho;
+      om = mlp_omega<C>(p.mlp, om0, rho, m0 * iu, m1 * iu, m2 * iu, P00, P11, P22, P01, P12, P02);
     }
   }
 
-  // Relaxation folded into three multiply-adds per direction:
-  //   (1 - om) f + om f_eq = (1 - om) f + om a0 + cm (3 om + om a2 cm)
+  // ---- relaxation, one opposite pair at a time:
+  //   (1 - om) f + om f_eq = (1 - om) f + [om a0 + om a2 cm^2] +- [3 om cm]
   const C one_m = sub_(C(1), om);
   const C oa0 = mul_(om, a0), o3 = mul_(C(3), om), oa2 = mul_(om, a2);
-  // Guo source (1 - om/2) rho [3 (c - u).g + 9 (c.u)(c.g)] with u = m / rho:
-  //   c.g (hs3 + hs9 c.m) + sA,  hs9 = 9 hs / rho,  sA = -hs3 u.g
-  C gx = C(0), gy = C(0), gz = C(0), hs3 = C(0), hs9 = C(0), sA = C(0);
+  // Guo source (1 - om/2) rho [3 (c - u).g + 9 (c.u)(c.g)] with u = m / rho,
+  // times sigma with DEV:  even part hs9 cm cg + sA, odd part hs3 cg, with
+  // hs = (1 - om/2) rho, hs3 = 3 sigma hs, hs9 = 9 hs / rho, sA = -3 hs (m.g) / rho.
+  C hs3 = C(0), hs9 = C(0), c0 = oa0;
   if (p.has_force) {
-    gx = C(p.g[0]);
-    gy = C(p.g[1]);
-    gz = C(p.g[2]);
+    const C gx = par_g<C>(p, 0), gy = par_g<C>(p, 1), gz = par_g<C>(p, 2);
     const C hs = mul_(sub_(C(1), mul_(C(0.5), om)), rho);
-    hs3 = mul_(C(3), hs);
+    const C h3 = mul_(C(3), hs);
+    hs3 = DEV ? mul_(h3, sig) : h3;
     hs9 = mul_(mul_(C(9), hs), inv_rho);
-    sA = -mul_(hs3, mul_(fma_(m2, gz, fma_(m1, gy, mul_(m0, gx))), inv_rho));
+    const C sA = -mul_(h3, mul_(fma_(m2, gz, fma_(m1, gy, mul_(m0, gx))), inv_rho));
+    c0 = add_(oa0, sA);
   }
-#pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    const C cm = cdot<Q, C>(i, m0, m1, m2);
-    C fn = fma_(one_m, f[i], fma_(fma_(oa2, cm, o3), cm, oa0));
-    if (p.has_force) {
-      const C cg = cdot<Q, C>(i, gx, gy, gz);
-      fn = add_(fn, fma_(cg, fma_(hs9, cm, hs3), sA));
+  f[0] = fma_(one_m, f[0], c0);
+  static_for<Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    if constexpr (Pr::rep(i)) {
+      constexpr int j = Lt::inv(i);
+      const C cm = cdot<Q, C>(i, m0, m1, m2);
+      C P = fma_(mul_(oa2, cm), cm, c0);
+      C A = mul_(o3, cm);
+      if (p.has_force) {
+        const C cg = par_cg<C>(p, i);
+        P = fma_(mul_(hs9, cg), cm, P);
+        A = fma_(hs3, cg, A);
+      }
+      f[i] = fma_(one_m, f[i], add_(P, A));
+      f[j] = fma_(one_m, f[j], sub_(P, A));
     }
-    f[i] = fn;
-  }
+  });
 }
 
 }  // namespace aslb

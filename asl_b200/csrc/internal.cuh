@@ -59,6 +59,11 @@ struct StepParams {
   double g[3];
   double Om[3];
   double cs;         // Smagorinsky constant
+  // FP32 copies of the scalars above and c_i . g per direction, set on the
+  // host before every launch so kernels convert nothing per cell.
+  float nuf, csf, gf[3], Omf[3];
+  float cgf[27];
+  double cgd[27];
   int has_force;
   int has_coriolis;
   int compressible;
@@ -85,6 +90,9 @@ struct Store<float> {
   using C = float;
   __device__ static __forceinline__ C load(const float* p, const StepParams&) { return *p; }
   __device__ static __forceinline__ void store(float* p, C v, const StepParams&) { *p = v; }
+  // Values in the collision's representation: f itself.
+  static constexpr bool kDev = false;
+  __device__ static __forceinline__ C load_c(const float* p) { return *p; }
   __device__ static __forceinline__ float encode(C v, const StepParams&) { return v; }
   // deviation from rest (f - 1)
   __device__ static __forceinline__ C dev(const float* p, float) { return *p - 1.0f; }
@@ -98,6 +106,8 @@ struct Store<double> {
   using C = double;
   __device__ static __forceinline__ C load(const double* p, const StepParams&) { return *p; }
   __device__ static __forceinline__ void store(double* p, C v, const StepParams&) { *p = v; }
+  static constexpr bool kDev = false;
+  __device__ static __forceinline__ C load_c(const double* p) { return *p; }
   __device__ static __forceinline__ double encode(C v, const StepParams&) { return v; }
   __device__ static __forceinline__ C dev(const double* p, float) { return *p - 1.0; }
   __device__ static __forceinline__ void set_dev(double* p, C d, float) { *p = 1.0 + d; }
@@ -117,9 +127,12 @@ struct Store<__half> {
   __device__ static __forceinline__ void store(__half* p, C v, const StepParams& sp) {
     *p = __float2half_rn((v - 1.0f) * sp.scale);
   }
-  __device__ static __forceinline__ __half encode(C v, const StepParams& sp) {
-    return __float2half_rn((v - 1.0f) * sp.scale);
-  }
+  // The collision works on the stored quantity D = (f - 1) * scale directly
+  // (its moments and equilibrium are rescaled, see collide.cuh), so a load
+  // and a store are one conversion each.
+  static constexpr bool kDev = true;
+  __device__ static __forceinline__ C load_c(const __half* p) { return __half2float(*p); }
+  __device__ static __forceinline__ __half encode(C v, const StepParams&) { return __float2half_rn(v); }
   __device__ static __forceinline__ C dev(const __half* p, float inv_scale) { return __half2float(*p) * inv_scale; }
   __device__ static __forceinline__ void set_dev(__half* p, C d, float scale) { *p = __float2half_rn(d * scale); }
   __device__ static __forceinline__ C val(const __half* p, float inv_scale) { return 1.0f + __half2float(*p) * inv_scale; }

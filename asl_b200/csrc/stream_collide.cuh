@@ -93,10 +93,10 @@ __device__ __forceinline__ void cell_update(S* __restrict__ F, const GridDesc& g
     } else {
       idx = (unsigned)Lt::inv(i) * ds + s;
     }
-    f[i] = Store<S>::load(F + idx, p);
+    f[i] = Store<S>::load_c(F + idx);
   }
   C rho, u[3];
-  collide_cell<Q, C, CL>(f, p, rho, u);
+  collide_cell<Q, C, CL, Store<S>::kDev>(f, p, rho, u);
   if (p.write_macro) {
     const long long a = aidx(g, x, y, z);
     if (p.write_rho) rho_out[a] = rho;

@@ -166,18 +166,18 @@ __global__ void __launch_bounds__(kTmaThreads, TmaOccupancy<S, CL>::blocks)
           // bounce-back: the other slot of the pair, read from global memory
           const unsigned up = s + (unsigned)(ox[1 - Lt::c(i, 0)] + oy[1 - Lt::c(i, 1)] + oz[1 - Lt::c(i, 2)]);
           const unsigned idx = ODD ? (unsigned)Lt::inv(i) * ds + s : (unsigned)i * ds + up;
-          f[i] = Store<S>::load(F + idx, p);
+          f[i] = Store<S>::load_c(F + idx);
         } else if (ODD) {
           // upstream cell z - c_z (wrapped on a periodic z axis) inside the staged row
           const int pos = z + oz[1 - Lt::c(i, 2)] - (1 + seg * sh.tz);
           if (pos >= 0 && pos < sh.span) {
-            f[i] = Store<S>::load(stage_pop<S>(smem, sh, st, lr, i, Q) + pos, p);
+            f[i] = Store<S>::load_c(stage_pop<S>(smem, sh, st, lr, i, Q) + pos);
           } else {  // ghost z, or a periodic wrap into another segment of a long row
             const unsigned up = s + (unsigned)(ox[1 - Lt::c(i, 0)] + oy[1 - Lt::c(i, 1)] + oz[1 - Lt::c(i, 2)]);
-            f[i] = Store<S>::load(F + (unsigned)i * ds + up, p);
+            f[i] = Store<S>::load_c(F + (unsigned)i * ds + up);
           }
         } else {
-          f[i] = Store<S>::load(stage_pop<S>(smem, sh, st, lr, i, Q) + lz, p);
+          f[i] = Store<S>::load_c(stage_pop<S>(smem, sh, st, lr, i, Q) + lz);
         }
       }
     }
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kTmaThreads, TmaOccupancy<S, CL>::blocks)
     if (!valid) continue;
 
     C rho, u[3];
-    collide_cell<Q, C, CL>(f, p, rho, u);
+    collide_cell<Q, C, CL, Store<S>::kDev>(f, p, rho, u);
     if (p.write_macro) {
       const long long a = aidx(g, x, y, z);
       if (p.write_rho) rho_out[a] = rho;
