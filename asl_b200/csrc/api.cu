@@ -662,7 +662,7 @@ int aslb_lbgk_sync(aslb_lbgk* h) {
 
 int aslb_lbgk_set_kernel(aslb_lbgk* h, int variant) {
   ASLB_CHECK_HANDLE(h);
-  if (variant != 0 && variant != 1) return fail(ASLB_ERR_ARG, "aslb_lbgk_set_kernel: variant must be 0 or 1");
+  if (variant < 0 || variant > 2) return fail(ASLB_ERR_ARG, "aslb_lbgk_set_kernel: variant must be 0, 1 or 2");
   h->d.variant = variant;
   h->version++;
   return ASLB_OK;

@@ -67,22 +67,16 @@ __device__ __forceinline__ void store_slot(S* __restrict__ slot, typename Store<
   }
 }
 
-// Load, collide and store one cell. MASKED: apply the fused no-slip links
-// (bounce bits select the bounce-back slot, elide bits skip stores).
-template <int Q, class S, int CL, bool ODD, bool MASKED>
-__device__ __forceinline__ void cell_update(S* __restrict__ F, const GridDesc& g, const StepParams& p,
-                                            typename MacroT<S>::T* __restrict__ rho_out,
-                                            typename MacroT<S>::T* __restrict__ u_out, int x, int y, int z,
-                                            unsigned s, const int (&ox)[3], const int (&oy)[3], const int (&oz)[3],
-                                            uint32_t bounce, uint32_t elide) {
+// Gather the Q incoming populations of cell s. MASKED: bounce bits select
+// the bounce-back slot (this cell's own outgoing population: the upstream and
+// own slots swap roles between representations).
+template <int Q, class S, bool ODD, bool MASKED>
+__device__ __forceinline__ void cell_load(const S* __restrict__ F, unsigned ds, unsigned s, const int (&ox)[3],
+                                          const int (&oy)[3], const int (&oz)[3], uint32_t bounce,
+                                          typename Store<S>::C (&f)[Q]) {
   using Lt = Lattice<Q>;
-  using C = typename Store<S>::C;
-  const unsigned ds = (unsigned)g.dstride;
-  C f[Q];
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
-    // Upstream neighbour slot, or for a bounce-back link this cell's own
-    // outgoing population: the two slots swap roles between representations.
     const bool b = MASKED && ((bounce >> i) & 1u);
     unsigned idx;
     if (ODD) {
@@ -95,6 +89,19 @@ __device__ __forceinline__ void cell_update(S* __restrict__ F, const GridDesc& g
     }
     f[i] = Store<S>::load_c(F + idx);
   }
+}
+
+// Collide cell (x, y, z) at storage index s, write rho / u when asked, and
+// store the outgoing populations (elide bits keep the slot, store_slot).
+template <int Q, class S, int CL, bool ODD, bool MASKED>
+__device__ __forceinline__ void cell_finish(S* __restrict__ F, const GridDesc& g, const StepParams& p,
+                                            typename MacroT<S>::T* __restrict__ rho_out,
+                                            typename MacroT<S>::T* __restrict__ u_out, int x, int y, int z,
+                                            unsigned s, const int (&ox)[3], const int (&oy)[3], const int (&oz)[3],
+                                            uint32_t elide, typename Store<S>::C (&f)[Q]) {
+  using Lt = Lattice<Q>;
+  using C = typename Store<S>::C;
+  const unsigned ds = (unsigned)g.dstride;
   C rho, u[3];
   collide_cell<Q, C, CL, Store<S>::kDev>(f, p, rho, u);
   if (p.write_macro) {
@@ -127,7 +134,6 @@ template <int Q, class S, int CL, bool ODD, bool FUSED>
 __global__ void __launch_bounds__(256, StepOccupancy<Q, S, CL, FUSED>::blocks)
     k_stream_collide(S* __restrict__ F, const GridDesc g, const StepParams p,
                      typename MacroT<S>::T* __restrict__ rho_out, typename MacroT<S>::T* __restrict__ u_out) {
-  using Lt = Lattice<Q>;
   using C = typename Store<S>::C;
   const int z = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -144,7 +150,48 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, CL, FUSED>::blocks)
   }
   int ox[3], oy[3], oz[3];
   nb_offsets(g, x, y, z, ox, oy, oz);
-  cell_update<Q, S, CL, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, z, s, ox, oy, oz, bounce, elide);
+  C f[Q];
+  cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, s, ox, oy, oz, bounce, f);
+  cell_finish<Q, S, CL, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, z, s, ox, oy, oz, elide, f);
+}
+
+// Two cells per thread, z and z + 32 of the same row: a warp covers 64
+// consecutive cells, and each thread has the loads of both cells in flight
+// before it collides the first, which doubles the bytes in flight per
+// register-limited warp. Used for the plain (no closure) FP32/FP16 step of
+// D3Q15/D3Q19 domains with fused links, at three blocks (80 registers) per
+// SM; without fused links the schedule hoists every address of both cells
+// (over 128 registers) and the one-cell kernel is faster.
+template <int Q, class S, bool ODD, bool FUSED>
+__global__ void __launch_bounds__(256, 3)
+    k_stream_collide_pair(S* __restrict__ F, const GridDesc g, const StepParams p,
+                          typename MacroT<S>::T* __restrict__ rho_out, typename MacroT<S>::T* __restrict__ u_out) {
+  using C = typename Store<S>::C;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int za = blockIdx.x * (2 * blockDim.x) + 64 * w + lane + 1;
+  const int zb = za + 32;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int x = blockIdx.z + 1;
+  if (za > g.nz || y > g.ny) return;
+  const bool has_b = zb <= g.nz;
+  const unsigned ds = (unsigned)g.dstride;
+  const unsigned sa = (unsigned)sidx(g, x, y, za);
+  const unsigned sb = sa + 32u;
+  uint2 ma = make_uint2(0u, 0u), mb = make_uint2(0u, 0u);
+  if (FUSED) {
+    ma = p.mask[sa];
+    if (has_b) mb = p.mask[sb];
+  }
+  int ox[3], oy[3], oza[3], ozb[3];
+  nb_offsets(g, x, y, za, ox, oy, oza);
+  ozb[0] = -1;  // zb >= 33: the lower neighbour never wraps
+  ozb[1] = 0;
+  ozb[2] = ((g.periodic & 4) && zb == g.nz) ? -(g.nz - 1) : 1;
+  C fa[Q], fb[Q];
+  cell_load<Q, S, ODD, FUSED>(F, ds, sa, ox, oy, oza, ma.x, fa);
+  if (has_b) cell_load<Q, S, ODD, FUSED>(F, ds, sb, ox, oy, ozb, mb.x, fb);
+  cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, za, sa, ox, oy, oza, ma.y, fa);
+  if (has_b) cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, zb, sb, ox, oy, ozb, mb.y, fb);
 }
 
 inline void step_launch_shape(const GridDesc& g, dim3& grid, dim3& block) {
@@ -159,13 +206,32 @@ inline void step_launch_shape(const GridDesc& g, dim3& grid, dim3& block) {
 template <int Q, class S, int CL>
 cudaError_t step_tma(const DomainDev& d, const StepParams& p, int parity_in, cudaStream_t st);
 
+// Two-cells-per-thread shape: 32-thread groups cover 64 cells of a row.
+inline void pair_launch_shape(const GridDesc& g, dim3& grid, dim3& block) {
+  int tz = ((g.nz + 63) / 64) * 32;
+  if (tz > 128) tz = 128;
+  int ty = 256 / tz;
+  block = dim3(tz, ty, 1);
+  grid = dim3((g.nz + 2 * tz - 1) / (2 * tz), (g.ny + ty - 1) / ty, g.nx);
+}
+
 template <int Q, class S, int CL>
 cudaError_t step_q_s_cl(const DomainDev& d, const StepParams& p, int parity_in, cudaStream_t st) {
   if (d.variant == 1) return step_tma<Q, S, CL>(d, p, parity_in, st);
   dim3 grid, block;
-  step_launch_shape(d.g, grid, block);
   using M = typename MacroT<S>::T;
   const bool fused = p.mask != nullptr;
+  if constexpr (CL == CL_NONE && Q != 27 && !std::is_same<S, double>::value) {
+    if (d.variant == 0 && fused) {
+      pair_launch_shape(d.g, grid, block);
+      if (parity_in == 0)
+        k_stream_collide_pair<Q, S, true, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+      else
+        k_stream_collide_pair<Q, S, false, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+      return cudaGetLastError();
+    }
+  }
+  step_launch_shape(d.g, grid, block);
   if (parity_in == 0) {
     if (fused)
       k_stream_collide<Q, S, CL, true, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);

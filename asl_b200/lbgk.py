@@ -167,7 +167,8 @@ class LBGK:
         L.check(self.lib.aslb_lbgk_sync(self.h), "LBGK::sync")
 
     def setKernel(self, variant: int):
-        """0: direct-load stream-collide (default), 1: TMA-staged persistent kernel."""
+        """0: direct loads, two cells per thread where available (default);
+        1: TMA-staged persistent kernel; 2: direct loads, one cell per thread."""
         L.check(self.lib.aslb_lbgk_set_kernel(self.h, int(variant)), "LBGK::setKernel")
 
     @property

@@ -149,10 +149,12 @@ int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int us
 /* Wait for all work of the domain; fails with ASLB_ERR_STATE if a kernel's
  * bounded wait gave up. */
 int aslb_lbgk_sync(aslb_lbgk* h);
-/* Stream-collide kernel variant: 0 (default) is the one-cell-per-thread
- * kernel with direct loads; 1 stages every tile's population rows in shared
- * memory with asynchronous bulk copies (TMA) in a persistent, pipelined
- * kernel. Both give identical results. */
+/* Stream-collide kernel variant: 0 (default) loads directly, two cells per
+ * thread for the plain FP32/FP16 D3Q15/D3Q19 step with fused no-slip links
+ * (one cell per thread otherwise); 1 stages
+ * every tile's population rows in shared memory with asynchronous bulk copies
+ * (TMA) in a persistent, pipelined kernel; 2 loads directly, one cell per
+ * thread. All give identical results. */
 int aslb_lbgk_set_kernel(aslb_lbgk* h, int variant);
 int aslb_lbgk_get_kernel(aslb_lbgk* h);
 /* Steps taken so far. */

@@ -282,7 +282,7 @@ def test_fused_noslip_bitwise_equals_separate_condition(gpu, storage, case):
 
 
 @pytest.mark.parametrize("fuse", ["none", "walls", "map", "both"])
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 def test_unnormalised_map_matches_oracle(gpu, oracle_mod, fuse, variant):
     """A raw (unnormalised) distance map leaves solid cells below the -0.9999
     guard next to fluid; those links are not bounce-back and stream collided
@@ -342,11 +342,11 @@ def test_destroy_domain_before_its_conditions(gpu):
 @pytest.mark.parametrize("shape,periodic", [((6, 5, 300), (True, True, True)),    # two z segments, z wrap
                                             ((9, 7, 40), (False, True, True)),    # 4 rows per tile, partial group
                                             ((5, 3, 17), (True, False, False))])  # short rows
-def test_tma_kernel_bitwise_equals_direct_kernel(gpu, q, storage, shape, periodic):
+def test_kernel_variants_bitwise_equal(gpu, q, storage, shape, periodic):
     g = tuple(s + 2 for s in shape)
     rho, u = smooth_field(g, 3 + q)
     lbs = []
-    for variant in (0, 1):
+    for variant in (0, 1, 2):
         lb = A.LBGK(A.Block(shape), 0.03, VT[q], storage=storage, periodic=periodic, body_force=(1e-4, 0, 0))
         lb.setKernel(variant)
         A.LBGKUtilities(lb).initF(rho, u)
@@ -356,18 +356,20 @@ def test_tma_kernel_bitwise_equals_direct_kernel(gpu, q, storage, shape, periodi
     for lb, bcs in lbs:
         lb.run(7, bcs)
         lb.sync()
-    assert lbs[1][0].kernel == 1 and lbs[0][0].kernel == 0
-    assert np.array_equal(lbs[0][0].getF(), lbs[1][0].getF(), equal_nan=True)
-    assert np.array_equal(lbs[0][0].getVelocity(), lbs[1][0].getVelocity())
+    assert [lb.kernel for lb, _ in lbs] == [0, 1, 2]
+    for lb, _ in lbs[1:]:
+        assert np.array_equal(lbs[0][0].getF(), lb.getF(), equal_nan=True)
+        assert np.array_equal(lbs[0][0].getVelocity(), lb.getVelocity())
 
 
-def test_tma_kernel_fused_porous_bitwise(gpu):
+def test_kernel_variants_fused_porous_bitwise(gpu):
     w = W.porous_channel(size=(80, 40, 36), rmin=2.0, rmax=5.0, solid_fraction=0.35, steps=0)
     out = []
-    for variant in (0, 1):
+    for variant in (0, 1, 2):
         lb, bcs = W.build_lbgk(w, fuse=True)
         lb.setKernel(variant)
         lb.run(9, bcs)
         lb.sync()
         out.append(lb.getF())
     assert np.array_equal(out[0], out[1], equal_nan=True)
+    assert np.array_equal(out[0], out[2], equal_nan=True)
