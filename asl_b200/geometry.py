@@ -212,3 +212,26 @@ def rasterize_spheres(block, pack: SpherePack, periodic_x: bool = True, margin: 
             sub = m[x0:x1 + 1, y0:y1 + 1, z0:z1 + 1]
             np.minimum(sub, d, out=sub)
     return m
+
+
+def rasterize_union(block, shapes, margin: float = 2.0) -> np.ndarray:
+    """normalize(union of shapes, dx) on the ghosted block, evaluating each
+    shape only inside its bounding box grown by ``margin`` cells (outside it the
+    normalised distance is clipped to +1 anyway). ``shapes``: (df, lo, hi) with
+    lo / hi the physical corners of the shape's bounding box."""
+    gx, gy, gz = block.ghosted
+    m = np.ones((gx, gy, gz), dtype=np.float32)
+    dx = float(block.dx)
+    for df, lo, hi in shapes:
+        nd = normalize(df, dx)
+        idx_lo = [max(int(math.floor((lo[a] - block.position[a]) / dx - margin)) + 1, 0) for a in range(3)]
+        idx_hi = [min(int(math.ceil((hi[a] - block.position[a]) / dx + margin)) + 1, (gx, gy, gz)[a] - 1)
+                  for a in range(3)]
+        if any(idx_lo[a] > idx_hi[a] for a in range(3)):
+            continue
+        axes = [np.float32(block.position[a]) + (np.arange(idx_lo[a], idx_hi[a] + 1, dtype=np.float32)
+                                                 - np.float32(1.0)) * np.float32(dx) for a in range(3)]
+        pos = np.stack(np.meshgrid(*axes, indexing="ij")).astype(np.float32)
+        sub = m[idx_lo[0]:idx_hi[0] + 1, idx_lo[1]:idx_hi[1] + 1, idx_lo[2]:idx_hi[2] + 1]
+        np.minimum(sub, nd.distance(pos), out=sub)
+    return m

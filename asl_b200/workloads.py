@@ -9,7 +9,10 @@ generated from a seed (base seed 20261203, configuration k uses seed + k).
   porous_channel    D3Q19 512x256x256, non-overlapping random spheres
                     (r ~ U[4,12], solid fraction 0.4), periodic in x, no-slip
                     Y/Z walls, body force g=1e-6 along x, tau=0.6.
-  (the batched, turbulence and D3Q27 vehicle cases live beside their drivers)
+  vehicle_d3q27     D3Q27 768x384x384 wind tunnel, 12 seeded boxes / vertical
+                    cylinders standing on the floor (Z0), velocity 0.05 along x
+                    at the inlet (X0), the far field (Y0, YE, ZE) and the moving
+                    floor (Z0), pressure 1 at the outlet (XE), tau=0.51.
 """
 from __future__ import annotations
 
@@ -121,3 +124,38 @@ def build_lbgk(w: Workload, storage="f32", compVel=True, compRho=True, closure_c
 
 WALL_BITS = {"X0": 1, "XE": 2, "Y0": 4, "YE": 8, "Z0": 16, "ZE": 32}
 SLICE_KIND = {"noslip": 0, "velocity": 1, "pressure": 2, "pressure_velocity": 3}
+
+
+def vehicle_d3q27(size=(768, 384, 384), u_in=0.05, tau=0.51, n_obstacles=12, steps=10000,
+                  seed=BASE_SEED + 5) -> Workload:
+    """Bluff bodies on a moving floor: boxes (even k) and vertical cylinders
+    (odd k) with seeded positions and sizes, all resting on the floor, in the
+    upstream half of the tunnel."""
+    from .lbgk import Block
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = size
+    block = Block(size, 1.0)
+    shapes = []
+    for k in range(n_obstacles):
+        cx = rng.uniform(0.15, 0.55) * nx
+        cy = rng.uniform(0.2, 0.8) * ny
+        if k % 2 == 0:
+            h = np.array([rng.uniform(0.02, 0.05) * nx, rng.uniform(0.03, 0.08) * ny, rng.uniform(0.06, 0.2) * nz])
+            c = np.array([cx, cy, h[2] - 0.5])  # bottom face half a cell below the first interior layer
+            shapes.append((G.generateDFBox(c, h), c - h, c + h))
+        else:
+            r = rng.uniform(0.02, 0.05) * ny
+            hgt = rng.uniform(0.1, 0.3) * nz
+            c = np.array([cx, cy, hgt / 2 - 0.5])
+            shapes.append((G.generateDFCylinder(r, (0.0, 0.0, hgt), c), c - np.array([r, r, hgt / 2]),
+                           c + np.array([r, r, hgt / 2])))
+    m = G.rasterize_union(block, shapes)
+    nu = (tau - 0.5) / 3.0
+    u = (u_in, 0.0, 0.0)
+    bcs = [BCSpec("velocity", ("X0", "Y0", "YE", "ZE", "Z0"), u=u),
+           BCSpec("pressure", ("XE",), p=1.0),
+           BCSpec("map_noslip")]
+    solid = float((m[1:-1, 1:-1, 1:-1] <= 0).mean())
+    return Workload("vehicle_d3q27_%dx%dx%d" % tuple(size), tuple(size), 27, nu, bcs=bcs, map=m, steps=steps,
+                    init_u=u, info={"obstacles": n_obstacles, "solid_fraction": solid, "seed": seed, "tau": tau,
+                                    "u_in": u_in})

@@ -46,6 +46,11 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp16", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=20)
+    ap.add_argument("--accuracy-steps", type=int, default=5000,
+                    help="steps of the FP16/FP32-against-FP64 accuracy study (0: skip)")
+    ap.add_argument("--q27-steps", type=int, default=400,
+                    help="timed steps of the D3Q27 vehicle workload (0: skip)")
+    ap.add_argument("--q27-size", default="768,384,384")
     return ap.parse_args()
 
 
@@ -186,6 +191,88 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+def storage_accuracy(W, w, steps: int):
+    """The porous channel advanced `steps` steps with FP64, FP32 and FP16
+    storage (fused no-slip, CUDA graph). FP64 is the reference (the GPU FP64
+    kernel matches the FP64 CPU oracle to 1e-12 in the tests). Reports the
+    permeability k = nu <u_x> / g (superficial velocity: solid cells count as
+    zero) and the relative L2 error of u over the fluid cells."""
+    import numpy as np
+    g = w.body_force[0]
+    fluid = w.map[1:-1, 1:-1, 1:-1] > 0
+    out = {"steps": steps, "reference": "FP64 storage on the GPU", "permeability": {}, "permeability_rel_err": {},
+           "velocity_rel_l2": {}, "ms_per_step": {}}
+    ref = None
+    for storage in ("f64", "f32", "f16"):
+        import torch
+        lb, bcs = W.build_lbgk(w, storage=storage, compVel=False, compRho=False, fuse=True)
+        st = torch.cuda.ExternalStream(lb.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        lb.run(steps - 1, bcs, use_graph=True)
+        lb.requestMacro()
+        lb.run(1, bcs)
+        e1.record(st)
+        e1.synchronize()
+        u = lb.getVelocity(np.float64)[:, 1:-1, 1:-1, 1:-1][:, fluid]
+        del lb, bcs
+        k = w.nu * float(u[0].sum()) / fluid.size / g
+        out["permeability"][storage] = k
+        out["ms_per_step"][storage] = e0.elapsed_time(e1) / steps
+        if ref is None:
+            ref = (u, k)
+        else:
+            out["permeability_rel_err"][storage] = abs(k - ref[1]) / abs(ref[1])
+            out["velocity_rel_l2"][storage] = float(np.sqrt(((u - ref[0]) ** 2).sum() / (ref[0] ** 2).sum()))
+    out["unit"] = "lattice units (dx = 1)"
+    return out
+
+
+def vehicle_run(W, size, steps: int, peak: float):
+    """D3Q27 vehicle-like channel (seeded boxes and cylinders on the floor):
+    MLUPS of the full step (inlet / far-field / moving-floor velocity
+    conditions, outlet pressure, fused no-slip obstacles) and a drag / lift
+    series from the surface force on the obstacles."""
+    import numpy as np
+    import torch
+    w = W.vehicle_d3q27(size=size, steps=steps)
+    lb, bcs = W.build_lbgk(w, storage="f32", compVel=False, compRho=False, fuse=True)
+    from asl_b200 import lbgk as A
+    force = A.generateComputeSurfaceForce(lb, w.map)
+    st = torch.cuda.ExternalStream(lb.stream)
+    lb.run(4, bcs, use_graph=True)
+    lb.sync()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    lb.run(steps, bcs, use_graph=True)
+    e1.record(st)
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    nk = 20
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0.record(st)
+    lb.execute(nk)
+    k1.record(st)
+    k1.synchronize()
+    tk = k0.elapsed_time(k1) / 1e3 / nk
+    series = []
+    every = max(1, steps // 8)
+    for n in range(8):
+        lb.run(every, bcs, use_graph=True)
+        fx = force.execute()
+        series.append([int(lb.steps), float(fx[0]), float(fx[2])])
+    nonslip = sum(b.kernels for b in bcs)
+    bpc = BYTES_PER_CELL[("f32", 27)]
+    res = {"workload": w.name, "cells": w.cells, "steps": steps, "value": w.cells * steps / t / 1e6,
+           "unit": "MLUPS", "ms_per_step": t / steps * 1e3, "kernel_ms": tk * 1e3,
+           "kernel_frac_of_peak": bpc * w.cells / tk / 1e9 / peak, "boundary_kernels_per_step": nonslip,
+           "obstacles": w.info["obstacles"], "drag_lift_series": series,
+           "series_columns": ["step", "drag (sum F_x)", "lift (sum F_z)"]}
+    del force, lb, bcs
+    return res
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -307,6 +394,13 @@ def run_ours(args):
         fp16["storage"] = "(f - 1) * 1024 in FP16, FP32 arithmetic"
         del lb, bcs
 
+    accuracy = None
+    if world == 1 and args.accuracy_steps > 0:
+        accuracy = storage_accuracy(W, w, args.accuracy_steps)
+    vehicle = None
+    if world == 1 and args.q27_steps > 0:
+        vehicle = vehicle_run(W, parse_size(args.q27_size), args.q27_steps, peak)
+
     bpc = BYTES_PER_CELL[(args.storage, w.q)]
     achieved = bpc * w.cells / tk / 1e9
     traffic = profile_traffic(f"stream_collide_d3q19_{args.storage}_porous.md", w.cells)
@@ -334,8 +428,8 @@ def run_ours(args):
                            "time_loop": "CUDA graph of two steps, replayed"},
                 "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "clocks": clk,
                 "gpu_launches": K * head["launches_per_step"],
-                "separate_conditions": sep, "tma_kernel": direct, "fp16": fp16, "finite": finite,
-                "mass": mom[0]}
+                "separate_conditions": sep, "tma_kernel": direct, "fp16": fp16, "accuracy": accuracy,
+                "d3q27_vehicle": vehicle, "finite": finite, "mass": mom[0]}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

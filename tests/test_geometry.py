@@ -66,3 +66,24 @@ def test_rasterized_spheres_match_direct_union():
             df = s if df is None else (df | s)
     direct = G.initData(b, G.normalize(df, 1.0))
     assert np.abs(fast - direct).max() < 1e-5
+
+
+def test_rasterized_union_matches_direct_union():
+    b = Block((30, 20, 16))
+    shapes = [(G.generateDFBox((8.0, 6.0, 3.5), (3.0, 2.0, 4.0)), (5.0, 4.0, -0.5), (11.0, 8.0, 7.5)),
+              (G.generateDFCylinder(2.5, (0.0, 0.0, 6.0), (20.0, 12.0, 2.5)), (17.5, 9.5, -0.5), (22.5, 14.5, 5.5))]
+    fast = G.rasterize_union(b, shapes)
+    direct = G.initData(b, G.normalize(shapes[0][0] | shapes[1][0], 1.0))
+    assert np.abs(fast - direct).max() < 1e-6
+
+
+def test_vehicle_workload_is_seeded_and_on_the_floor():
+    from asl_b200 import workloads as W
+    a = W.vehicle_d3q27(size=(96, 48, 48))
+    b = W.vehicle_d3q27(size=(96, 48, 48))
+    assert np.array_equal(a.map, b.map) and a.q == 27
+    solid = a.map[1:-1, 1:-1, 1:-1] <= 0
+    assert 0.002 < solid.mean() < 0.1
+    # every obstacle stands on the floor: solid cells in the first layer, none at the top
+    assert solid[:, :, 0].any() and not solid[:, :, -1].any()
+    assert [s.kind for s in a.bcs] == ["velocity", "pressure", "map_noslip"]
