@@ -77,6 +77,11 @@ PROTOTYPES = {
     "aslb_force_compute": (C.c_int, [_vp, _pd, _pf, _pd]),
     "aslb_force_destroy": (C.c_int, [_vp]),
     "aslb_force_compute_noalloc": (C.c_int, [_vp, _pd, _pd]),
+    "aslb_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(_vp)]),
+    "aslb_batch_run": (C.c_int, [_vp, C.c_int, C.POINTER(_vp), C.POINTER(C.c_int), C.c_int]),
+    "aslb_batch_sync": (C.c_int, [_vp]),
+    "aslb_batch_tiles": (C.c_longlong, [_vp]),
+    "aslb_batch_destroy": (C.c_int, [_vp]),
     "aslb_geom_pack_spheres": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                          C.c_ulonglong, C.c_int, C.c_int, C.c_int, _pd, _pd, C.POINTER(C.c_int)]),
 }

@@ -66,6 +66,7 @@ struct aslb_lbgk {
   // releases their device memory and detaches them (any destruction order)
   std::vector<aslb_bc*> bcs;
   std::vector<aslb_force*> forces;
+  std::vector<aslb_batch*> batches;  // batches this domain belongs to
 };
 
 struct aslb_bc {
@@ -388,10 +389,13 @@ int aslb_lbgk_create(int nx, int ny, int nz, int q, int storage, double nu, unsi
   return ASLB_OK;
 }
 
+void batch_detach(aslb_batch* b, aslb_lbgk* h);
+
 int aslb_lbgk_destroy(aslb_lbgk* h) {
   if (!h) return ASLB_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
   drop_graph(h);
+  for (aslb_batch* b : std::vector<aslb_batch*>(h->batches)) batch_detach(b, h);
   for (aslb_bc* bc : h->bcs) {
     cudaFree(bc->anchors);
     cudaFree(bc->dlinks);
@@ -1101,5 +1105,343 @@ extern "C" int aslb_force_compute_noalloc(aslb_force* fc, const double r0[3], do
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess)
     return fail(ASLB_ERR_CUDA, std::string("aslb_force_compute_noalloc: ") + cudaGetErrorString(e));
+  return ASLB_OK;
+}
+
+// ---- batches of independent domains -----------------------------------------
+
+struct aslb_batch {
+  std::vector<aslb_lbgk*> doms;
+  bool detached = false;  // a member domain was destroyed
+  int q = 0, storage = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  // device tables
+  std::vector<BatchDom> host_doms;
+  BatchDom* dev_doms = nullptr;
+  long long ntiles = 0;
+  bool any_mask = false;
+  std::vector<BatchBc*> dev_pos;  // one table per condition position
+  std::vector<int> pos_n;
+  std::vector<long long> pos_links;
+  std::vector<aslb_bc*> key;      // conditions the tables were built for
+  std::vector<int> key_n;
+  long long table_version = -1;   // sum of the domains' versions at build
+  // time-loop graph
+  cudaGraphExec_t graph = nullptr;
+  int graph_parity = -1;
+  long long graph_version = -1;
+};
+
+void batch_detach(aslb_batch* b, aslb_lbgk* h) {
+  for (auto& d : b->doms)
+    if (d == h) d = nullptr;
+  b->detached = true;
+  auto& v = h->batches;
+  v.erase(std::remove(v.begin(), v.end(), b), v.end());
+}
+
+namespace {
+
+void batch_free_tables(aslb_batch* b) {
+  cudaFree(b->dev_doms);
+  b->dev_doms = nullptr;
+  for (BatchBc* t : b->dev_pos) cudaFree(t);
+  b->dev_pos.clear();
+  b->pos_n.clear();
+  b->pos_links.clear();
+}
+
+void batch_drop_graph(aslb_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+  b->graph_parity = -1;
+}
+
+long long batch_version(const aslb_batch* b) {
+  long long v = 0;
+  for (const aslb_lbgk* h : b->doms) v += h->version;
+  return v;
+}
+
+// (Re)build the domain table and one link table per condition position.
+int batch_tables(aslb_batch* b, aslb_bc* const* bcs, const int* nbc) {
+  batch_free_tables(b);
+  const int n = (int)b->doms.size();
+  b->host_doms.assign(n, BatchDom{});
+  b->ntiles = 0;
+  b->any_mask = false;
+  for (int i = 0; i < n; ++i) {
+    aslb_lbgk* h = b->doms[i];
+    BatchDom& D = b->host_doms[i];
+    const GridDesc& g = h->d.g;
+    D.g = g;
+    D.F = h->d.F;
+    D.mask = h->fresh ? nullptr : h->mask_dev;
+    b->any_mask |= D.mask != nullptr;
+    D.rho = h->d.rho;
+    D.u = h->d.u;
+    D.om0f = 1.0f / (3.0f * (float)h->p.nu + 0.5f);
+    D.om0d = 1.0 / (3.0 * h->p.nu + 0.5);
+    D.row_tiles = (int)(((long long)g.ny * g.nz + 255) / 256);
+    D.nz_inv = (unsigned)((0x100000000ULL + (unsigned long long)g.nz - 1) / (unsigned long long)g.nz);
+    D.tile0 = b->ntiles;
+    b->ntiles += (long long)g.nx * D.row_tiles;
+  }
+  ASLB_CUDA(cudaMalloc((void**)&b->dev_doms, n * sizeof(BatchDom)));
+  ASLB_CUDA(cudaMemcpy(b->dev_doms, b->host_doms.data(), n * sizeof(BatchDom), cudaMemcpyHostToDevice));
+  // condition positions: the j-th separate condition of every domain
+  std::vector<std::vector<BatchBc>> pos;
+  std::vector<long long> pos_total;
+  int off = 0;
+  for (int i = 0; i < n; ++i) {
+    int j = 0;
+    for (int c = 0; c < nbc[i]; ++c) {
+      aslb_bc* bc = bcs[off + c];
+      if (bc->fused) continue;
+      if ((int)pos.size() <= j) {
+        pos.resize(j + 1);
+        pos_total.resize(j + 1, 0);
+      }
+      if (bc->nd > 0) {
+        BatchBc e{};
+        e.F = b->doms[i]->d.F;
+        e.dstride = b->doms[i]->d.g.dstride;
+        e.links = bc->dlinks;
+        e.ls = bc->ls;
+        e.bp = bc->bp;
+        e.link0 = pos_total[j];
+        pos_total[j] += bc->nd;
+        pos[j].push_back(e);
+      }
+      ++j;
+    }
+    off += nbc[i];
+  }
+  for (size_t j = 0; j < pos.size(); ++j) {
+    const auto& v = pos[j];
+    BatchBc* t = nullptr;
+    const long long links = pos_total[j];
+    if (!v.empty()) {
+      ASLB_CUDA(cudaMalloc((void**)&t, v.size() * sizeof(BatchBc)));
+      ASLB_CUDA(cudaMemcpy(t, v.data(), v.size() * sizeof(BatchBc), cudaMemcpyHostToDevice));
+    }
+    b->dev_pos.push_back(t);
+    b->pos_n.push_back((int)v.size());
+    b->pos_links.push_back(links);
+  }
+  b->table_version = batch_version(b);
+  return ASLB_OK;
+}
+
+// One step of every domain: the batched stream-collide, then each condition
+// position in order (ASL's order within every domain).
+int batch_step(aslb_batch* b) {
+  aslb_lbgk* h0 = b->doms[0];
+  prepare_params(h0);
+  const int parity = h0->parity;
+  cudaError_t e = launch_batch_step(b->q, b->storage, b->dev_doms, (int)b->doms.size(), b->ntiles, b->any_mask,
+                                    h0->p, parity, b->stream);
+  for (size_t j = 0; e == cudaSuccess && j < b->dev_pos.size(); ++j)
+    if (b->pos_n[j] > 0)
+      e = launch_batch_links(b->q, b->storage, b->dev_pos[j], b->pos_n[j], b->pos_links[j], parity ^ 1, b->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("batch step: ") + cudaGetErrorString(e));
+  for (aslb_lbgk* h : b->doms) {
+    h->parity ^= 1;
+    h->steps += 1;
+    if (h->macro_once) {
+      h->macro_once = false;
+      h->version++;
+    }
+  }
+  return ASLB_OK;
+}
+
+}  // namespace
+
+int aslb_batch_create(aslb_lbgk* const* domains, int n, aslb_batch** out) {
+  if (!out || !domains || n <= 0) return fail(ASLB_ERR_ARG, "aslb_batch_create: bad arguments");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    aslb_lbgk* h = domains[i];
+    if (!h) return fail(ASLB_ERR_ARG, "aslb_batch_create: null domain");
+    for (int j = 0; j < i; ++j)
+      if (domains[j] == h) return fail(ASLB_ERR_ARG, "aslb_batch_create: a domain appears twice");
+    if (h->d.q != domains[0]->d.q || h->d.storage != domains[0]->d.storage)
+      return fail(ASLB_ERR_ARG, "aslb_batch_create: domains differ in lattice or storage");
+    if (h->device != domains[0]->device) return fail(ASLB_ERR_ARG, "aslb_batch_create: domains on different devices");
+  }
+  aslb_batch* b = new aslb_batch();
+  b->doms.assign(domains, domains + n);
+  b->q = domains[0]->d.q;
+  b->storage = domains[0]->d.storage;
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return fail(ASLB_ERR_CUDA, std::string("aslb_batch_create: ") + cudaGetErrorString(e));
+  }
+  for (aslb_lbgk* h : b->doms) h->batches.push_back(b);
+  *out = b;
+  return ASLB_OK;
+}
+
+int aslb_batch_run(aslb_batch* b, int nsteps, aslb_bc* const* bcs, const int* nbc, int use_graph) {
+  ASLB_CHECK_HANDLE(b);
+  if (b->detached) return fail(ASLB_ERR_STATE, "aslb_batch_run: a domain of the batch was destroyed");
+  const int n = (int)b->doms.size();
+  if (nsteps < 0 || !nbc) return fail(ASLB_ERR_ARG, "aslb_batch_run: bad arguments");
+  // every domain must step like the first one: same parity, closure and
+  // batch-wide parameters (only the viscosity, geometry and conditions differ)
+  aslb_lbgk* h0 = b->doms[0];
+  int total = 0;
+  for (int i = 0; i < n; ++i) {
+    aslb_lbgk* h = b->doms[i];
+    if (nbc[i] < 0) return fail(ASLB_ERR_ARG, "aslb_batch_run: negative condition count");
+    if (h->parity != h0->parity) return fail(ASLB_ERR_STATE, "aslb_batch_run: domains are at different parities");
+    if (h->closure != CL_NONE) return fail(ASLB_ERR_ARG, "aslb_batch_run: batches run the plain BGK collision only");
+    if (h->p.compressible != h0->p.compressible || h->p.has_force != h0->p.has_force ||
+        h->p.has_coriolis != h0->p.has_coriolis || h->p.scale != h0->p.scale || h->comp_vel != h0->comp_vel ||
+        h->comp_rho != h0->comp_rho || h->macro_once != h0->macro_once ||
+        std::memcmp(h->p.g, h0->p.g, sizeof(h->p.g)) != 0 || std::memcmp(h->p.Om, h0->p.Om, sizeof(h->p.Om)) != 0)
+      return fail(ASLB_ERR_ARG, "aslb_batch_run: domains differ in a batch-wide parameter (body force, rotation, "
+                                "compressibility, FP16 scale or output fields)");
+    for (int c = 0; c < nbc[i]; ++c) {
+      aslb_bc* bc = bcs ? bcs[total + c] : nullptr;
+      if (!bc || bc->h != h) return fail(ASLB_ERR_ARG, "aslb_batch_run: condition of another domain");
+      if (c > 0 && bcs[total + c - 1]->fused && !bc->fused)
+        return fail(ASLB_ERR_ARG, "aslb_batch_run: fused conditions must come after all separate ones");
+      if (!bc->fused && bc->n > 0)
+        return fail(ASLB_ERR_ARG, "aslb_batch_run: velocity maps and links across periodic faces are not batched");
+    }
+    total += nbc[i];
+  }
+  std::vector<aslb_bc*> key(bcs, bcs + total);
+  std::vector<int> key_n(nbc, nbc + n);
+  // the batch's stream follows every domain's pending work
+  for (aslb_lbgk* h : b->doms) {
+    ASLB_CUDA(cudaEventRecord(b->ev, h->stream));
+    ASLB_CUDA(cudaStreamWaitEvent(b->stream, b->ev, 0));
+  }
+  auto refresh = [&]() -> int {
+    if (b->key == key && b->key_n == key_n && b->table_version == batch_version(b)) return ASLB_OK;
+    ASLB_CUDA(cudaStreamSynchronize(b->stream));
+    batch_drop_graph(b);
+    int r = batch_tables(b, bcs, nbc);
+    if (r) return r;
+    b->key = key;
+    b->key_n = key_n;
+    return ASLB_OK;
+  };
+  // after the first step every fused condition has run: incoming slots are no
+  // longer the initial values, the fused links take effect
+  auto after_step = [&]() {
+    int off = 0;
+    for (int i = 0; i < n; ++i) {
+      aslb_lbgk* h = b->doms[i];
+      for (int c = 0; c < nbc[i]; ++c)
+        if (bcs[off + c]->fused && h->fresh) {
+          h->fresh = false;
+          h->version++;
+        }
+      off += nbc[i];
+    }
+  };
+  auto eager = [&](int k) -> int {
+    for (int s = 0; s < k; ++s) {
+      int r = refresh();
+      if (r) return r;
+      r = batch_step(b);
+      if (r) return r;
+      after_step();
+    }
+    return ASLB_OK;
+  };
+  int done = 0, r = ASLB_OK;
+  bool fresh = false;
+  for (aslb_lbgk* h : b->doms) fresh |= h->fresh || h->macro_once;
+  if (!use_graph || nsteps < 2) {
+    r = eager(nsteps);
+    done = nsteps;
+  } else {
+    if (fresh) {
+      r = eager(1);
+      done = 1;
+    }
+    if (!r) r = refresh();
+    if (!r && !(b->graph && b->graph_version == batch_version(b) && b->graph_parity == h0->parity)) {
+      if (b->graph && b->graph_version == batch_version(b) && done < nsteps) {
+        // graph of the other parity: one eager step realigns
+        r = eager(1);
+        done += 1;
+      }
+      if (!r && !(b->graph && b->graph_version == batch_version(b) && b->graph_parity == h0->parity)) {
+        batch_drop_graph(b);
+        std::vector<int> par(n);
+        std::vector<long long> st(n);
+        for (int i = 0; i < n; ++i) {
+          par[i] = b->doms[i]->parity;
+          st[i] = b->doms[i]->steps;
+        }
+        cudaGraph_t graph = nullptr;
+        ASLB_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        int rr = batch_step(b);
+        if (!rr) rr = batch_step(b);
+        cudaError_t ce = cudaStreamEndCapture(b->stream, &graph);
+        for (int i = 0; i < n; ++i) {  // capture enqueued nothing
+          b->doms[i]->parity = par[i];
+          b->doms[i]->steps = st[i];
+        }
+        if (rr) {
+          if (graph) cudaGraphDestroy(graph);
+          return rr;
+        }
+        if (ce != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&b->graph, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) {
+          b->graph = nullptr;
+          return fail(ASLB_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(ce));
+        }
+        b->graph_parity = h0->parity;
+        b->graph_version = batch_version(b);
+      }
+    }
+    if (!r) {
+      const int pairs = (nsteps - done) / 2;
+      for (int i = 0; i < pairs; ++i) ASLB_CUDA(cudaGraphLaunch(b->graph, b->stream));
+      for (aslb_lbgk* h : b->doms) h->steps += 2LL * pairs;
+      done += 2 * pairs;
+      r = eager(nsteps - done);
+    }
+  }
+  // every domain's later work follows the batch
+  ASLB_CUDA(cudaEventRecord(b->ev, b->stream));
+  for (aslb_lbgk* h : b->doms) ASLB_CUDA(cudaStreamWaitEvent(h->stream, b->ev, 0));
+  return r;
+}
+
+int aslb_batch_sync(aslb_batch* b) {
+  ASLB_CHECK_HANDLE(b);
+  ASLB_CUDA(cudaStreamSynchronize(b->stream));
+  return ASLB_OK;
+}
+
+long long aslb_batch_tiles(aslb_batch* b) { return b ? b->ntiles : -1; }
+
+int aslb_batch_destroy(aslb_batch* b) {
+  if (!b) return ASLB_OK;
+  cudaStreamSynchronize(b->stream);
+  batch_drop_graph(b);
+  batch_free_tables(b);
+  for (aslb_lbgk* h : b->doms)
+    if (h) {
+      auto& v = h->batches;
+      v.erase(std::remove(v.begin(), v.end(), b), v.end());
+    }
+  cudaEventDestroy(b->ev);
+  cudaStreamDestroy(b->stream);
+  delete b;
   return ASLB_OK;
 }

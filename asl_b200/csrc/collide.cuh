@@ -116,11 +116,19 @@ __device__ __forceinline__ C par_cs(const StepParams& p) {
   if constexpr (std::is_same<C, double>::value) return p.cs; else return p.csf;
 }
 
+// omega = 1 / (3 nu + 1/2), evaluated on the host in the storage's arithmetic
+template <class C>
+__device__ __forceinline__ C step_omega(const StepParams& p) {
+  if constexpr (std::is_same<C, double>::value) return p.om0d; else return p.om0f;
+}
+
 // f: the Q values of one cell in the collision representation (f, or
 // D = (f - 1) sigma when DEV), replaced by the post-collision values.
+// om0: the BGK relaxation rate (step_omega, or a batch domain's own).
 // rho_out / u_out: density and velocity (ASL's compRho / compVel fields).
 template <int Q, class C, int CL, bool DEV = false>
-__device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, C& rho_out, C (&u_out)[3]) {
+__device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, const C om0, C& rho_out,
+                                             C (&u_out)[3]) {
   using Lt = Lattice<Q>;
   using Pr = Pairs<Q>;
   // ---- moments: pair sums and differences, per weight class
@@ -165,8 +173,6 @@ __device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, C& 
   const C isig = DEV ? C(p.inv_scale) : C(1);
   const C rho = DEV ? fma_(V, isig, C(1)) : V;
 
-  // omega = 1 / (3 nu + 1/2), evaluated on the host in the storage's arithmetic
-  const C om0 = std::is_same<C, double>::value ? C(p.om0d) : C(p.om0f);
   C om = om0;
   if (p.has_coriolis) {
     // component-sequential, as ACL emits `momentum += (2/w) Omega x momentum`

@@ -4,6 +4,7 @@
 // with its FP64 reduction, and global moments.
 #include <type_traits>
 #include "kernels.h"
+#include "bc_links.cuh"
 #include "stream_collide.cuh"
 
 namespace aslb {
@@ -194,24 +195,6 @@ cudaError_t launch_import_f(const DomainDev& d, const StepParams& p, const void*
 // Within one boundary condition no OUT slot is an IN slot (IN belongs to a
 // ghost/solid cell, OUT to a fluid cell), so links run in parallel; separate
 // boundary conditions run in the user's order, later writers winning as in ASL.
-template <class S>
-struct BcArith {
-  using C = typename Store<S>::C;
-  static constexpr bool kDev = std::is_same<S, __half>::value;
-  // value of f, in the arithmetic the storage keeps exact (deviation for FP16)
-  __device__ static __forceinline__ C get(const S* p, const BcParams& bp) {
-    return kDev ? Store<S>::dev(p, bp.inv_scale) : Store<S>::val(p, bp.inv_scale);
-  }
-  __device__ static __forceinline__ void put(S* p, C v, const BcParams& bp) {
-    if (kDev)
-      Store<S>::set_dev(p, v, bp.scale);
-    else
-      Store<S>::set_val(p, v, bp.scale);
-  }
-  // representation of a constant population value P (absolute) in get/put arithmetic
-  __device__ static __forceinline__ C rep(C v) { return kDev ? v - C(1) : v; }
-};
-
 template <int Q, class S>
 __global__ void __launch_bounds__(256) k_bc(S* __restrict__ F, const GridDesc g, const int4* __restrict__ anchors,
                                             int n, const BcParams bp, int parity) {
@@ -320,37 +303,9 @@ cudaError_t launch_bc(const DomainDev& d, const int4* anchors, int n, const BcPa
 template <int Q, class S>
 __global__ void __launch_bounds__(256) k_bc_links(S* __restrict__ F, const GridDesc g, const int* __restrict__ links,
                                                   int n, const LinkSet ls, const BcParams bp, int parity) {
-  using C = typename Store<S>::C;
-  using A = BcArith<S>;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  int k = 1;
-  while (t >= ls.seg[k + 1]) ++k;
-  const int wa = links[t];
-  const int wq = wa + ls.off[k];
-  const int kb = ls.inv[k];
-  S* in;
-  S* out;
-  if (parity == 0) {
-    in = F + (size_t)k * g.dstride + wa;
-    out = F + (size_t)kb * g.dstride + wq;
-  } else {
-    in = F + (size_t)kb * g.dstride + wq;
-    out = F + (size_t)k * g.dstride + wa;
-  }
-  const C v = std::is_same<C, double>::value ? C(ls.vald[k]) : C(ls.val[k]);
-  switch (bp.kind) {
-    case BCK_NOSLIP:
-    case BCK_MAP_NOSLIP:
-      *in = *out;
-      break;
-    case BCK_VELOCITY:
-      A::put(in, A::get(out, bp) + v, bp);
-      break;
-    default:  // pressure, pressure + velocity, equilibrium: a constant per direction
-      A::put(in, A::rep(v), bp);
-      break;
-  }
+  link_apply<Q, S>(F, g.dstride, links, t, ls, bp, parity);
 }
 
 template <int Q, class S>

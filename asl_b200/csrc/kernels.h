@@ -54,4 +54,36 @@ cudaError_t launch_moments(const DomainDev& d, const StepParams& p, int parity, 
 // Sum `nblocks` rows of `width` doubles into out (fixed order, one block).
 cudaError_t launch_reduce_rows(const double* partials, int nblocks, int width, double* out, cudaStream_t st);
 
+
+// ---- batches of independent domains ----------------------------------------
+// One entry per domain of a batch (device table, ordered by tile0).
+struct BatchDom {
+  GridDesc g;
+  void* F;
+  const uint2* mask;  // fused links, or null
+  void* rho;
+  void* u;
+  float om0f;
+  double om0d;
+  int row_tiles;     // 256-cell tiles per x plane: ceil(ny * nz / 256)
+  unsigned nz_inv;   // ceil(2^32 / nz): y = l / nz by a multiply-high
+  long long tile0;   // first tile of this domain in the batch
+};
+// One entry per (domain, condition) of a batched link launch (ordered by link0).
+struct BatchBc {
+  void* F;
+  long long dstride;
+  const int* links;
+  long long link0;  // first link of this entry in the launch
+  LinkSet ls;
+  BcParams bp;
+};
+// One stream-collide step of every domain of a batch (same lattice, storage
+// and parity; CL_NONE), a persistent grid over all domains' tiles.
+cudaError_t launch_batch_step(int q, int storage, const BatchDom* doms, int ndom, long long ntiles, bool fused,
+                              const StepParams& p, int parity_in, cudaStream_t st);
+// Every link of the entries (one condition position across the batch).
+cudaError_t launch_batch_links(int q, int storage, const BatchBc* bcs, int nbc, long long nlinks, int parity,
+                               cudaStream_t st);
+
 }  // namespace aslb

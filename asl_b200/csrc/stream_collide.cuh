@@ -98,12 +98,13 @@ __device__ __forceinline__ void cell_finish(S* __restrict__ F, const GridDesc& g
                                             typename MacroT<S>::T* __restrict__ rho_out,
                                             typename MacroT<S>::T* __restrict__ u_out, int x, int y, int z,
                                             unsigned s, const int (&ox)[3], const int (&oy)[3], const int (&oz)[3],
-                                            uint32_t elide, typename Store<S>::C (&f)[Q]) {
+                                            uint32_t elide, typename Store<S>::C (&f)[Q],
+                                            typename Store<S>::C om0) {
   using Lt = Lattice<Q>;
   using C = typename Store<S>::C;
   const unsigned ds = (unsigned)g.dstride;
   C rho, u[3];
-  collide_cell<Q, C, CL, Store<S>::kDev>(f, p, rho, u);
+  collide_cell<Q, C, CL, Store<S>::kDev>(f, p, om0, rho, u);
   if (p.write_macro) {
     const long long a = aidx(g, x, y, z);
     if (p.write_rho) rho_out[a] = rho;
@@ -152,7 +153,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, CL, FUSED>::blocks)
   nb_offsets(g, x, y, z, ox, oy, oz);
   C f[Q];
   cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, s, ox, oy, oz, bounce, f);
-  cell_finish<Q, S, CL, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, z, s, ox, oy, oz, elide, f);
+  cell_finish<Q, S, CL, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, z, s, ox, oy, oz, elide, f, step_omega<C>(p));
 }
 
 // Two cells per thread, z and z + 32 of the same row: a warp covers 64
@@ -190,8 +191,9 @@ __global__ void __launch_bounds__(256, 3)
   C fa[Q], fb[Q];
   cell_load<Q, S, ODD, FUSED>(F, ds, sa, ox, oy, oza, ma.x, fa);
   if (has_b) cell_load<Q, S, ODD, FUSED>(F, ds, sb, ox, oy, ozb, mb.x, fb);
-  cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, za, sa, ox, oy, oza, ma.y, fa);
-  if (has_b) cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, zb, sb, ox, oy, ozb, mb.y, fb);
+  const C om0 = step_omega<C>(p);
+  cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, za, sa, ox, oy, oza, ma.y, fa, om0);
+  if (has_b) cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, zb, sb, ox, oy, ozb, mb.y, fb, om0);
 }
 
 inline void step_launch_shape(const GridDesc& g, dim3& grid, dim3& block) {

@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kTmaThreads, TmaOccupancy<S, CL>::blocks)
     if (!valid) continue;
 
     C rho, u[3];
-    collide_cell<Q, C, CL, Store<S>::kDev>(f, p, rho, u);
+    collide_cell<Q, C, CL, Store<S>::kDev>(f, p, step_omega<C>(p), rho, u);
     if (p.write_macro) {
       const long long a = aidx(g, x, y, z);
       if (p.write_rho) rho_out[a] = rho;

@@ -462,6 +462,53 @@ def generateComputeSurfaceForce(lbgk: LBGK, m: np.ndarray) -> ComputeSurfaceForc
     return ComputeSurfaceForce(lbgk, m)
 
 
+class Batch:
+    """Extension (no ASL analogue): many independent LBGK domains advanced
+    together, one stream-collide launch per step for all of them plus one link
+    launch per condition position, replayed from a CUDA graph
+    (aslb_batch_create / aslb_batch_run)."""
+
+    def __init__(self, domains: Sequence[LBGK]):
+        self.domains = list(domains)
+        if not self.domains:
+            raise L.ASLError("ASL ERROR: Batch: no domains")
+        self.lib = self.domains[0].lib
+        arr = (C.c_void_p * len(self.domains))(*[d.h.value if isinstance(d.h, C.c_void_p) else d.h
+                                                  for d in self.domains])
+        h = C.c_void_p()
+        L.check(self.lib.aslb_batch_create(arr, len(self.domains), C.byref(h)), "Batch")
+        self.h = h
+
+    def run(self, nsteps: int, bcs: Sequence[Sequence["BC"]] = (), use_graph: bool = True):
+        """`for n: for each domain: execute(); executeAll(its bcs)`, batched.
+        ``bcs[i]``: the conditions of domain i, in ASL's order."""
+        lists = list(bcs) if bcs else [[] for _ in self.domains]
+        if len(lists) != len(self.domains):
+            raise L.ASLError("ASL ERROR: Batch::run: one condition list per domain")
+        flat = [b.h for lst in lists for b in lst]
+        arr = (C.c_void_p * max(1, len(flat)))(*flat)
+        counts = (C.c_int * len(lists))(*[len(lst) for lst in lists])
+        L.check(self.lib.aslb_batch_run(self.h, int(nsteps), arr, counts, 1 if use_graph else 0), "Batch::run")
+
+    def sync(self):
+        L.check(self.lib.aslb_batch_sync(self.h), "Batch::sync")
+
+    @property
+    def tiles(self) -> int:
+        return int(self.lib.aslb_batch_tiles(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.aslb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def initAll(items):
     for it in items:
         it.init()

@@ -9,6 +9,10 @@ generated from a seed (base seed 20261203, configuration k uses seed + k).
   porous_channel    D3Q19 512x256x256, non-overlapping random spheres
                     (r ~ U[4,12], solid fraction 0.4), periodic in x, no-slip
                     Y/Z walls, body force g=1e-6 along x, tau=0.6.
+  batch_channels    256 independent D3Q19 channels, sizes x ~ U[32,128],
+                    y, z ~ U[32,64] (about 47 M cells in all), each with one box
+                    or sphere obstacle, inlet velocity ~ U[0.02,0.08] at X0,
+                    pressure 1 at XE, no-slip Y/Z walls, tau ~ U[0.52,0.8].
   vehicle_d3q27     D3Q27 768x384x384 wind tunnel, 12 seeded boxes / vertical
                     cylinders standing on the floor (Z0), velocity 0.05 along x
                     at the inlet (X0), the far field (Y0, YE, ZE) and the moving
@@ -159,3 +163,45 @@ def vehicle_d3q27(size=(768, 384, 384), u_in=0.05, tau=0.51, n_obstacles=12, ste
     return Workload("vehicle_d3q27_%dx%dx%d" % tuple(size), tuple(size), 27, nu, bcs=bcs, map=m, steps=steps,
                     init_u=u, info={"obstacles": n_obstacles, "solid_fraction": solid, "seed": seed, "tau": tau,
                                     "u_in": u_in})
+
+
+def batch_channels(n=256, steps=2000, seed=BASE_SEED + 3) -> list:
+    """The many-small-domains case: n seeded channels of random size, each
+    with one box or sphere obstacle (alternating) in its upstream half."""
+    from .lbgk import Block
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        size = (int(rng.integers(32, 129)), int(rng.integers(32, 65)), int(rng.integers(32, 65)))
+        nx, ny, nz = size
+        u_in = float(rng.uniform(0.02, 0.08))
+        tau = float(rng.uniform(0.52, 0.8))
+        cx, cy, cz = rng.uniform(0.25, 0.45) * nx, rng.uniform(0.35, 0.65) * ny, rng.uniform(0.35, 0.65) * nz
+        r = float(rng.uniform(0.12, 0.22)) * min(ny, nz)
+        block = Block(size, 1.0)
+        if i % 2 == 0:
+            c = np.array([cx, cy, cz])
+            h = np.array([r, r, r])
+            shape = (G.generateDFBox(c, h), c - h, c + h)
+        else:
+            c = np.array([cx, cy, cz])
+            shape = (G.generateDFSphere(r, c), c - r, c + r)
+        m = G.rasterize_union(block, [shape])
+        u = (u_in, 0.0, 0.0)
+        bcs = [BCSpec("velocity", ("X0",), u=u), BCSpec("pressure", ("XE",), p=1.0),
+               BCSpec("noslip", ("Y0", "YE", "Z0", "ZE")), BCSpec("map_noslip")]
+        out.append(Workload("batch_channel_%d_%dx%dx%d" % (i, *size), size, 19, (tau - 0.5) / 3.0, bcs=bcs, map=m,
+                            steps=steps, init_u=u, info={"tau": tau, "u_in": u_in, "obstacle": "box" if i % 2 == 0
+                                                         else "sphere"}))
+    return out
+
+
+def build_batch(ws, storage="f32", fuse=True):
+    """All workloads of a batch on the GPU plus the Batch that steps them."""
+    from . import lbgk as A
+    lbs, bcs = [], []
+    for w in ws:
+        lb, bc = build_lbgk(w, storage=storage, compVel=False, compRho=False, fuse=fuse)
+        lbs.append(lb)
+        bcs.append(bc)
+    return A.Batch(lbs), lbs, bcs

@@ -51,6 +51,9 @@ def parse_args():
     ap.add_argument("--q27-steps", type=int, default=400,
                     help="timed steps of the D3Q27 vehicle workload (0: skip)")
     ap.add_argument("--q27-size", default="768,384,384")
+    ap.add_argument("--batch-steps", type=int, default=2000,
+                    help="timed steps of the 256-domain batch (0: skip)")
+    ap.add_argument("--batch-domains", type=int, default=256)
     return ap.parse_args()
 
 
@@ -273,6 +276,59 @@ def vehicle_run(W, size, steps: int, peak: float):
     return res
 
 
+def batch_run(W, n: int, steps: int, peak: float):
+    """Many small domains (seeded channels of random size, viscosity, obstacle
+    and inlet velocity): the batch (one persistent stream-collide launch per
+    step for all domains plus one link launch per condition position, CUDA
+    graph) against ASL's loop over the domains (execute + executeAll of each
+    domain, one launch per domain and condition)."""
+    import torch
+    ws = W.batch_channels(n=n, steps=steps)
+    cells = sum(w.cells for w in ws)
+    batch, lbs, bcs = W.build_batch(ws, storage="f32", fuse=True)
+    st = torch.cuda.ExternalStream(lbs[0].stream)
+    batch.run(6, bcs)
+    batch.sync()
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)  # the first domain's stream waits for the batch
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    t = timed(lambda: batch.run(steps, bcs))
+    nk = min(steps, 200) // 2 * 2
+    none = [[] for _ in lbs]
+    batch.run(4, none)  # tables and graph for the stream-collide alone
+    tk = timed(lambda: batch.run(nk, none)) / nk
+    launches = 1 + max(sum(1 for b in bc if not b.fused) for bc in bcs)
+    # ASL's loop: every domain and condition launched on its own
+    sep_steps = max(2, min(steps, 100))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(sep_steps):
+        for lb, bc in zip(lbs, bcs):
+            lb.execute()
+            for b in bc:
+                b.execute()
+    for lb in lbs:
+        lb.sync()
+    t_sep = time.perf_counter() - t0
+    bpc = BYTES_PER_CELL[("f32", 19)]
+    res = {"domains": n, "cells": cells, "steps": steps, "value": cells * steps / t / 1e6, "unit": "MLUPS",
+           "ms_per_step": t / steps * 1e3, "launches_per_step": launches, "tiles_per_step": batch.tiles,
+           "kernel_ms": tk * 1e3, "kernel_frac_of_peak": bpc * cells / tk / 1e9 / peak,
+           "separate_launches": {"value": cells * sep_steps / t_sep / 1e6, "unit": "MLUPS", "steps": sep_steps,
+                                 "launches_per_step": sum(1 + sum(b.kernels for b in bc) for bc in bcs),
+                                 "timing": "host clock around the loop, device synchronised at both ends"}}
+    batch.close()
+    del lbs, bcs
+    return res
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -397,6 +453,9 @@ def run_ours(args):
     accuracy = None
     if world == 1 and args.accuracy_steps > 0:
         accuracy = storage_accuracy(W, w, args.accuracy_steps)
+    batched = None
+    if world == 1 and args.batch_steps > 0:
+        batched = batch_run(W, args.batch_domains, args.batch_steps, peak)
     vehicle = None
     if world == 1 and args.q27_steps > 0:
         vehicle = vehicle_run(W, parse_size(args.q27_size), args.q27_steps, peak)
@@ -429,7 +488,7 @@ def run_ours(args):
                 "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "clocks": clk,
                 "gpu_launches": K * head["launches_per_step"],
                 "separate_conditions": sep, "tma_kernel": direct, "fp16": fp16, "accuracy": accuracy,
-                "d3q27_vehicle": vehicle, "finite": finite, "mass": mom[0]}
+                "d3q27_vehicle": vehicle, "batched_domains": batched, "finite": finite, "mass": mom[0]}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -78,6 +78,7 @@ extern "C" {
 typedef struct aslb_lbgk aslb_lbgk;
 typedef struct aslb_bc aslb_bc;
 typedef struct aslb_force aslb_force;
+typedef struct aslb_batch aslb_batch;
 
 /* Last error message of the calling thread ("" if none). */
 const char* aslb_last_error(void);
@@ -226,6 +227,32 @@ int aslb_force_destroy(aslb_force* fc);
  * first call before any stream capture. All calls share the array: calls
  * whose work overlaps on the GPU (different streams) race. Synchronises. */
 int aslb_force_compute_noalloc(aslb_force* fc, const double r0[3], double out6[6]);
+
+/* ---- batches of independent domains ------------------------------------ */
+
+/* Extension (no ASL analogue; an ASL program steps each LBGK object with its
+ * own execute() and executeAll(bc), src/num/aslNumMethod.h:47-77): advance many
+ * independent domains together. One persistent stream-collide launch per step
+ * covers every domain, and the k-th separate condition of every domain is one
+ * link launch; the whole step is replayed from a CUDA graph. The domains must
+ * share lattice, storage and device; aslb_batch_run also requires the same
+ * parity, the plain BGK collision (no closure) and equal batch-wide
+ * parameters (body force, rotation, compressibility, FP16 scale, output
+ * fields); viscosity, size, geometry and conditions are per domain. The batch
+ * refers to its domains: destroying a domain detaches it and later runs fail
+ * with ASLB_ERR_STATE. Each domain's pending work is waited for, and its later
+ * work waits for the batch. */
+int aslb_batch_create(aslb_lbgk* const* domains, int n, aslb_batch** out);
+/* nsteps steps of every domain. bcs: the conditions of domain 0 in ASL's
+ * order, then those of domain 1, ...; nbc[i] of them for domain i (fused
+ * no-slip conditions last, as in aslb_lbgk_run). Velocity maps and links
+ * across periodic faces are not batched (ASLB_ERR_ARG). use_graph as in
+ * aslb_lbgk_run. */
+int aslb_batch_run(aslb_batch* b, int nsteps, aslb_bc* const* bcs, const int* nbc, int use_graph);
+int aslb_batch_sync(aslb_batch* b);
+/* Tiles (256 cells of one x plane) of one batched step, over all domains. */
+long long aslb_batch_tiles(aslb_batch* b);
+int aslb_batch_destroy(aslb_batch* b);
 
 /* ---- workload geometry (host) ----------------------------------------- */
 
