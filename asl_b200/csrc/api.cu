@@ -1183,10 +1183,9 @@ int batch_tables(aslb_batch* b, aslb_bc* const* bcs, const int* nbc) {
     D.u = h->d.u;
     D.om0f = 1.0f / (3.0f * (float)h->p.nu + 0.5f);
     D.om0d = 1.0 / (3.0 * h->p.nu + 0.5);
-    D.row_tiles = (int)(((long long)g.ny * g.nz + 255) / 256);
     D.nz_inv = (unsigned)((0x100000000ULL + (unsigned long long)g.nz - 1) / (unsigned long long)g.nz);
     D.tile0 = b->ntiles;
-    b->ntiles += (long long)g.nx * D.row_tiles;
+    b->ntiles += g.nx;
   }
   ASLB_CUDA(cudaMalloc((void**)&b->dev_doms, n * sizeof(BatchDom)));
   ASLB_CUDA(cudaMemcpy(b->dev_doms, b->host_doms.data(), n * sizeof(BatchDom), cudaMemcpyHostToDevice));

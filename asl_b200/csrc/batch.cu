@@ -2,22 +2,25 @@
 // different sizes and viscosities advanced by one launch per step (plus one
 // per condition position), instead of one launch per domain and condition.
 // Each domain keeps its own allocation and layout; a device table maps the
-// launch's tiles (256 consecutive cells of one x plane, z fastest across y
-// rows) and links to domains.
+// launch's tiles (one x plane of one domain, its cells taken 256 at a time,
+// z fastest across y rows) and links to domains.
 #include "kernels.h"
 #include "stream_collide.cuh"
 #include "bc_links.cuh"
 
 namespace aslb {
 
+// Resident blocks per SM of the persistent batched step.
+constexpr int kBatchBlocks = 4;
+
 template <int Q, class S, bool ODD, bool FUSED>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, kBatchBlocks)
     k_batch_step(const BatchDom* __restrict__ doms, int ndom, long long ntiles, const StepParams p) {
   using C = typename Store<S>::C;
   using M = typename MacroT<S>::T;
   int d = -1;
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    // tiles of one block only move forward: advance the domain index
+    // a block's tiles only move forward: advance the domain index
     if (d < 0) {
       int lo = 0, hi = ndom - 1;
       while (lo < hi) {
@@ -29,28 +32,30 @@ __global__ void __launch_bounds__(256, 3)
     while (d + 1 < ndom && doms[d + 1].tile0 <= tile) ++d;
     const BatchDom& D = doms[d];
     const GridDesc g = D.g;
-    const long long local = tile - D.tile0;
-    const int x = (int)(local / D.row_tiles) + 1;
-    const unsigned l = (unsigned)(local % D.row_tiles) * 256u + threadIdx.x;
-    if (l >= (unsigned)(g.ny * g.nz)) continue;
-    unsigned yq = __umulhi(l, D.nz_inv);
-    if (yq * (unsigned)g.nz > l) --yq;  // exact quotient for l < 2^32 / nz
-    const int y = (int)yq + 1;
-    const int z = (int)(l - yq * (unsigned)g.nz) + 1;
-    const unsigned s = (unsigned)sidx(g, x, y, z);
-    uint32_t bounce = 0, elide = 0;
-    if (FUSED && D.mask) {
-      const uint2 m = D.mask[s];
-      bounce = m.x;
-      elide = m.y;
-    }
-    int ox[3], oy[3], oz[3];
-    nb_offsets(g, x, y, z, ox, oy, oz);
+    const int x = (int)(tile - D.tile0) + 1;  // one tile = one x plane
+    const unsigned plane_cells = (unsigned)(g.ny * g.nz);
+    const unsigned nz = (unsigned)g.nz, nz_inv = D.nz_inv;
     S* F = (S*)D.F;
-    C f[Q];
-    cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, s, ox, oy, oz, bounce, f);
+    const uint2* mask = D.mask;
     const C om0 = std::is_same<C, double>::value ? C(D.om0d) : C(D.om0f);
-    cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, (M*)D.rho, (M*)D.u, x, y, z, s, ox, oy, oz, elide, f, om0);
+    for (unsigned l = threadIdx.x; l < plane_cells; l += 256u) {
+      unsigned yq = __umulhi(l, nz_inv);
+      if (yq * nz > l) --yq;  // exact quotient for l < 2^32 / nz
+      const int y = (int)yq + 1;
+      const int z = (int)(l - yq * nz) + 1;
+      const unsigned s = (unsigned)sidx(g, x, y, z);
+      uint32_t bounce = 0, elide = 0;
+      if (FUSED && mask) {
+        const uint2 m = mask[s];
+        bounce = m.x;
+        elide = m.y;
+      }
+      int ox[3], oy[3], oz[3];
+      nb_offsets(g, x, y, z, ox, oy, oz);
+      C f[Q];
+      cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, s, ox, oy, oz, bounce, f);
+      cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, (M*)D.rho, (M*)D.u, x, y, z, s, ox, oy, oz, elide, f, om0);
+    }
   }
 }
 
@@ -83,7 +88,7 @@ template <int Q, class S>
 cudaError_t batch_step_impl(const BatchDom* doms, int ndom, long long ntiles, bool fused, const StepParams& p,
                             int parity_in, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
-  const long long cap = (long long)sm_count() * 3;
+  const long long cap = (long long)sm_count() * kBatchBlocks;
   const int grid = (int)(ntiles < cap ? ntiles : cap);
   if (parity_in == 0) {
     if (fused) k_batch_step<Q, S, true, true><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);

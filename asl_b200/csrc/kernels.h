@@ -65,9 +65,8 @@ struct BatchDom {
   void* u;
   float om0f;
   double om0d;
-  int row_tiles;     // 256-cell tiles per x plane: ceil(ny * nz / 256)
   unsigned nz_inv;   // ceil(2^32 / nz): y = l / nz by a multiply-high
-  long long tile0;   // first tile of this domain in the batch
+  long long tile0;   // first tile (x plane) of this domain in the batch
 };
 // One entry per (domain, condition) of a batched link launch (ordered by link0).
 struct BatchBc {

@@ -250,7 +250,7 @@ int aslb_batch_create(aslb_lbgk* const* domains, int n, aslb_batch** out);
  * aslb_lbgk_run. */
 int aslb_batch_run(aslb_batch* b, int nsteps, aslb_bc* const* bcs, const int* nbc, int use_graph);
 int aslb_batch_sync(aslb_batch* b);
-/* Tiles (256 cells of one x plane) of one batched step, over all domains. */
+/* Tiles (x planes) of one batched step, over all domains. */
 long long aslb_batch_tiles(aslb_batch* b);
 int aslb_batch_destroy(aslb_batch* b);
 
