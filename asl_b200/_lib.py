@@ -18,7 +18,7 @@ PERIODIC_X, PERIODIC_Y, PERIODIC_Z = 8, 16, 32
 CLOSURE_NONE, CLOSURE_ASL_INTENT, CLOSURE_SMAGORINSKY, CLOSURE_MLP = 0, 1, 2, 3
 BC_NOSLIP, BC_VELOCITY, BC_PRESSURE, BC_PRESSURE_VELOCITY = 0, 1, 2, 3
 BC_MAP_NOSLIP, BC_MAP_VELOCITY, BC_MAP_VELOCITY_ROTATION, BC_MAP_PRESSURE_VELOCITY = 10, 11, 12, 13
-FIELD_RHO, FIELD_VELOCITY, FIELD_F = 0, 1, 2
+FIELD_RHO, FIELD_VELOCITY, FIELD_F, FIELD_CS2 = 0, 1, 2, 3
 
 
 class ASLError(RuntimeError):
@@ -77,6 +77,13 @@ PROTOTYPES = {
     "aslb_force_compute": (C.c_int, [_vp, _pd, _pf, _pd]),
     "aslb_force_destroy": (C.c_int, [_vp]),
     "aslb_force_compute_noalloc": (C.c_int, [_vp, _pd, _pd]),
+    "aslb_lbgk_set_mlp_period": (C.c_int, [_vp, C.c_int]),
+    "aslb_lbgk_closure_features": (C.c_int, [_vp, _vp]),
+    "aslb_mlp_param_count": (C.c_int, []),
+    "aslb_mlp_grad_scratch_floats": (C.c_size_t, []),
+    "aslb_mlp_grad": (C.c_int, [_vp, _vp, _vp, C.c_longlong, _vp, C.c_float, _vp, _vp, _vp]),
+    "aslb_mlp_adam": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, _vp]),
+    "aslb_mlp_pack": (C.c_int, [_vp, _vp, C.c_float, _vp]),
     "aslb_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(_vp)]),
     "aslb_batch_run": (C.c_int, [_vp, C.c_int, C.POINTER(_vp), C.POINTER(C.c_int), C.c_int]),
     "aslb_batch_sync": (C.c_int, [_vp]),

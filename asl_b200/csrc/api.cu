@@ -22,6 +22,8 @@ int fail(int code, const std::string& msg) {
 }
 }  // namespace
 
+void aslb::set_last_error(const std::string& msg) { g_err = msg; }
+
 #define ASLB_CUDA(expr)                                                                              \
   do {                                                                                               \
     cudaError_t e_ = (expr);                                                                         \
@@ -45,6 +47,10 @@ struct aslb_lbgk {
   double pos0[3] = {0, 0, 0};
   double dx = 1.0;
   void* mlp_dev = nullptr;
+  // learned closure: Cs^2 per storage cell, refreshed every mlp_period steps
+  float* cs2_field = nullptr;
+  int mlp_period = 8;
+  long long mlp_last = -1;  // step at which the field was last computed
   double* red_partials = nullptr;  // moments scratch
   double* red_out = nullptr;
   double* host_out = nullptr;      // pinned
@@ -116,12 +122,28 @@ void prepare_params(aslb_lbgk* h) {
   h->p.write_rho = (h->comp_rho || h->macro_once) ? 1 : 0;
   h->p.write_vel = (h->comp_vel || h->macro_once) ? 1 : 0;
   h->p.write_macro = h->p.write_rho | h->p.write_vel;
-  h->p.mlp = h->mlp_dev;
+  h->p.cs2 = h->cs2_field;
   h->p.mask = h->fresh ? nullptr : h->mask_dev;
+}
+
+bool mlp_due(const aslb_lbgk* h) {
+  return h->closure == CL_MLP && (h->mlp_last < 0 || h->steps - h->mlp_last >= h->mlp_period);
+}
+
+// Steps of one replayed time-loop graph: two (the AA parities), or a whole
+// refresh period of the learned closure (even, so it starts on one parity).
+int graph_cycle(const aslb_lbgk* h) {
+  if (h->closure != CL_MLP) return 2;
+  return h->mlp_period % 2 == 0 ? h->mlp_period : 2 * h->mlp_period;
 }
 
 int do_step(aslb_lbgk* h) {
   prepare_params(h);
+  if (mlp_due(h)) {
+    cudaError_t e = launch_closure_field(h->d, h->p, h->mlp_dev, h->cs2_field, h->parity, h->stream);
+    if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("closure-field launch: ") + cudaGetErrorString(e));
+    h->mlp_last = h->steps;
+  }
   cudaError_t e = launch_step(h->d, h->p, h->closure, h->parity, h->stream);
   if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("stream-collide launch: ") + cudaGetErrorString(e));
   h->parity ^= 1;
@@ -422,6 +444,7 @@ int aslb_lbgk_destroy(aslb_lbgk* h) {
   cudaFree(h->d.rho);
   cudaFree(h->d.u);
   cudaFree(h->mlp_dev);
+  cudaFree(h->cs2_field);
   cudaFree(h->mask_dev);
   cudaFree(h->red_partials);
   cudaFree(h->red_out);
@@ -498,6 +521,14 @@ int aslb_lbgk_set_closure(aslb_lbgk* h, int closure, double cs) {
   if (closure < CL_NONE || closure > CL_MLP) return fail(ASLB_ERR_ARG, "aslb_lbgk_set_closure: unknown closure");
   if (closure == CL_MLP && !h->mlp_dev)
     return fail(ASLB_ERR_STATE, "aslb_lbgk_set_closure: load a network with aslb_lbgk_set_mlp first");
+  if (closure == CL_MLP && (h->d.q == 15 || h->d.storage == ST_F64))
+    return fail(ASLB_ERR_ARG, "aslb_lbgk_set_closure: the learned closure runs on D3Q19 / D3Q27 with FP32 or FP16 storage");
+  if (closure == CL_MLP && !h->cs2_field) {
+    const size_t n = (size_t)h->d.g.dstride + 4096;
+    ASLB_CUDA(cudaMalloc((void**)&h->cs2_field, n * sizeof(float)));
+    ASLB_CUDA(cudaMemset(h->cs2_field, 0, n * sizeof(float)));
+  }
+  h->mlp_last = -1;
   h->closure = closure;
   h->p.cs = cs;
   h->version++;
@@ -513,7 +544,27 @@ int aslb_lbgk_set_mlp(aslb_lbgk* h, const void* net_host, size_t bytes) {
   if (!h->mlp_dev) ASLB_CUDA(cudaMalloc(&h->mlp_dev, sizeof(MlpNet)));
   ASLB_CUDA(cudaMemcpyAsync(h->mlp_dev, net_host, sizeof(MlpNet), cudaMemcpyHostToDevice, h->stream));
   ASLB_CUDA(cudaStreamSynchronize(h->stream));
+  h->mlp_last = -1;  // new weights: recompute the field before the next step
   h->version++;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_set_mlp_period(aslb_lbgk* h, int steps) {
+  ASLB_CHECK_HANDLE(h);
+  if (steps < 1) return fail(ASLB_ERR_ARG, "aslb_lbgk_set_mlp_period: period must be >= 1");
+  h->mlp_period = steps;
+  h->mlp_last = -1;
+  h->version++;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_closure_features(aslb_lbgk* h, float* out_dev) {
+  ASLB_CHECK_HANDLE(h);
+  if (!out_dev) return fail(ASLB_ERR_ARG, "aslb_lbgk_closure_features: null output");
+  prepare_params(h);
+  cudaError_t e = launch_closure_features(h->d, h->p, out_dev, h->parity, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_closure_features: ") + cudaGetErrorString(e));
   return ASLB_OK;
 }
 
@@ -609,16 +660,25 @@ int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int us
     }
     return ASLB_OK;
   };
-  if (!use_graph || h->stream == nullptr || nsteps < 2) return eager(nsteps);
+  const int cycle = graph_cycle(h);
+  if (!use_graph || h->stream == nullptr || nsteps < cycle) return eager(nsteps);
   int done = 0;
   if (h->macro_once || h->fresh) {
     int r = eager(1);
     if (r) return r;
     done = 1;
   }
+  // the learned closure's graph starts where a field refresh is due
+  if (h->closure == CL_MLP)
+    while (done < nsteps && !mlp_due(h)) {
+      int r = eager(1);
+      if (r) return r;
+      done += 1;
+    }
+  if (nsteps - done < cycle) return eager(nsteps - done);
   std::vector<aslb_bc*> key(bcs, bcs + nbc);
   const bool valid = h->graph && h->graph_version == h->version && h->graph_bcs == key;
-  if (valid && h->graph_parity != h->parity && done < nsteps) {
+  if (valid && h->graph_parity != h->parity && h->closure != CL_MLP && done < nsteps) {
     int r = eager(1);
     if (r) return r;
     done += 1;
@@ -627,12 +687,14 @@ int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int us
     drop_graph(h);
     const int start_parity = h->parity;
     const long long start_steps = h->steps;
+    const long long start_mlp = h->mlp_last;
     cudaGraph_t graph = nullptr;
     ASLB_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    int r = eager(2);
+    int r = eager(cycle);
     cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
     h->parity = start_parity;  // capture enqueued nothing
     h->steps = start_steps;
+    h->mlp_last = start_mlp;
     if (r) {
       if (graph) cudaGraphDestroy(graph);
       return r;
@@ -648,10 +710,11 @@ int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int us
     h->graph_parity = start_parity;
     h->graph_version = h->version;
   }
-  const int pairs = (nsteps - done) / 2;
-  for (int i = 0; i < pairs; ++i) ASLB_CUDA(cudaGraphLaunch(h->graph, h->stream));
-  h->steps += 2LL * pairs;
-  done += 2 * pairs;
+  const int reps = (nsteps - done) / cycle;
+  for (int i = 0; i < reps; ++i) ASLB_CUDA(cudaGraphLaunch(h->graph, h->stream));
+  h->steps += (long long)cycle * reps;
+  if (h->closure == CL_MLP && reps > 0) h->mlp_last = h->steps - cycle + (cycle - h->mlp_period);
+  done += cycle * reps;
   return eager(nsteps - done);
 }
 
@@ -681,11 +744,28 @@ int aslb_lbgk_read(aslb_lbgk* h, int field, int dtype, void* host_out) {
   if (!host_out) return fail(ASLB_ERR_ARG, "aslb_lbgk_read: null output");
   if (dtype != ASLB_F32 && dtype != ASLB_F64) return fail(ASLB_ERR_ARG, "aslb_lbgk_read: dtype must be F32 or F64");
   const size_t L = (size_t)h->d.g.L;
-  const size_t mb = macro_bytes(h->d.storage);
+  const size_t mb = field == ASLB_FIELD_CS2 ? sizeof(float) : macro_bytes(h->d.storage);
   size_t count;
   void* dev = nullptr;
   bool own = false;
-  if (field == ASLB_FIELD_RHO) {
+  if (field == ASLB_FIELD_CS2) {
+    if (h->closure != CL_MLP || !h->cs2_field)
+      return fail(ASLB_ERR_STATE, "aslb_lbgk_read: the Cs^2 field exists with the learned closure only");
+    if (mlp_due(h)) {  // the field the next step will use
+      prepare_params(h);
+      cudaError_t e = launch_closure_field(h->d, h->p, h->mlp_dev, h->cs2_field, h->parity, h->stream);
+      if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_read: ") + cudaGetErrorString(e));
+      h->mlp_last = h->steps;
+    }
+    count = L;
+    ASLB_CUDA(cudaMalloc(&dev, count * mb));
+    own = true;
+    cudaError_t e = launch_gather_cells(h->d.g, h->cs2_field, (float*)dev, h->stream);
+    if (e != cudaSuccess) {
+      cudaFree(dev);
+      return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_read: ") + cudaGetErrorString(e));
+    }
+  } else if (field == ASLB_FIELD_RHO) {
     count = L;
     dev = h->d.rho;
   } else if (field == ASLB_FIELD_VELOCITY) {

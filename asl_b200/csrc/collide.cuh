@@ -122,16 +122,19 @@ __device__ __forceinline__ C step_omega(const StepParams& p) {
   if constexpr (std::is_same<C, double>::value) return p.om0d; else return p.om0f;
 }
 
-// f: the Q values of one cell in the collision representation (f, or
-// D = (f - 1) sigma when DEV), replaced by the post-collision values.
-// om0: the BGK relaxation rate (step_omega, or a batch domain's own).
-// rho_out / u_out: density and velocity (ASL's compRho / compVel fields).
-template <int Q, class C, int CL, bool DEV = false>
-__device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, const C om0, C& rho_out,
-                                             C (&u_out)[3]) {
+// Moments of one cell and the equilibrium coefficients,
+//   f_eq,i = a0 + 3 c_i.m + a2 (c_i.m)^2,
+// in the collision representation (m and a0 scaled by sigma with DEV).
+template <class C>
+struct Moments {
+  C V, rho, inv_rho, m0, m1, m2, ium, a0, a2;
+};
+
+template <int Q, class C, bool DEV>
+__device__ __forceinline__ Moments<C> cell_moments(const C (&f)[Q], const StepParams& p, const C om0) {
   using Lt = Lattice<Q>;
   using Pr = Pairs<Q>;
-  // ---- moments: pair sums and differences, per weight class
+  // pair sums and differences, per weight class
   C S[4], M[4][3];
   static_for<Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
@@ -150,6 +153,7 @@ __device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, con
       });
     }
   });
+  Moments<C> r;
   C V = mul_(C(Lt::w(0)), f[0]);
   C m0 = C(0), m1 = C(0), m2 = C(0);
   static_for<4>([&](auto kc) {
@@ -172,11 +176,9 @@ __device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, con
   const C sig = DEV ? C(p.scale) : C(1);
   const C isig = DEV ? C(p.inv_scale) : C(1);
   const C rho = DEV ? fma_(V, isig, C(1)) : V;
-
-  C om = om0;
   if (p.has_coriolis) {
     // component-sequential, as ACL emits `momentum += (2/w) Omega x momentum`
-    const C k = div_(C(2), om);
+    const C k = div_(C(2), om0);
     const C O0 = par_Om<C>(p, 0), O1 = par_Om<C>(p, 1), O2 = par_Om<C>(p, 2);
     m0 = fma_(k, sub_(mul_(O1, m2), mul_(O2, m1)), m0);
     m1 = fma_(k, sub_(mul_(O2, m0), mul_(O0, m2)), m1);
@@ -192,70 +194,108 @@ __device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, con
   // factor taking the stored momentum to velocity (u = m / rho, or m when
   // incompressible), with the 1 / sigma of DEV folded in
   const C ium = p.compressible ? (DEV ? mul_(isig, inv_rho) : inv_rho) : isig;
+  const C mm = fma_(m2, m2, fma_(m1, m1, mul_(m0, m0)));
+  r.a2 = (DEV || p.compressible) ? mul_(C(4.5), ium) : C(4.5);
+  r.a0 = (DEV || p.compressible) ? sub_(V, mul_(mul_(C(1.5), mm), ium)) : sub_(V, mul_(C(1.5), mm));
+  r.V = V;
+  r.rho = rho;
+  r.inv_rho = inv_rho;
+  r.m0 = m0;
+  r.m1 = m1;
+  r.m2 = m2;
+  r.ium = ium;
+  return r;
+}
+
+// Non-equilibrium stress Pi_ab = sum_i w_i c_ia c_ib (f_i - f_eq,i) in ASL's
+// normalisation, order (00, 11, 22, 01, 12, 02).
+template <int Q, class C, bool DEV>
+__device__ __forceinline__ void cell_pneq(const C (&f)[Q], const Moments<C>& mo, const StepParams& p, C (&P)[6]) {
+  using Lt = Lattice<Q>;
+  C P00 = C(0), P11 = C(0), P22 = C(0), P01 = C(0), P12 = C(0), P02 = C(0);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const C cm = cdot<Q, C>(i, mo.m0, mo.m1, mo.m2);
+    const C feq = fma_(mo.a2, mul_(cm, cm), fma_(C(3), cm, mo.a0));
+    const C wd = mul_(C(Lt::w(i)), sub_(f[i], feq));
+    if (Lt::c(i, 0) != 0) P00 += wd;
+    if (Lt::c(i, 1) != 0) P11 += wd;
+    if (Lt::c(i, 2) != 0) P22 += wd;
+    if (Lt::c(i, 0) * Lt::c(i, 1) > 0) P01 += wd;
+    if (Lt::c(i, 0) * Lt::c(i, 1) < 0) P01 -= wd;
+    if (Lt::c(i, 1) * Lt::c(i, 2) > 0) P12 += wd;
+    if (Lt::c(i, 1) * Lt::c(i, 2) < 0) P12 -= wd;
+    if (Lt::c(i, 0) * Lt::c(i, 2) > 0) P02 += wd;
+    if (Lt::c(i, 0) * Lt::c(i, 2) < 0) P02 -= wd;
+  }
+  if (DEV) {
+    const C isig = C(p.inv_scale);
+    P00 = mul_(P00, isig); P11 = mul_(P11, isig); P22 = mul_(P22, isig);
+    P01 = mul_(P01, isig); P12 = mul_(P12, isig); P02 = mul_(P02, isig);
+  }
+  P[0] = P00; P[1] = P11; P[2] = P22; P[3] = P01; P[4] = P12; P[5] = P02;
+}
+
+// f: the Q values of one cell in the collision representation (f, or
+// D = (f - 1) sigma when DEV), replaced by the post-collision values.
+// om0: the BGK relaxation rate (step_omega, or a batch domain's own).
+// cs2_cell: the cell's Smagorinsky coefficient Cs^2 for the learned closure
+// (CL_MLP, from the closure field); unused otherwise.
+// rho_out / u_out: density and velocity (ASL's compRho / compVel fields).
+template <int Q, class C, int CL, bool DEV = false>
+__device__ __forceinline__ void collide_cell(C (&f)[Q], const StepParams& p, const C om0, const C cs2_cell,
+                                             C& rho_out, C (&u_out)[3]) {
+  using Lt = Lattice<Q>;
+  using Pr = Pairs<Q>;
+  const Moments<C> mo = cell_moments<Q, C, DEV>(f, p, om0);
+  const C rho = mo.rho, inv_rho = mo.inv_rho, m0 = mo.m0, m1 = mo.m1, m2 = mo.m2, a0 = mo.a0, a2 = mo.a2;
+  const C sig = DEV ? C(p.scale) : C(1);
+  const C isig = DEV ? C(p.inv_scale) : C(1);
   rho_out = rho;
   if (DEV || p.compressible) {
-    u_out[0] = mul_(m0, ium);
-    u_out[1] = mul_(m1, ium);
-    u_out[2] = mul_(m2, ium);
+    u_out[0] = mul_(m0, mo.ium);
+    u_out[1] = mul_(m1, mo.ium);
+    u_out[2] = mul_(m2, mo.ium);
   } else {
     u_out[0] = m0;
     u_out[1] = m1;
     u_out[2] = m2;
   }
-  const C mm = fma_(m2, m2, fma_(m1, m1, mul_(m0, m0)));
-  const C a2 = (DEV || p.compressible) ? mul_(C(4.5), ium) : C(4.5);
-  const C a0 = (DEV || p.compressible) ? sub_(V, mul_(mul_(C(1.5), mm), ium)) : sub_(V, mul_(C(1.5), mm));
 
-  if constexpr (CL == CL_ASL_INTENT || CL == CL_SMAGORINSKY || CL == CL_MLP) {
-    // Non-equilibrium quantities need f_eq first (scaled by sigma with DEV).
+  C om = om0;
+  if constexpr (CL == CL_ASL_INTENT) {
+    // LBGKTurbulence's limiter: w = 4 |f - f_eq|^2 / |f|^2 (f_eq scaled by sigma with DEV)
     C sn = C(0), sf = C(0);
-    C P00 = C(0), P11 = C(0), P22 = C(0), P01 = C(0), P12 = C(0), P02 = C(0);
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
       const C cm = cdot<Q, C>(i, m0, m1, m2);
       const C feq = fma_(a2, mul_(cm, cm), fma_(C(3), cm, a0));
       const C d = sub_(f[i], feq);
-      if (CL == CL_ASL_INTENT) {
-        const C fa = DEV ? fma_(f[i], isig, C(1)) : f[i];
-        sn = fma_(d, d, sn);
-        sf = fma_(fa, fa, sf);
-      } else {
-        const C wd = mul_(C(Lt::w(i)), d);
-        if (Lt::c(i, 0) != 0) P00 += wd;
-        if (Lt::c(i, 1) != 0) P11 += wd;
-        if (Lt::c(i, 2) != 0) P22 += wd;
-        if (Lt::c(i, 0) * Lt::c(i, 1) > 0) P01 += wd;
-        if (Lt::c(i, 0) * Lt::c(i, 1) < 0) P01 -= wd;
-        if (Lt::c(i, 1) * Lt::c(i, 2) > 0) P12 += wd;
-        if (Lt::c(i, 1) * Lt::c(i, 2) < 0) P12 -= wd;
-        if (Lt::c(i, 0) * Lt::c(i, 2) > 0) P02 += wd;
-        if (Lt::c(i, 0) * Lt::c(i, 2) < 0) P02 -= wd;
-      }
+      const C fa = DEV ? fma_(f[i], isig, C(1)) : f[i];
+      sn = fma_(d, d, sn);
+      sf = fma_(fa, fa, sf);
     }
-    if (DEV) {
-      sn = mul_(mul_(sn, isig), isig);
-      P00 = mul_(P00, isig); P11 = mul_(P11, isig); P22 = mul_(P22, isig);
-      P01 = mul_(P01, isig); P12 = mul_(P12, isig); P02 = mul_(P02, isig);
-    }
-    if constexpr (CL == CL_ASL_INTENT) {
-      // LBGKTurbulence's limiter: w = 4 |f - f_eq|^2 / |f|^2
-      const C wl = mul_(C(4), div_(sn, sf));
-      if (wl > C(1)) om = div_(C(1), add_(mul_(C(3), fmin(mul_(par_nu<C>(p), wl), C(0.5))), C(0.5)));
-    } else if constexpr (CL == CL_SMAGORINSKY) {
-      // Hou, Sterling, Chen & Doolen (1996): tau = (tau0 + sqrt(tau0^2 + 18 sqrt(2) Cs^2 |Pi_neq| / rho)) / 2
-      const C q2 = add_(fma_(P22, P22, fma_(P11, P11, mul_(P00, P00))),
-                        mul_(C(2), fma_(P02, P02, fma_(P12, P12, mul_(P01, P01)))));
-      const C tau0 = div_(C(1), om0);
+    if (DEV) sn = mul_(mul_(sn, isig), isig);
+    const C wl = mul_(C(4), div_(sn, sf));
+    if (wl > C(1)) om = div_(C(1), add_(mul_(C(3), fmin(mul_(par_nu<C>(p), wl), C(0.5))), C(0.5)));
+  } else if constexpr (CL == CL_SMAGORINSKY || CL == CL_MLP) {
+    // Hou, Sterling, Chen & Doolen (1996): tau = (tau0 + sqrt(tau0^2 + 18 sqrt(2) Cs^2 |Pi_neq| / rho)) / 2,
+    // Cs^2 constant (Smagorinsky) or the network's per-cell value (learned closure)
+    C P[6];
+    cell_pneq<Q, C, DEV>(f, mo, p, P);
+    const C q2 = add_(fma_(P[2], P[2], fma_(P[1], P[1], mul_(P[0], P[0]))),
+                      mul_(C(2), fma_(P[5], P[5], fma_(P[4], P[4], mul_(P[3], P[3])))));
+    const C tau0 = div_(C(1), om0);
+    C cs2;
+    if constexpr (CL == CL_SMAGORINSKY) {
       const C cs = par_cs<C>(p);
-      const C cs2 = mul_(cs, cs);
-      const C tau = mul_(C(0.5), add_(tau0, sqrt(fma_(tau0, tau0, mul_(mul_(mul_(C(25.455844122715710), cs2),
-                                                                            sqrt(q2)), inv_rho)))));
-      om = div_(C(1), tau);
+      cs2 = mul_(cs, cs);
     } else {
-      // Learned closure: tau_eff from invariants of Pi_neq and the strain.
-      const C iu = DEV ? mul_(isig, inv_rho) : inv_rho;
-      om = mlp_omega<C>(p.mlp, om0, rho, m0 * iu, m1 * iu, m2 * iu, P00, P11, P22, P01, P12, P02);
+      cs2 = cs2_cell;
     }
+    const C tau = mul_(C(0.5), add_(tau0, sqrt(fma_(tau0, tau0, mul_(mul_(mul_(C(25.455844122715710), cs2),
+                                                                          sqrt(q2)), inv_rho)))));
+    om = div_(C(1), tau);
   }
 
   // ---- relaxation, one opposite pair at a time:

@@ -70,7 +70,7 @@ struct StepParams {
   int write_macro;   // write rho and u (ASL's compVel/compRho) this step
   int write_rho, write_vel;
   float scale, inv_scale;  // FP16 storage: d = (f - 1) * scale
-  const void* mlp;         // closure network (device), CL == 3
+  const float* cs2;        // learned closure (CL == 3): Cs^2 per storage cell
   // Fused no-slip conditions (null when none), two words per storage cell.
   // x (bounce): bit k = population k enters this cell through a fused link,
   // so it is read by bounce-back from the cell's own outgoing population.

@@ -2,11 +2,15 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <string>
 #include "internal.cuh"
 
 namespace aslb {
 
 enum StorageKind { ST_F32 = 0, ST_F16 = 1, ST_F64 = 2 };
+
+// Message returned by aslb_last_error() on the calling thread.
+void set_last_error(const std::string& msg);
 
 struct DomainDev {
   GridDesc g;
@@ -54,6 +58,16 @@ cudaError_t launch_moments(const DomainDev& d, const StepParams& p, int parity, 
 // Sum `nblocks` rows of `width` doubles into out (fixed order, one block).
 cudaError_t launch_reduce_rows(const double* partials, int nblocks, int width, double* out, cudaStream_t st);
 
+
+// Learned closure: Cs^2 per storage cell from the network (closure_field.cu),
+// and the nine raw features per interior cell, out[k * cells + compact index]
+// (x-major, z fastest), for training. D3Q19 / D3Q27, FP32 or FP16 storage.
+cudaError_t launch_closure_field(const DomainDev& d, const StepParams& p, const void* net, float* cs2, int parity,
+                                 cudaStream_t st);
+cudaError_t launch_closure_features(const DomainDev& d, const StepParams& p, float* out, int parity,
+                                    cudaStream_t st);
+// One float per storage cell (interior) -> ASL's ghosted layout, 0 on ghosts.
+cudaError_t launch_gather_cells(const GridDesc& g, const float* src, float* dst_asl, cudaStream_t st);
 
 // ---- batches of independent domains ----------------------------------------
 // One entry per domain of a batch (device table, ordered by tile0).

@@ -58,41 +58,4 @@ __host__ __device__ inline void mlp_features(C rho, C ux, C uy, C uz, C P00, C P
 
 __host__ __device__ inline float mlp_softplus(float y) { return y > 20.f ? y : log1pf(expf(y)); }
 
-// Scalar FP32 forward of one cell (the reference path and the fallback-free
-// definition that the fused tensor-core path is checked against).
-__device__ inline float mlp_forward_scalar(const MlpNet* __restrict__ net, const float (&x)[kMlpIn]) {
-  float xin[kMlpIn];
-#pragma unroll
-  for (int i = 0; i < kMlpIn; ++i) xin[i] = (x[i] - net->in_shift[i]) * net->in_scale[i];
-  float h1[kMlpHidden];
-#pragma unroll 4
-  for (int o = 0; o < kMlpHidden; ++o) {
-    float s = net->b1[o];
-#pragma unroll
-    for (int i = 0; i < kMlpIn; ++i) s += __bfloat162float(net->w1[o][i]) * xin[i];
-    h1[o] = fmaxf(s, 0.f);
-  }
-  float y = net->b3;
-  for (int o = 0; o < kMlpHidden; ++o) {
-    float s = net->b2[o];
-#pragma unroll 8
-    for (int i = 0; i < kMlpHidden; ++i) s += __bfloat162float(net->w2[o][i]) * h1[i];
-    y += __bfloat162float(net->w3[o]) * fmaxf(s, 0.f);
-  }
-  return net->out_scale * mlp_softplus(y);
-}
-
-template <class C>
-__device__ inline C mlp_omega(const void* netp, C om0, C rho, C ux, C uy, C uz, C P00, C P11, C P22, C P01, C P12,
-                              C P02) {
-  const MlpNet* net = static_cast<const MlpNet*>(netp);
-  float x[kMlpIn];
-  mlp_features<C>(rho, ux, uy, uz, P00, P11, P22, P01, P12, P02, x);
-  const C cs2 = C(mlp_forward_scalar(net, x));
-  const C q2 = P00 * P00 + P11 * P11 + P22 * P22 + C(2) * (P01 * P01 + P12 * P12 + P02 * P02);
-  const C tau0 = C(1) / om0;
-  const C tau = C(0.5) * (tau0 + sqrt(tau0 * tau0 + C(25.455844122715710) * cs2 * sqrt(q2) / rho));
-  return C(1) / tau;
-}
-
 }  // namespace aslb

@@ -104,7 +104,8 @@ __device__ __forceinline__ void cell_finish(S* __restrict__ F, const GridDesc& g
   using C = typename Store<S>::C;
   const unsigned ds = (unsigned)g.dstride;
   C rho, u[3];
-  collide_cell<Q, C, CL, Store<S>::kDev>(f, p, om0, rho, u);
+  const C cs2 = CL == CL_MLP ? C(p.cs2[s]) : C(0);
+  collide_cell<Q, C, CL, Store<S>::kDev>(f, p, om0, cs2, rho, u);
   if (p.write_macro) {
     const long long a = aidx(g, x, y, z);
     if (p.write_rho) rho_out[a] = rho;

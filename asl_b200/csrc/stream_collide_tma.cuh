@@ -186,7 +186,8 @@ __global__ void __launch_bounds__(kTmaThreads, TmaOccupancy<S, CL>::blocks)
     if (!valid) continue;
 
     C rho, u[3];
-    collide_cell<Q, C, CL, Store<S>::kDev>(f, p, step_omega<C>(p), rho, u);
+    const C cs2 = CL == CL_MLP ? C(p.cs2[s]) : C(0);
+    collide_cell<Q, C, CL, Store<S>::kDev>(f, p, step_omega<C>(p), cs2, rho, u);
     if (p.write_macro) {
       const long long a = aidx(g, x, y, z);
       if (p.write_rho) rho_out[a] = rho;

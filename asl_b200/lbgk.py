@@ -215,6 +215,19 @@ class LBGK:
         buf = C.create_string_buffer(bytes(blob), len(blob))
         L.check(self.lib.aslb_lbgk_set_mlp(self.h, C.cast(buf, C.c_void_p), len(blob)), "LBGK::setMLP")
 
+    def setMLPPeriod(self, steps: int):
+        """Steps between two evaluations of the closure network (default 8)."""
+        L.check(self.lib.aslb_lbgk_set_mlp_period(self.h, int(steps)), "LBGK::setMLPPeriod")
+
+    def closureFeatures(self, out_dev_ptr: int):
+        """Write the nine raw closure features of every interior cell to device
+        memory at ``out_dev_ptr`` (9 x cells floats, cells x-major, z fastest)."""
+        L.check(self.lib.aslb_lbgk_closure_features(self.h, C.c_void_p(int(out_dev_ptr))), "LBGK::closureFeatures")
+
+    def getCs2(self, dtype=np.float64) -> np.ndarray:
+        """The learned closure's Cs^2 field the next step uses (ghosted layout)."""
+        return self._read(L.FIELD_CS2, 1, dtype)[0]
+
     def getVectorTemplate(self) -> VectorTemplate:
         return self.vectorTemplate
 

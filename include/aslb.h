@@ -74,6 +74,7 @@ extern "C" {
 #define ASLB_FIELD_RHO 0
 #define ASLB_FIELD_VELOCITY 1
 #define ASLB_FIELD_F 2
+#define ASLB_FIELD_CS2 3 /* learned closure: the Cs^2 field the next step uses */
 
 typedef struct aslb_lbgk aslb_lbgk;
 typedef struct aslb_bc aslb_bc;
@@ -121,10 +122,22 @@ int aslb_lbgk_set_body_force(aslb_lbgk* h, const double g[3]);
 /* asl::LBGKTurbulence (src/num/aslLBGK.cxx:298-355) and extensions; cs is the
  * Smagorinsky constant (ignored otherwise). */
 int aslb_lbgk_set_closure(aslb_lbgk* h, int closure, double cs);
-/* Learned closure network: `bytes` of the packed device layout produced by
- * the training code (see aslb_mlp_layout_bytes). Copied to the device. */
+/* Learned closure network (extension standing in for LBGKTurbulence's
+ * limiter): `bytes` of the packed device layout produced by the training code
+ * (see aslb_mlp_layout_bytes). Copied to the device. With closure
+ * ASLB_CLOSURE_MLP, every `period` steps (aslb_lbgk_set_mlp_period, default
+ * 8) a tensor-core kernel evaluates the network on the invariants of every
+ * cell's non-equilibrium stress and stores a Cs^2 field; each step then
+ * applies the Smagorinsky closed form with that cell's Cs^2. D3Q19 / D3Q27,
+ * FP32 or FP16 storage. */
 size_t aslb_mlp_layout_bytes(void);
 int aslb_lbgk_set_mlp(aslb_lbgk* h, const void* net_host, size_t bytes);
+int aslb_lbgk_set_mlp_period(aslb_lbgk* h, int steps);
+/* The network's nine input features of every interior cell, before
+ * normalisation, from the populations the next step reads: out_dev is DEVICE
+ * memory of 9 * nx * ny * nz floats, feature-major, cells x-major with z
+ * fastest. Training data for the closure. Synchronises. */
+int aslb_lbgk_closure_features(aslb_lbgk* h, float* out_dev);
 /* FP16 storage scale: stored half = (f - 1) * scale (default 1024). */
 int aslb_lbgk_set_fp16_scale(aslb_lbgk* h, double scale);
 /* Physical position of interior cell (0,0,0) and the spacing
@@ -227,6 +240,29 @@ int aslb_force_destroy(aslb_force* fc);
  * first call before any stream capture. All calls share the array: calls
  * whose work overlaps on the GPU (different streams) race. Synchronises. */
 int aslb_force_compute_noalloc(aslb_force* fc, const double r0[3], double out6[6]);
+
+/* ---- learned closure: training (extension, no ASL analogue) ------------ */
+
+/* The network's own training kernels. All pointers are DEVICE memory except
+ * in aslb_mlp_pack; `stream` is a cudaStream_t (null: the default stream).
+ * Parameters: aslb_mlp_param_count() FP32 values, W1[64][9], b1[64],
+ * W2[64][64], b2[64], w3[64], b3. Model: x' = (x - norm[0:9]) * norm[9:18],
+ * h1 = relu(W1 x' + b1), h2 = relu(W2 h1 + b2), y = w3.h2 + b3,
+ * Cs^2 = out_scale * softplus(y); loss = mean over samples of (Cs^2 - t)^2. */
+int aslb_mlp_param_count(void);
+/* Scratch the gradient kernel needs, in floats. */
+size_t aslb_mlp_grad_scratch_floats(void);
+/* Gradient of the loss over n samples (x: 9 x n floats, feature-major; t: n
+ * targets) into grad_loss[0 .. P-1], and the sum of squared errors into
+ * grad_loss[P]. Deterministic (fixed reduction order). */
+int aslb_mlp_grad(const float* params, const float* x, const float* t, long long n, const float* norm,
+                  float out_scale, float* scratch, float* grad_loss, void* stream);
+/* One Adam step (Kingma & Ba 2015) of the parameters; step counts from 1. */
+int aslb_mlp_adam(float* params, const float* grad, float* m, float* v, int step, float lr, float beta1,
+                  float beta2, float eps, void* stream);
+/* HOST memory: the inference layout (aslb_mlp_layout_bytes() bytes, weights
+ * rounded to BF16) from FP32 parameters and the input normalisation. */
+int aslb_mlp_pack(const float* params_host, const float* norm_host, float out_scale, void* net_host);
 
 /* ---- batches of independent domains ------------------------------------ */
 

@@ -1,0 +1,170 @@
+"""GPU tests of the learned closure: the training kernels against the CPU
+oracle (gradient, Adam), the feature kernel against features recomputed on
+the CPU from the exported populations, the tensor-core network against its
+BF16 oracle, and the closure's stream-collide against Smagorinsky."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from asl_b200 import _lib as L
+from asl_b200 import closure as CL
+from asl_b200 import lbgk as A
+from oracle import mlp_oracle as M
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def rand_problem(n, seed):
+    rng = np.random.default_rng(seed)
+    P = M.param_count()
+    p = rng.normal(0, 0.25, P).astype(np.float32)
+    x = rng.normal(0, 1, (9, n)).astype(np.float32)
+    t = rng.uniform(0, 0.05, n).astype(np.float32)
+    norm = np.concatenate([rng.normal(0, 0.1, 9), rng.uniform(0.5, 2, 9)]).astype(np.float32)
+    return p, x, t, norm
+
+
+def gpu_grad(p, x, t, norm):
+    lib = L.load()
+    P = lib.aslb_mlp_param_count()
+    d = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in dict(p=p, x=x, t=t, norm=norm).items()}
+    grad = torch.zeros(P + 1, device="cuda")
+    scratch = torch.zeros(lib.aslb_mlp_grad_scratch_floats(), device="cuda")
+    L.check(lib.aslb_mlp_grad(d["p"].data_ptr(), d["x"].data_ptr(), d["t"].data_ptr(), x.shape[1],
+                              d["norm"].data_ptr(), CL.OUT_SCALE, scratch.data_ptr(), grad.data_ptr(), None), "grad")
+    torch.cuda.synchronize()
+    return grad.cpu().numpy().astype(np.float64)
+
+
+@pytest.mark.parametrize("n", [1, 127, 5000])
+def test_mlp_gradient_matches_oracle(gpu, n):
+    p, x, t, norm = rand_problem(n, 3 + n)
+    g = gpu_grad(p, x, t, norm)
+    sse, want = M.loss_and_grad(p.astype(np.float64), x.astype(np.float64), t.astype(np.float64),
+                                norm.astype(np.float64), CL.OUT_SCALE)
+    P = len(want)
+    assert abs(g[P] - sse) <= 1e-4 * sse + 1e-12
+    scale = np.abs(want).max()
+    assert np.abs(g[:P] - want).max() <= 1e-4 * scale, np.abs(g[:P] - want).max() / scale
+    # deterministic: same bits twice
+    assert np.array_equal(g, gpu_grad(p, x, t, norm))
+
+
+def test_mlp_adam_matches_oracle(gpu):
+    lib = L.load()
+    rng = np.random.default_rng(9)
+    P = M.param_count()
+    p = rng.normal(0, 1, P).astype(np.float32)
+    gr = rng.normal(0, 1, P).astype(np.float32)
+    dp, dg = torch.from_numpy(p.copy()).cuda(), torch.from_numpy(gr).cuda()
+    m, v = torch.zeros(P, device="cuda"), torch.zeros(P, device="cuda")
+    want, mm, vv = p.astype(np.float64), np.zeros(P), np.zeros(P)
+    for step in (1, 2, 3):
+        L.check(lib.aslb_mlp_adam(dp.data_ptr(), dg.data_ptr(), m.data_ptr(), v.data_ptr(), step, 1e-3, 0.9, 0.999,
+                                  1e-8, None), "adam")
+        want, mm, vv = M.adam(want, gr.astype(np.float64), mm, vv, step, 1e-3)
+    assert np.abs(dp.cpu().numpy() - want).max() < 1e-6
+
+
+def test_training_fits_a_known_closure(gpu):
+    """The network learns Cs^2 = 0.02 + 0.015 tanh(x0 - x2) from features."""
+    rng = np.random.default_rng(4)
+    N = 200000
+    X = torch.from_numpy(rng.normal(0.3, 2.0, (9, N)).astype(np.float32)).cuda()
+    T = (0.02 + 0.015 * torch.tanh((X[0] - X[2]) / 2.0)).contiguous()
+    r = CL.train(X, T, iters=600, batch=8192, lr=3e-3)
+    first, last = r.loss[0][1], r.loss[-1][1]
+    assert last < 0.05 * first and last < 2e-6, r.loss
+
+
+def smooth_state(size, steps=4, closure=L.CLOSURE_SMAGORINSKY, storage="f32"):
+    g = tuple(s + 2 for s in size)
+    rng = np.random.default_rng(21)
+    x = np.stack(np.meshgrid(*[np.arange(n) for n in g], indexing="ij")).astype(float)
+    u = np.zeros((3, *g))
+    for d in range(3):
+        k = rng.integers(1, 3, size=3)
+        u[d] = 0.05 * np.sin(2 * np.pi * k[0] * x[0] / size[0]) * np.cos(2 * np.pi * k[1] * x[1] / size[1]) \
+            * np.sin(2 * np.pi * k[2] * x[2] / size[2] + d)
+    lb = A.LBGK(A.Block(size), 0.0002, A.d3q19(), storage=storage, periodic=(True, True, True))
+    lb.setClosure(closure, 0.17)
+    A.LBGKUtilities(lb).initF(u)
+    lb.execute(steps)
+    return lb
+
+
+@pytest.mark.parametrize("steps", [3, 4])
+def test_closure_features_match_oracle(gpu, steps):
+    size = (24, 20, 16)
+    lb = smooth_state(size, steps)
+    got = CL.features(lb).cpu().numpy().astype(np.float64).reshape(9, *size)
+    # the populations the next step reads: f*_i(x - c_i), periodic
+    fs = lb.getF()[:, 1:-1, 1:-1, 1:-1]
+    c = A.lattice_vectors(19)
+    w = A.lattice_weights(19)
+    f = np.stack([np.roll(fs[i], shift=tuple(c[i]), axis=(0, 1, 2)) for i in range(19)])
+    rho, u, P = M.moments_pneq(f, c, w)
+    want = M.features(rho, *u, P)
+    for k in range(9):
+        scale = np.abs(want[k]).max() + 1e-30
+        err = np.abs(got[k] - want[k])
+        assert np.median(err) <= 1e-4 * scale and np.quantile(err, 0.99) <= 2e-3 * scale, (k, err.max() / scale)
+
+
+def test_closure_network_matches_bf16_oracle(gpu):
+    size = (32, 16, 16)
+    lb = smooth_state(size, 4)
+    X = CL.features(lb)
+    rng = np.random.default_rng(5)
+    p = rng.normal(0, 0.2, M.param_count()).astype(np.float32)
+    norm = torch.cat([X.mean(1), 1.0 / X.std(1).clamp(min=1e-12)]).cpu().numpy()
+    lb.setMLP(CL.pack(p, norm))
+    lb.setClosure(L.CLOSURE_MLP)
+    got = lb.getCs2()[1:-1, 1:-1, 1:-1].reshape(-1)
+    want = M.infer_bf16(p, X.cpu().numpy().astype(np.float64), norm.astype(np.float64), CL.OUT_SCALE)
+    rel = np.abs(got - want) / np.abs(want)
+    assert np.median(rel) < 2e-3 and rel.max() < 5e-2, (np.median(rel), rel.max())
+
+
+def test_constant_network_equals_smagorinsky(gpu):
+    """A network whose output is the constant Cs^2 = 0.17^2 gives the
+    Smagorinsky step (same Hou et al. closed form)."""
+    size = (20, 18, 16)
+    a = smooth_state(size, 2, closure=L.CLOSURE_SMAGORINSKY)
+    b = smooth_state(size, 2, closure=L.CLOSURE_NONE)
+    p = np.zeros(M.param_count(), dtype=np.float32)
+    y = np.log(np.expm1(0.17 ** 2 / CL.OUT_SCALE))
+    p[-1] = y
+    norm = np.concatenate([np.zeros(9), np.ones(9)]).astype(np.float32)
+    b.setMLP(CL.pack(p, norm))
+    b.setClosure(L.CLOSURE_MLP)
+    b.setMLPPeriod(3)
+    cs2 = b.getCs2()[1:-1, 1:-1, 1:-1]
+    assert np.allclose(cs2, 0.17 ** 2, rtol=1e-6)
+    b.setF(a.getF())
+    for lb in (a, b):
+        lb.execute(10)
+    assert np.abs(a.getF() - b.getF())[:, 1:-1, 1:-1, 1:-1].max() < 1e-6
+
+
+@pytest.mark.parametrize("period", [1, 3, 4])
+def test_learned_closure_graph_equals_eager(gpu, period):
+    size = (24, 16, 16)
+    out = []
+    for use_graph in (True, False):
+        lb = smooth_state(size, 1, closure=L.CLOSURE_NONE)
+        rng = np.random.default_rng(8)
+        p = rng.normal(0, 0.1, M.param_count()).astype(np.float32)
+        lb.setMLP(CL.pack(p, np.concatenate([np.zeros(9), np.ones(9)]).astype(np.float32)))
+        lb.setClosure(L.CLOSURE_MLP)
+        lb.setMLPPeriod(period)
+        lb.run(3, use_graph=False)
+        lb.run(17, use_graph=use_graph)
+        lb.run(9, use_graph=use_graph)
+        lb.sync()
+        assert lb.steps == 30
+        out.append(lb.getF())
+    assert np.array_equal(out[0], out[1], equal_nan=True)
