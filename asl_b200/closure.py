@@ -10,7 +10,9 @@ Pipeline (D3Q19, FP32):
    coarse grid (n) and the fine grid (2n); the fine samples sit half a fine
    cell off so that a 2x2x2 box average is centred on a coarse cell.
 2. The fine run (2n cubed, nu_fine = 2 nu under acoustic scaling, step 2t
-   against the coarse step t) is box-filtered by 2 at snapshot times.
+   against the coarse step t; Smagorinsky at the fine grid scale, since plain
+   BGK at tau = 0.501 does not stay stable for this field) is box-filtered
+   by 2 at snapshot times.
 3. Targets: the subgrid stress of the box filter, tau_ab = <u_a u_b> -
    <u_a><u_b>, projected on the filtered strain S (3^3-averaged
    least squares), nu_t = max(0, -tau^d : S / (2 S : S)), Cs^2 = nu_t / |S|
@@ -72,20 +74,23 @@ def sample_modes(modes, n_src: int, n: int, shift: float = 0.0):
     """Real field (3, n, n, n) of the modes of an n_src grid on an n grid
     (n >= n_src, zero padding), sampled at x_j = j + shift (grid units of n)."""
     torch = _torch()
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    modes = modes.to(dev)
     h = n_src // 2
-    out = torch.zeros((3, n, n, n // 2 + 1), dtype=torch.complex128)
+    out = torch.zeros((3, n, n, n // 2 + 1), dtype=torch.complex128, device=dev)
     idx = list(range(0, h)) + list(range(n - h, n))
     src = list(range(0, h)) + list(range(n_src - h, n_src))
-    ii = torch.tensor(idx)
-    ss = torch.tensor(src)
-    out[:, ii[:, None, None], ii[None, :, None], torch.arange(h)[None, None, :]] = \
-        modes[:, ss[:, None, None], ss[None, :, None], torch.arange(h)[None, None, :]]
+    ii = torch.tensor(idx, device=dev)
+    ss = torch.tensor(src, device=dev)
+    hz = torch.arange(h, device=dev)
+    out[:, ii[:, None, None], ii[None, :, None], hz[None, None, :]] = \
+        modes[:, ss[:, None, None], ss[None, :, None], hz[None, None, :]]
     if shift != 0.0:
-        kx = torch.fft.fftfreq(n, 1.0 / n)
-        kz = torch.fft.rfftfreq(n, 1.0 / n)
+        kx = torch.fft.fftfreq(n, 1.0 / n, device=dev)
+        kz = torch.fft.rfftfreq(n, 1.0 / n, device=dev)
         ph = torch.exp(1j * 2 * math.pi * shift / n * (kx[:, None, None] + kx[None, :, None] + kz[None, None, :]))
         out = out * ph
-    return torch.fft.irfftn(out, s=(n, n, n), dim=(1, 2, 3)) * (n / n_src) ** 3
+    return (torch.fft.irfftn(out, s=(n, n, n), dim=(1, 2, 3)) * (n / n_src) ** 3).cpu()
 
 
 def turbulence_field(n: int, seed: int, fine: bool = False):
@@ -138,11 +143,11 @@ def _ghost(u):
     return np.pad(u, ((0, 0), (1, 1), (1, 1), (1, 1)), mode="wrap")
 
 
-def make_lbgk(n: int, tau: float, u0, closure=L.CLOSURE_NONE, storage="f32"):
+def make_lbgk(n: int, tau: float, u0, closure=L.CLOSURE_NONE, storage="f32", cs=CS_SMAG):
     lb = A.LBGK(A.Block((n, n, n)), (tau - 0.5) / 3.0, A.d3q19(), compVel=False, compRho=False, storage=storage,
                 periodic=(True, True, True))
     if closure == L.CLOSURE_SMAGORINSKY:
-        lb.setClosure(closure, CS_SMAG)
+        lb.setClosure(closure, cs)
     A.LBGKUtilities(lb).initF(_ghost(u0))
     return lb
 
@@ -273,7 +278,7 @@ def study(n=256, seed=20261207, times=(250, 500, 1000), train_times=(200, 400, 6
     # fine run: snapshots for training (2 t) and for the judge (2 t)
     t0 = time.perf_counter()
     uf0 = turbulence_field(n, seed, fine=True)
-    fine = make_lbgk(2 * n, tau_f, uf0)
+    fine = make_lbgk(2 * n, tau_f, uf0, closure=L.CLOSURE_SMAGORINSKY)
     del uf0
     snap = sorted(set(2 * t for t in times) | set(2 * t for t in train_times))
     ref_E, train_sets = {}, []
@@ -304,6 +309,8 @@ def study(n=256, seed=20261207, times=(250, 500, 1000), train_times=(200, 400, 6
     del Xs, Ts, train_sets
     ok = torch.isfinite(X).all(0) & torch.isfinite(T)
     X, T = X[:, ok].contiguous(), T[ok].contiguous()
+    if T.numel() == 0:
+        raise RuntimeError("closure study: no finite training samples (the fine run diverged)")
     res["train_samples"] = int(T.numel())
     res["target_mean_cs2"] = float(T.mean())
     t1 = time.perf_counter()
@@ -315,11 +322,17 @@ def study(n=256, seed=20261207, times=(250, 500, 1000), train_times=(200, 400, 6
     res["smag_loss"] = float(((T - CS_SMAG ** 2) ** 2).mean())
     del X, T
     log("trained: loss %s (constant %.3g, Smagorinsky %.3g)" % (tr.loss[-1], res["const_loss"], res["smag_loss"]))
-    # judge: coarse runs from the coarse field
+    # judge: coarse runs from the coarse field. "smagorinsky_fit" uses the
+    # constant Cs^2 that best fits the same targets (their mean): what the
+    # network adds beyond calibrating one constant.
     uc0 = turbulence_field(n, seed)
+    cs_fit = math.sqrt(res["target_mean_cs2"])
+    res["cs_fit"] = cs_fit
     runs = {}
-    for name in ("none", "smagorinsky", "learned"):
-        lb = make_lbgk(n, tau_c, uc0, closure=L.CLOSURE_SMAGORINSKY if name == "smagorinsky" else L.CLOSURE_NONE)
+    for name in ("none", "smagorinsky", "smagorinsky_fit", "learned"):
+        smag = name.startswith("smagorinsky")
+        lb = make_lbgk(n, tau_c, uc0, closure=L.CLOSURE_SMAGORINSKY if smag else L.CLOSURE_NONE,
+                       cs=cs_fit if name == "smagorinsky_fit" else CS_SMAG)
         if name == "learned":
             lb.setMLP(tr.blob)
             lb.setMLPPeriod(period)
@@ -336,3 +349,32 @@ def study(n=256, seed=20261207, times=(250, 500, 1000), train_times=(200, 400, 6
     res["runs"] = runs
     res["blob"] = tr.blob
     return res
+
+
+def closure_speed(n: int, blob: bytes, steps: int = 200, period: int = 8, seed: int = 20261207):
+    """MLUPS of the plain, Smagorinsky and learned steps on an n^3 periodic
+    turbulence field (CUDA graph, CUDA events on the domain's stream)."""
+    torch = _torch()
+    u0 = turbulence_field(n, seed)
+    out = {}
+    for name in ("plain", "smagorinsky", "learned"):
+        lb = make_lbgk(n, 0.5005, u0, closure=L.CLOSURE_SMAGORINSKY if name == "smagorinsky" else L.CLOSURE_NONE)
+        if name == "learned":
+            lb.setMLP(blob)
+            lb.setMLPPeriod(period)
+            lb.setClosure(L.CLOSURE_MLP)
+        st = torch.cuda.ExternalStream(lb.stream)
+        lb.run(2 * period, use_graph=True)
+        lb.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        lb.run(steps, use_graph=True)
+        e1.record(st)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        out[name] = {"mlups": n ** 3 * steps / t / 1e6, "ms_per_step": t / steps * 1e3}
+        del lb
+    out["learned_overhead_vs_smagorinsky"] = out["smagorinsky"]["mlups"] / out["learned"]["mlups"] - 1.0
+    out["period"] = period
+    out["steps"] = steps
+    return out

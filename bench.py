@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--batch-steps", type=int, default=2000,
                     help="timed steps of the 256-domain batch (0: skip)")
     ap.add_argument("--batch-domains", type=int, default=256)
+    ap.add_argument("--closure-size", type=int, default=256,
+                    help="coarse grid of the learned-closure study (fine = 2x; 0: skip)")
     return ap.parse_args()
 
 
@@ -276,6 +278,19 @@ def vehicle_run(W, size, steps: int, peak: float):
     return res
 
 
+def closure_run(n: int):
+    """Decaying turbulence at n^3 (fine run 2n^3): the learned closure trained
+    on the filtered fine run by the library's kernels, judged by the energy
+    spectrum against Smagorinsky (Cs 0.17 and the best constant), plus the
+    step rates."""
+    from asl_b200 import closure as CL
+    res = CL.study(n=n, log=lambda *a: None)
+    blob = res.pop("blob")
+    res["speed"] = CL.closure_speed(n, blob)
+    res["metric"] = "relative L2 of log E(k), 2 <= k <= n/4, against the 2x box-filtered fine run"
+    return res
+
+
 def batch_run(W, n: int, steps: int, peak: float):
     """Many small domains (seeded channels of random size, viscosity, obstacle
     and inlet velocity): the batch (one persistent stream-collide launch per
@@ -456,6 +471,9 @@ def run_ours(args):
     batched = None
     if world == 1 and args.batch_steps > 0:
         batched = batch_run(W, args.batch_domains, args.batch_steps, peak)
+    learned = None
+    if world == 1 and args.closure_size > 0:
+        learned = closure_run(args.closure_size)
     vehicle = None
     if world == 1 and args.q27_steps > 0:
         vehicle = vehicle_run(W, parse_size(args.q27_size), args.q27_steps, peak)
@@ -488,7 +506,8 @@ def run_ours(args):
                 "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "clocks": clk,
                 "gpu_launches": K * head["launches_per_step"],
                 "separate_conditions": sep, "tma_kernel": direct, "fp16": fp16, "accuracy": accuracy,
-                "d3q27_vehicle": vehicle, "batched_domains": batched, "finite": finite, "mass": mom[0]}
+                "d3q27_vehicle": vehicle, "batched_domains": batched, "learned_closure": learned,
+                "finite": finite, "mass": mom[0]}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
