@@ -55,23 +55,40 @@ constexpr int kFieldThreads = 256;
 constexpr int kFieldWarps = kFieldThreads / 32;
 
 template <int Q, class S, bool ODD, bool FUSED>
-__global__ void __launch_bounds__(kFieldThreads)
+__global__ void __launch_bounds__(kFieldThreads, 3)
     k_closure_field(const S* __restrict__ F, const GridDesc g, const StepParams p, const MlpNet* __restrict__ net,
                     float* __restrict__ cs2) {
-  __shared__ __align__(16) __nv_bfloat16 w1[kMlpHidden][kMlpInPad];
-  __shared__ __align__(16) __nv_bfloat16 w2[kMlpHidden][kMlpHidden];
-  __shared__ __align__(16) __nv_bfloat16 xs[kFieldWarps][32][kMlpInPad];
+  // rows padded by 8 BF16 (16 bytes) so that the eight rows a fragment load
+  // touches fall in different banks
+  __shared__ __align__(16) __nv_bfloat16 w1[kMlpHidden][kMlpInPad + 8];
+  __shared__ __align__(16) __nv_bfloat16 w2[kMlpHidden][kMlpHidden + 8];
+  __shared__ __align__(16) __nv_bfloat16 xs[kFieldWarps][32][kMlpInPad + 8];
   __shared__ float ys[kFieldWarps][32];
+  __shared__ float vb1[kMlpHidden], vb2[kMlpHidden], vw3[kMlpHidden], vin[2 * kMlpInPad];
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   {
     const uint32_t* s1 = reinterpret_cast<const uint32_t*>(&net->w1[0][0]);
     const uint32_t* s2 = reinterpret_cast<const uint32_t*>(&net->w2[0][0]);
-    uint32_t* d1 = reinterpret_cast<uint32_t*>(&w1[0][0]);
-    uint32_t* d2 = reinterpret_cast<uint32_t*>(&w2[0][0]);
     const int nt = blockDim.x * blockDim.y;
-    for (int i = tid; i < kMlpHidden * kMlpInPad / 2; i += nt) d1[i] = s1[i];
-    for (int i = tid; i < kMlpHidden * kMlpHidden / 2; i += nt) d2[i] = s2[i];
+    for (int i = tid; i < kMlpHidden * kMlpInPad / 2; i += nt) {
+      const int r = i / (kMlpInPad / 2), c = i % (kMlpInPad / 2);
+      *reinterpret_cast<uint32_t*>(&w1[r][2 * c]) = s1[i];
+    }
+    for (int i = tid; i < kMlpHidden * kMlpHidden / 2; i += nt) {
+      const int r = i / (kMlpHidden / 2), c = i % (kMlpHidden / 2);
+      *reinterpret_cast<uint32_t*>(&w2[r][2 * c]) = s2[i];
+    }
+    for (int i = tid; i < kMlpHidden; i += nt) {
+      vb1[i] = net->b1[i];
+      vb2[i] = net->b2[i];
+      vw3[i] = __bfloat162float(net->w3[i]);
+    }
+    for (int i = tid; i < kMlpInPad; i += nt) {
+      vin[i] = net->in_shift[i];
+      vin[kMlpInPad + i] = net->in_scale[i];
+    }
   }
+  __syncthreads();
   const int warp = tid >> 5, lane = tid & 31;
   const int z = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -83,19 +100,20 @@ __global__ void __launch_bounds__(kFieldThreads)
   if (valid) {
     cell_features<Q, S, ODD, FUSED>(F, g, p, x, y, z, s, feat);
   } else {
-    for (int k = 0; k < kMlpIn; ++k) feat[k] = net->in_shift[k];
+    for (int k = 0; k < kMlpIn; ++k) feat[k] = vin[k];
   }
 #pragma unroll
   for (int k = 0; k < kMlpInPad; k += 2) {
-    const float a = k < kMlpIn ? (feat[k] - net->in_shift[k]) * net->in_scale[k] : 0.f;
-    const float b = k + 1 < kMlpIn ? (feat[k + 1] - net->in_shift[k + 1]) * net->in_scale[k + 1] : 0.f;
+    const float a = k < kMlpIn ? (feat[k] - vin[k]) * vin[kMlpInPad + k] : 0.f;
+    const float b = k + 1 < kMlpIn ? (feat[k + 1] - vin[k + 1]) * vin[kMlpInPad + k + 1] : 0.f;
     *reinterpret_cast<uint32_t*>(&xs[warp][lane][k]) = pack_bf16(a, b);
   }
   __syncthreads();
 
   const int gr = lane >> 2, c0 = (lane & 3) * 2;
-  // layer 1: H1 = relu(X W1^T + b1), 32 x 64, as 2 x 8 tiles of 16 x 8
-  float h[2][8][4];
+  // layer 1: H1 = relu(X W1^T + b1), 32 x 64, as 2 x 8 tiles of 16 x 8; each
+  // m-tile's FP32 output becomes the BF16 A fragments of layer 2 (K = 64) in place
+  uint32_t ha[2][4][4];
 #pragma unroll
   for (int mt = 0; mt < 2; ++mt) {
     uint32_t a[4];
@@ -105,34 +123,32 @@ __global__ void __launch_bounds__(kFieldThreads)
     a[2] = *reinterpret_cast<const uint32_t*>(&xs[warp][r0][c0 + 8]);
     a[3] = *reinterpret_cast<const uint32_t*>(&xs[warp][r0 + 8][c0 + 8]);
 #pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      const int n = nt * 8 + gr;
-      const float bb0 = net->b1[nt * 8 + c0], bb1 = net->b1[nt * 8 + c0 + 1];
-      h[mt][nt][0] = bb0;
-      h[mt][nt][1] = bb1;
-      h[mt][nt][2] = bb0;
-      h[mt][nt][3] = bb1;
-      mma16816(h[mt][nt], a, *reinterpret_cast<const uint32_t*>(&w1[n][c0]),
-               *reinterpret_cast<const uint32_t*>(&w1[n][c0 + 8]));
+    for (int j = 0; j < 4; ++j) {
+      float h[2][4];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int nt = 2 * j + q;
+        const int n = nt * 8 + gr;
+        const float bb0 = vb1[nt * 8 + c0], bb1 = vb1[nt * 8 + c0 + 1];
+        h[q][0] = bb0;
+        h[q][1] = bb1;
+        h[q][2] = bb0;
+        h[q][3] = bb1;
+        mma16816(h[q], a, *reinterpret_cast<const uint32_t*>(&w1[n][c0]),
+                 *reinterpret_cast<const uint32_t*>(&w1[n][c0 + 8]));
+      }
+      ha[mt][j][0] = pack_bf16(fmaxf(h[0][0], 0.f), fmaxf(h[0][1], 0.f));
+      ha[mt][j][1] = pack_bf16(fmaxf(h[0][2], 0.f), fmaxf(h[0][3], 0.f));
+      ha[mt][j][2] = pack_bf16(fmaxf(h[1][0], 0.f), fmaxf(h[1][1], 0.f));
+      ha[mt][j][3] = pack_bf16(fmaxf(h[1][2], 0.f), fmaxf(h[1][3], 0.f));
     }
   }
-  // layer 2: the FP32 tiles of H1 become BF16 A fragments of K = 64 in place
-  uint32_t ha[2][4][4];
-#pragma unroll
-  for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      ha[mt][j][0] = pack_bf16(fmaxf(h[mt][2 * j][0], 0.f), fmaxf(h[mt][2 * j][1], 0.f));
-      ha[mt][j][1] = pack_bf16(fmaxf(h[mt][2 * j][2], 0.f), fmaxf(h[mt][2 * j][3], 0.f));
-      ha[mt][j][2] = pack_bf16(fmaxf(h[mt][2 * j + 1][0], 0.f), fmaxf(h[mt][2 * j + 1][1], 0.f));
-      ha[mt][j][3] = pack_bf16(fmaxf(h[mt][2 * j + 1][2], 0.f), fmaxf(h[mt][2 * j + 1][3], 0.f));
-    }
   float yp[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // [mt][row g, row g + 8]
 #pragma unroll
   for (int nt = 0; nt < 8; ++nt) {
     const int n = nt * 8 + gr;
-    const float bb0 = net->b2[nt * 8 + c0], bb1 = net->b2[nt * 8 + c0 + 1];
-    const float v0 = __bfloat162float(net->w3[nt * 8 + c0]), v1 = __bfloat162float(net->w3[nt * 8 + c0 + 1]);
+    const float bb0 = vb2[nt * 8 + c0], bb1 = vb2[nt * 8 + c0 + 1];
+    const float v0 = vw3[nt * 8 + c0], v1 = vw3[nt * 8 + c0 + 1];
 #pragma unroll
     for (int mt = 0; mt < 2; ++mt) {
       float acc[4] = {bb0, bb1, bb0, bb1};
