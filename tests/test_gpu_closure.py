@@ -2,8 +2,6 @@
 oracle (gradient, Adam), the feature kernel against features recomputed on
 the CPU from the exported populations, the tensor-core network against its
 BF16 oracle, and the closure's stream-collide against Smagorinsky."""
-import ctypes as C
-
 import numpy as np
 import pytest
 
@@ -175,8 +173,7 @@ def test_trained_closure_beats_smagorinsky_on_spectrum(gpu):
     """The whole study at 64^3 (fine 128^3): the network trained on the
     filtered fine run matches the fine spectrum better than Smagorinsky with
     Cs = 0.17 at every time, and better on average than Smagorinsky with the
-    best constant fitted to the same targets; plain BGK at tau 0.5005 does
-    not stay finite."""
+    best constant fitted to the same targets."""
     res = CL.study(n=64, iters=800, log=lambda *a: None)
     runs = res["runs"]
     le = runs["learned"]["spectrum_rel_l2_logE"]
