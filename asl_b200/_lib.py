@@ -15,6 +15,7 @@ ASLB_OK = 0
 F32, F16, F64 = 0, 1, 2
 NO_VELOCITY, NO_RHO, INCOMPRESSIBLE = 1, 2, 4
 PERIODIC_X, PERIODIC_Y, PERIODIC_Z = 8, 16, 32
+PACKED_ROWS = 64
 CLOSURE_NONE, CLOSURE_ASL_INTENT, CLOSURE_SMAGORINSKY, CLOSURE_MLP = 0, 1, 2, 3
 BC_NOSLIP, BC_VELOCITY, BC_PRESSURE, BC_PRESSURE_VELOCITY = 0, 1, 2, 3
 BC_MAP_NOSLIP, BC_MAP_VELOCITY, BC_MAP_VELOCITY_ROTATION, BC_MAP_PRESSURE_VELOCITY = 10, 11, 12, 13

@@ -378,3 +378,29 @@ def closure_speed(n: int, blob: bytes, steps: int = 192, period: int = 16, seed:
     out["period"] = period
     out["steps"] = steps
     return out
+
+
+def _main(argv=None):
+    """python -m asl_b200.closure study [--n N] | speed [--n N] [--steps K]"""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(prog="python -m asl_b200.closure")
+    ap.add_argument("what", choices=["study", "speed"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=192)
+    ap.add_argument("--period", type=int, default=16)
+    a = ap.parse_args(argv)
+    if a.what == "study":
+        res = study(n=a.n, period=a.period)
+        res.pop("blob")
+    else:
+        # the step rate does not depend on the weights: a seeded random network
+        rng = np.random.default_rng(5)
+        p = rng.normal(0, 0.1, L.load().aslb_mlp_param_count()).astype(np.float32)
+        blob = pack(p, np.concatenate([np.zeros(9), np.ones(9)]).astype(np.float32))
+        res = closure_speed(a.n, blob, steps=a.steps, period=a.period)
+    print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    _main()

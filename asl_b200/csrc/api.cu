@@ -355,10 +355,16 @@ int aslb_lbgk_create(int nx, int ny, int nz, int q, int storage, double nu, unsi
   g.nx = nx; g.ny = ny; g.nz = nz;
   g.gx = nx + 2; g.gy = ny + 2; g.gz = nz + 2;
   // Rows aligned to 128 bytes: the first interior cell (z = 1) of every row at
-  // a multiple of `align` elements.
+  // a multiple of `align` elements; or, with ASLB_PACKED_ROWS, rows back to
+  // back (each direction array still starts on a 128-byte boundary).
   const int align = int(128 / storage_bytes(storage));
-  g.zoff = align - 1;
-  g.pitch = ((g.gz + g.zoff + align - 1) / align) * align;
+  if (flags & ASLB_PACKED_ROWS) {
+    g.zoff = 0;
+    g.pitch = g.gz;
+  } else {
+    g.zoff = align - 1;
+    g.pitch = ((g.gz + g.zoff + align - 1) / align) * align;
+  }
   g.periodic = int((flags >> 3) & 7u);
   g.plane = (long long)g.gy * g.pitch;
   g.dstride = (((long long)g.gx * g.plane + align - 1) / align) * align;
@@ -730,6 +736,8 @@ int aslb_lbgk_sync(aslb_lbgk* h) {
 int aslb_lbgk_set_kernel(aslb_lbgk* h, int variant) {
   ASLB_CHECK_HANDLE(h);
   if (variant < 0 || variant > 2) return fail(ASLB_ERR_ARG, "aslb_lbgk_set_kernel: variant must be 0, 1 or 2");
+  if (variant == 1 && (h->flags & ASLB_PACKED_ROWS))
+    return fail(ASLB_ERR_ARG, "aslb_lbgk_set_kernel: the TMA-staged kernel needs aligned rows (no ASLB_PACKED_ROWS)");
   h->d.variant = variant;
   h->version++;
   return ASLB_OK;

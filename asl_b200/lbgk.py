@@ -123,18 +123,20 @@ class LBGK:
 
     ``storage`` picks the population format: "f32" (ASL with FlT=float), "f64"
     (FlT=double) or "f16" (shifted FP16 deviations, FP32 arithmetic).
-    ``periodic`` (x, y, z) and ``body_force`` are extensions without an ASL
-    analogue."""
+    ``periodic`` (x, y, z), ``body_force`` and ``packed_rows`` (z rows back to
+    back, for short rows) are extensions without an ASL analogue."""
 
     closure = L.CLOSURE_NONE
 
     def __init__(self, block: Block, nu: float, vt: VectorTemplate, compVel: bool = True, compRho: bool = True,
-                 storage="f32", periodic=(False, False, False), body_force=None):
+                 storage="f32", periodic=(False, False, False), body_force=None, packed_rows: bool = False):
         self.lib = L.load()
         self.block = block
         self.vectorTemplate = vt
         st = _STORAGE[storage]
         flags = (0 if compVel else L.NO_VELOCITY) | (0 if compRho else L.NO_RHO)
+        if packed_rows:
+            flags |= L.PACKED_ROWS
         for a, p in enumerate(periodic):
             if p:
                 flags |= (L.PERIODIC_X, L.PERIODIC_Y, L.PERIODIC_Z)[a]

@@ -88,7 +88,8 @@ def porous_channel(size=(512, 256, 256), rmin=4.0, rmax=12.0, solid_fraction=0.4
                     info={"spheres": int(len(pack.radii)), "solid_fraction": solid, "seed": seed, "tau": tau})
 
 
-def build_lbgk(w: Workload, storage="f32", compVel=True, compRho=True, closure_cls=None, fuse=False):
+def build_lbgk(w: Workload, storage="f32", compVel=True, compRho=True, closure_cls=None, fuse=False,
+               packed_rows=False):
     """Instantiate the workload on the GPU through the ASL-style API. With
     ``fuse`` the trailing no-slip conditions (walls and map, which every
     workload lists after its other conditions) are folded into the
@@ -98,7 +99,7 @@ def build_lbgk(w: Workload, storage="f32", compVel=True, compRho=True, closure_c
     cls = closure_cls or A.LBGK
     block = A.Block(w.size, w.dx, w.position)
     lb = cls(block, w.nu, vt, compVel=compVel, compRho=compRho, storage=storage, periodic=w.periodic,
-             body_force=w.body_force)
+             body_force=w.body_force, packed_rows=packed_rows)
     lb.init()
     A.LBGKUtilities(lb).initF(w.init_u)
     bcs = []
@@ -196,12 +197,13 @@ def batch_channels(n=256, steps=2000, seed=BASE_SEED + 3) -> list:
     return out
 
 
-def build_batch(ws, storage="f32", fuse=True):
-    """All workloads of a batch on the GPU plus the Batch that steps them."""
+def build_batch(ws, storage="f32", fuse=True, packed_rows=True):
+    """All workloads of a batch on the GPU plus the Batch that steps them
+    (short z rows: packed by default)."""
     from . import lbgk as A
     lbs, bcs = [], []
     for w in ws:
-        lb, bc = build_lbgk(w, storage=storage, compVel=False, compRho=False, fuse=fuse)
+        lb, bc = build_lbgk(w, storage=storage, compVel=False, compRho=False, fuse=fuse, packed_rows=packed_rows)
         lbs.append(lb)
         bcs.append(bc)
     return A.Batch(lbs), lbs, bcs

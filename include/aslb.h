@@ -49,6 +49,12 @@ extern "C" {
 #define ASLB_PERIODIC_X 8u     /* extension: periodic axes (no ASL analogue) */
 #define ASLB_PERIODIC_Y 16u
 #define ASLB_PERIODIC_Z 32u
+/* extension: z rows stored back to back instead of each row's first interior
+ * cell on a 128-byte boundary. Fewer HBM bytes when rows are short (below
+ * about 100 FP32 cells: the +-1 z neighbours then share the fetched pieces
+ * of the adjacent rows); results are identical. The TMA-staged kernel
+ * (variant 1) needs aligned rows and is unavailable. */
+#define ASLB_PACKED_ROWS 64u
 
 /* closures (aslb_lbgk_set_closure) */
 #define ASLB_CLOSURE_NONE 0        /* asl::LBGK                                        */

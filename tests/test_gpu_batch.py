@@ -27,7 +27,7 @@ def test_batch_bitwise_equals_separate_domains(gpu, storage, fuse, use_graph):
     batch, lbs, bcs = W.build_batch(ws, storage=storage, fuse=fuse)
     batch.run(steps, bcs, use_graph=use_graph)
     batch.sync()
-    for w, lb in zip(ws, lbs):
+    for w, lb in zip(ws, lbs):  # references in the aligned-row layout
         ref, rbcs = W.build_lbgk(w, storage=storage, compVel=False, compRho=False, fuse=fuse)
         ref.run(steps, rbcs)
         ref.sync()

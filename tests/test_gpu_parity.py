@@ -410,3 +410,26 @@ def test_vehicle_d3q27_downscale_matches_oracle(gpu, oracle_mod, storage, prec, 
     want = o.force(w.map, r0=(0.0, 0.0, 0.0))
     for a in (0, 2):  # drag, lift
         assert abs(got[a] - want[a]) <= (1e-9 if storage == "f64" else 1e-3) * max(abs(want[a]), 1e-6)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
+@pytest.mark.parametrize("variant", [0, 2])
+def test_packed_rows_bitwise_equal_aligned_rows(gpu, storage, variant):
+    """The packed-row layout gives the same populations, rho and u as the
+    aligned one (cylinder channel: velocity, pressure, fused walls and map)."""
+    w = W.channel_cylinder(size=(40, 24, 20), radius=4.0, center=(10.0, 12.0))
+    out = []
+    for packed in (False, True):
+        lb, bcs = W.build_lbgk(w, storage=storage, fuse=True, packed_rows=packed)
+        lb.setKernel(variant)
+        lb.run(11, bcs)
+        lb.sync()
+        out.append((lb.getF(), lb.getVelocity(), lb.getRho()))
+    for a, b in zip(*out):
+        assert np.array_equal(a, b, equal_nan=True)
+
+
+def test_packed_rows_reject_tma_variant(gpu):
+    lb = A.LBGK(A.Block((8, 8, 8)), 0.02, A.d3q19(), packed_rows=True)
+    with pytest.raises(A.L.ASLError):
+        lb.setKernel(1)
