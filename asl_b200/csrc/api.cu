@@ -68,6 +68,9 @@ struct aslb_lbgk {
   bool fresh = true;
   std::vector<uint2> mask_host;
   uint2* mask_dev = nullptr;
+  // one word per cell when no cell has both bounce and elide bits (bit 31:
+  // the low bits are elide bits), read by the two-cells-per-thread kernel
+  uint32_t* mask32_dev = nullptr;
   // conditions and force objects made on this domain; destroying the domain
   // releases their device memory and detaches them (any destruction order)
   std::vector<aslb_bc*> bcs;
@@ -124,6 +127,7 @@ void prepare_params(aslb_lbgk* h) {
   h->p.write_macro = h->p.write_rho | h->p.write_vel;
   h->p.cs2 = h->cs2_field;
   h->p.mask = h->fresh ? nullptr : h->mask_dev;
+  h->p.mask32 = h->fresh ? nullptr : h->mask32_dev;
 }
 
 bool mlp_due(const aslb_lbgk* h) {
@@ -452,6 +456,7 @@ int aslb_lbgk_destroy(aslb_lbgk* h) {
   cudaFree(h->mlp_dev);
   cudaFree(h->cs2_field);
   cudaFree(h->mask_dev);
+  cudaFree(h->mask32_dev);
   cudaFree(h->red_partials);
   cudaFree(h->red_out);
   cudaFree(h->d.err);
@@ -1009,6 +1014,22 @@ int aslb_bc_fuse(aslb_bc* bc) {
                                 wrapc(h, an.z + lattice_c(q, k, 2), 2));
       add(sa, interior(g, ax, ay, az), sf, k);
     }
+  // the compact form exists when every cell is either a bounce-back reader or
+  // a skipped writer
+  bool compact = true;
+  for (const uint2& w : m)
+    if (w.x && w.y) {
+      compact = false;
+      break;
+    }
+  cudaFree(h->mask32_dev);
+  h->mask32_dev = nullptr;
+  if (compact) {
+    std::vector<uint32_t> m32(m.size());
+    for (size_t i = 0; i < m.size(); ++i) m32[i] = m[i].y ? (m[i].y | 0x80000000u) : m[i].x;
+    ASLB_CUDA(cudaMalloc((void**)&h->mask32_dev, ((size_t)g.dstride + 4096) * sizeof(uint32_t)));
+    ASLB_CUDA(cudaMemcpy(h->mask32_dev, m32.data(), m32.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  }
   if (!h->mask_dev) ASLB_CUDA(cudaMalloc((void**)&h->mask_dev, ((size_t)g.dstride + 4096) * sizeof(uint2)));
   ASLB_CUDA(cudaStreamSynchronize(h->stream));
   ASLB_CUDA(cudaMemcpy(h->mask_dev, m.data(), m.size() * sizeof(uint2), cudaMemcpyHostToDevice));

@@ -79,6 +79,9 @@ struct StepParams {
   // its bits (FP32/FP64 skip the store; FP16 stores back what it holds, so
   // that warps write whole sectors).
   const uint2* mask;
+  // The same links in one word per cell, when no cell has both kinds: bit 31
+  // set = the low bits are elide bits, clear = bounce bits (or null).
+  const uint32_t* mask32;
 };
 
 // ---- storage formats -------------------------------------------------------

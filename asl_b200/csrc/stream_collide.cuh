@@ -164,7 +164,8 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, CL, FUSED>::blocks)
 // D3Q15/D3Q19 domains with fused links, at three blocks (80 registers) per
 // SM; without fused links the schedule hoists every address of both cells
 // (over 128 registers) and the one-cell kernel is faster.
-template <int Q, class S, bool ODD, bool FUSED>
+// M32: the links come from the one-word mask (p.mask32).
+template <int Q, class S, bool ODD, bool FUSED, bool M32>
 __global__ void __launch_bounds__(256, 3)
     k_stream_collide_pair(S* __restrict__ F, const GridDesc g, const StepParams p,
                           typename MacroT<S>::T* __restrict__ rho_out, typename MacroT<S>::T* __restrict__ u_out) {
@@ -180,7 +181,11 @@ __global__ void __launch_bounds__(256, 3)
   const unsigned sa = (unsigned)sidx(g, x, y, za);
   const unsigned sb = sa + 32u;
   uint2 ma = make_uint2(0u, 0u), mb = make_uint2(0u, 0u);
-  if (FUSED) {
+  if (FUSED && M32) {
+    const uint32_t wa = p.mask32[sa], wb = has_b ? p.mask32[sb] : 0u;
+    ma = (wa >> 31) ? make_uint2(0u, wa & 0x7fffffffu) : make_uint2(wa, 0u);
+    mb = (wb >> 31) ? make_uint2(0u, wb & 0x7fffffffu) : make_uint2(wb, 0u);
+  } else if (FUSED) {
     ma = p.mask[sa];
     if (has_b) mb = p.mask[sb];
   }
@@ -227,10 +232,14 @@ cudaError_t step_q_s_cl(const DomainDev& d, const StepParams& p, int parity_in, 
   if constexpr (CL == CL_NONE && Q != 27 && !std::is_same<S, double>::value) {
     if (d.variant == 0 && fused) {
       pair_launch_shape(d.g, grid, block);
-      if (parity_in == 0)
-        k_stream_collide_pair<Q, S, true, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
-      else
-        k_stream_collide_pair<Q, S, false, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+      const bool m32 = p.mask32 != nullptr;
+      if (parity_in == 0) {
+        if (m32) k_stream_collide_pair<Q, S, true, true, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+        else k_stream_collide_pair<Q, S, true, true, false><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+      } else {
+        if (m32) k_stream_collide_pair<Q, S, false, true, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+        else k_stream_collide_pair<Q, S, false, true, false><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+      }
       return cudaGetLastError();
     }
   }

@@ -433,3 +433,28 @@ def test_packed_rows_reject_tma_variant(gpu):
     lb = A.LBGK(A.Block((8, 8, 8)), 0.02, A.d3q19(), packed_rows=True)
     with pytest.raises(A.L.ASLError):
         lb.setKernel(1)
+
+
+def test_fused_cells_with_both_link_kinds(gpu):
+    """Map A is solid for x <= 5, map B (inside A) for x <= 5 and y <= 3: the
+    cells x = 5, y >= 4 are skipped writers (anchors) for A and bounce-back
+    readers (fluid ends) for B, so the one-word mask cannot hold them; fused
+    and separate conditions still agree bit for bit."""
+    size = (16, 10, 12)
+    g = tuple(s + 2 for s in size)
+    pos = np.stack(np.meshgrid(*[np.arange(n) - 1.0 for n in g], indexing="ij"))
+    map_a = np.clip((pos[0] - 5.5) / 1.8, -1, 1).astype(np.float32)
+    map_b = np.clip(np.maximum(pos[0] - 5.5, pos[1] - 3.5) / 1.8, -1, 1).astype(np.float32)
+    out = []
+    for fuse in (False, True):
+        lb = A.LBGK(A.Block(size), 0.02, A.d3q19(), periodic=(False, True, True))
+        rho, u = smooth_field(g, 31)
+        A.LBGKUtilities(lb).initF(rho, u)
+        bcs = [A.generateBCNoSlip(lb, [A.X0, A.XE]), A.generateBCNoSlip(lb, map_a), A.generateBCNoSlip(lb, map_b)]
+        if fuse:
+            for b in bcs:
+                b.fuse()
+        lb.run(9, bcs)
+        lb.sync()
+        out.append(lb.getF())
+    assert np.array_equal(out[0], out[1], equal_nan=True)
