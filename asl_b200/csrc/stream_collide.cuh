@@ -44,11 +44,12 @@ __device__ __forceinline__ void nb_offsets(const GridDesc& g, int x, int y, int 
 // four blocks (64 registers) with fused links, whose per-direction slot
 // selects keep the schedule compact; three (80 registers) without, where the
 // compiler hoists all addresses and 64 registers would spill (two, 128
-// registers, for D3Q27). Two for FP64 and the closures.
+// registers, for D3Q27). Three (80 registers) for the closures, two for FP64.
 template <int Q, class S, int CL, bool FUSED>
 struct StepOccupancy {
-  static constexpr int blocks =
-      (CL == CL_NONE && !std::is_same<S, double>::value) ? (FUSED ? 4 : (Q == 27 ? 2 : 3)) : 2;
+  static constexpr int blocks = std::is_same<S, double>::value
+                                    ? 2
+                                    : (CL == CL_NONE ? (FUSED ? 4 : (Q == 27 ? 2 : 3)) : 3);
 };
 
 // Store one outgoing population. An elided slot keeps its bits: FP32/FP64
