@@ -85,6 +85,10 @@ PROTOTYPES = {
     "aslb_mlp_grad": (C.c_int, [_vp, _vp, _vp, C.c_longlong, _vp, C.c_float, _vp, _vp, _vp]),
     "aslb_mlp_adam": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, _vp]),
     "aslb_mlp_pack": (C.c_int, [_vp, _vp, C.c_float, _vp]),
+    "aslb_lbgk_halo_bytes": (C.c_size_t, [_vp]),
+    "aslb_lbgk_halo_pack": (C.c_int, [_vp, C.c_int, _vp]),
+    "aslb_lbgk_halo_unpack": (C.c_int, [_vp, C.c_int, _vp]),
+    "aslb_lbgk_parity": (C.c_int, [_vp]),
     "aslb_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(_vp)]),
     "aslb_batch_run": (C.c_int, [_vp, C.c_int, C.POINTER(_vp), C.POINTER(C.c_int), C.c_int]),
     "aslb_batch_sync": (C.c_int, [_vp]),

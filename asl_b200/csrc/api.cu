@@ -853,6 +853,81 @@ void* aslb_lbgk_device_field(aslb_lbgk* h, int field) {
   return nullptr;
 }
 
+// ---- x-slab decomposition: face buffers ------------------------------------
+//
+// A domain split into x slabs, one per GPU, exchanges after every step the
+// populations that cross its two x faces; each direction's x plane is one
+// contiguous run of `plane` elements, so a face buffer is (directions whose
+// c_x points across the face) x plane, copied with one DMA per direction.
+// After an odd step (representation B) the populations this slab's boundary
+// cells pushed into its ghost plane belong to the neighbour's boundary cells;
+// after an even step (A) this slab's ghost plane must receive the neighbour's
+// boundary-plane populations that the next odd step pulls across the face.
+//   pack   parity 0: low face  -> plane 1,      dirs c_x = -1
+//                    high face -> plane nx,     dirs c_x = +1
+//          parity 1: low face  -> plane 0,      dirs c_x = +1
+//                    high face -> plane nx + 1, dirs c_x = -1
+//   unpack parity 0: low face  -> plane 0,      dirs c_x = +1
+//                    high face -> plane nx + 1, dirs c_x = -1
+//          parity 1: low face  -> plane 1,      dirs c_x = -1
+//                    high face -> plane nx,     dirs c_x = +1
+// What one slab packs on its high face is what its high neighbour unpacks on
+// its low face at the same parity.
+namespace {
+int halo_copy(aslb_lbgk* h, int face, void* buf, bool pack) {
+  const GridDesc& g = h->d.g;
+  const int q = h->d.q;
+  const bool p0 = h->parity == 0;
+  int x, sign;
+  if (pack) {
+    x = face == 0 ? (p0 ? 1 : 0) : (p0 ? g.nx : g.nx + 1);
+    sign = face == 0 ? (p0 ? -1 : +1) : (p0 ? +1 : -1);
+  } else {
+    x = face == 0 ? (p0 ? 0 : 1) : (p0 ? g.nx + 1 : g.nx);
+    sign = face == 0 ? (p0 ? +1 : -1) : (p0 ? -1 : +1);
+  }
+  const size_t eb = storage_bytes(h->d.storage);
+  const size_t pb = (size_t)g.plane * eb;
+  char* F = (char*)h->d.F;
+  char* b = (char*)buf;
+  int k = 0;
+  for (int i = 1; i < q; ++i) {
+    if (lattice_c(q, i, 0) != sign) continue;
+    char* slab = F + ((size_t)i * g.dstride + (size_t)x * g.plane) * eb;
+    char* dst = pack ? b + k * pb : slab;
+    const char* src = pack ? slab : b + k * pb;
+    ASLB_CUDA(cudaMemcpyAsync(dst, src, pb, cudaMemcpyDeviceToDevice, h->stream));
+    ++k;
+  }
+  return ASLB_OK;
+}
+}  // namespace
+
+size_t aslb_lbgk_halo_bytes(aslb_lbgk* h) {
+  if (!h) return 0;
+  int k = 0;
+  for (int i = 1; i < h->d.q; ++i) k += lattice_c(h->d.q, i, 0) == 1;
+  return (size_t)k * (size_t)h->d.g.plane * storage_bytes(h->d.storage);
+}
+
+int aslb_lbgk_halo_pack(aslb_lbgk* h, int face, void* dev_out) {
+  ASLB_CHECK_HANDLE(h);
+  if ((face != 0 && face != 1) || !dev_out) return fail(ASLB_ERR_ARG, "aslb_lbgk_halo_pack: bad arguments");
+  if (h->flags & ASLB_PERIODIC_X)
+    return fail(ASLB_ERR_STATE, "aslb_lbgk_halo_pack: a slab's x faces are exchanged, not periodic");
+  return halo_copy(h, face, dev_out, true);
+}
+
+int aslb_lbgk_halo_unpack(aslb_lbgk* h, int face, const void* dev_in) {
+  ASLB_CHECK_HANDLE(h);
+  if ((face != 0 && face != 1) || !dev_in) return fail(ASLB_ERR_ARG, "aslb_lbgk_halo_unpack: bad arguments");
+  if (h->flags & ASLB_PERIODIC_X)
+    return fail(ASLB_ERR_STATE, "aslb_lbgk_halo_unpack: a slab's x faces are exchanged, not periodic");
+  return halo_copy(h, face, const_cast<void*>(dev_in), false);
+}
+
+int aslb_lbgk_parity(aslb_lbgk* h) { return h ? h->parity : -1; }
+
 int aslb_lbgk_moments(aslb_lbgk* h, double out[4]) {
   ASLB_CHECK_HANDLE(h);
   if (!out) return fail(ASLB_ERR_ARG, "aslb_lbgk_moments: null output");

@@ -189,6 +189,21 @@ int aslb_lbgk_read(aslb_lbgk* h, int field, int dtype, void* host_out);
 int aslb_lbgk_write(aslb_lbgk* h, int field, int dtype, const void* host_in);
 /* Device pointer of RHO or VELOCITY (ASL layout; float, double for F64). */
 void* aslb_lbgk_device_field(aslb_lbgk* h, int field);
+/* Extension (no ASL analogue): x-slab decomposition across GPUs. A domain
+ * whose x range is split into slabs (one LBGK per slab, not x-periodic, its
+ * ghost planes x = 0 and nx + 1 standing for the neighbours' boundary planes)
+ * exchanges after every step, before that step's separate conditions, one
+ * face buffer per neighbour: aslb_lbgk_halo_pack(h, face, buf) fills the
+ * buffer the neighbour across `face` (0 = low x, 1 = high x) needs now, and
+ * the neighbour passes it to aslb_lbgk_halo_unpack(h, its opposite face, buf).
+ * Buffers are DEVICE memory of aslb_lbgk_halo_bytes(h) bytes (the directions
+ * crossing the face, one x plane each); the copies are enqueued on the
+ * domain's stream. Which plane and directions move depends on the parity
+ * (aslb_lbgk_parity: 0 after an even number of steps). */
+size_t aslb_lbgk_halo_bytes(aslb_lbgk* h);
+int aslb_lbgk_halo_pack(aslb_lbgk* h, int face, void* dev_out);
+int aslb_lbgk_halo_unpack(aslb_lbgk* h, int face, const void* dev_in);
+int aslb_lbgk_parity(aslb_lbgk* h);
 /* Global FP64 moments of the post-collision populations over interior cells:
  * out[0] mass, out[1..3] momentum (a blow-up watchdog). Synchronises. */
 int aslb_lbgk_moments(aslb_lbgk* h, double out[4]);
