@@ -94,6 +94,9 @@ PROTOTYPES = {
     "aslb_batch_sync": (C.c_int, [_vp]),
     "aslb_batch_tiles": (C.c_longlong, [_vp]),
     "aslb_batch_destroy": (C.c_int, [_vp]),
+    "aslb_batch_set_shape": (C.c_int, [_vp, C.c_int]),
+    "aslb_batch_get_shape": (C.c_int, [_vp]),
+    "aslb_batch_shape_times": (C.c_int, [_vp, C.POINTER(C.c_float), C.c_int]),
     "aslb_geom_pack_spheres": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                          C.c_ulonglong, C.c_int, C.c_int, C.c_int, _pd, _pd, C.POINTER(C.c_int)]),
 }

@@ -1315,6 +1315,12 @@ struct aslb_batch {
   cudaGraphExec_t graph = nullptr;
   int graph_parity = -1;
   long long graph_version = -1;
+  // launch shape of the batched step (batch_shape_count() choices): fixed by
+  // aslb_batch_set_shape, or chosen by timing (shape_auto) before the first
+  // graph is recorded
+  int shape = 0;
+  bool shape_auto = true;
+  std::vector<float> shape_ms;
 };
 
 void batch_detach(aslb_batch* b, aslb_lbgk* h) {
@@ -1424,7 +1430,7 @@ int batch_step(aslb_batch* b) {
   prepare_params(h0);
   const int parity = h0->parity;
   cudaError_t e = launch_batch_step(b->q, b->storage, b->dev_doms, (int)b->doms.size(), b->ntiles, b->any_mask,
-                                    h0->p, parity, b->stream);
+                                    h0->p, parity, b->shape, b->stream);
   for (size_t j = 0; e == cudaSuccess && j < b->dev_pos.size(); ++j)
     if (b->pos_n[j] > 0)
       e = launch_batch_links(b->q, b->storage, b->dev_pos[j], b->pos_n[j], b->pos_links[j], parity ^ 1, b->stream);
@@ -1553,6 +1559,31 @@ int aslb_batch_run(aslb_batch* b, int nsteps, aslb_bc* const* bcs, const int* nb
       done = 1;
     }
     if (!r) r = refresh();
+    // launch-shape tuner: two real steps (one of each parity) per shape,
+    // timed on the batch's stream; the fastest is kept
+    const int nshape = batch_shape_count();
+    if (!r && b->shape_auto && b->shape_ms.empty() && nsteps - done >= 2 * nshape + 2) {
+      cudaEvent_t t0 = nullptr, t1 = nullptr;
+      ASLB_CUDA(cudaEventCreate(&t0));
+      ASLB_CUDA(cudaEventCreate(&t1));
+      int best = 0;
+      for (int v = 0; v < nshape && !r; ++v) {
+        b->shape = v;
+        cudaEventRecord(t0, b->stream);
+        r = eager(2);
+        cudaEventRecord(t1, b->stream);
+        cudaEventSynchronize(t1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t0, t1);
+        b->shape_ms.push_back(ms);
+        if (ms < b->shape_ms[best]) best = v;
+        done += 2;
+      }
+      cudaEventDestroy(t0);
+      cudaEventDestroy(t1);
+      b->shape = best;
+      batch_drop_graph(b);
+    }
     if (!r && !(b->graph && b->graph_version == batch_version(b) && b->graph_parity == h0->parity)) {
       if (b->graph && b->graph_version == batch_version(b) && done < nsteps) {
         // graph of the other parity: one eager step realigns
@@ -1612,6 +1643,27 @@ int aslb_batch_sync(aslb_batch* b) {
 }
 
 long long aslb_batch_tiles(aslb_batch* b) { return b ? b->ntiles : -1; }
+
+int aslb_batch_set_shape(aslb_batch* b, int shape) {
+  ASLB_CHECK_HANDLE(b);
+  if (shape < -1 || shape >= batch_shape_count())
+    return fail(ASLB_ERR_ARG, "aslb_batch_set_shape: shape must be -1 (tune) or 0 .. " +
+                                  std::to_string(batch_shape_count() - 1));
+  b->shape_auto = shape < 0;
+  b->shape = shape < 0 ? 0 : shape;
+  b->shape_ms.clear();
+  batch_drop_graph(b);
+  return ASLB_OK;
+}
+
+int aslb_batch_get_shape(aslb_batch* b) { return b ? b->shape : -1; }
+
+int aslb_batch_shape_times(aslb_batch* b, float* ms_out, int n) {
+  ASLB_CHECK_HANDLE(b);
+  const int k = (int)b->shape_ms.size();
+  for (int i = 0; i < k && i < n; ++i) ms_out[i] = b->shape_ms[i];
+  return k;
+}
 
 int aslb_batch_destroy(aslb_batch* b) {
   if (!b) return ASLB_OK;

@@ -92,9 +92,11 @@ struct BatchBc {
   BcParams bp;
 };
 // One stream-collide step of every domain of a batch (same lattice, storage
-// and parity; CL_NONE), a persistent grid over all domains' tiles.
+// and parity; CL_NONE), a persistent grid over all domains' tiles; `shape`
+// (0 .. batch_shape_count() - 1) picks the resident blocks per SM.
 cudaError_t launch_batch_step(int q, int storage, const BatchDom* doms, int ndom, long long ntiles, bool fused,
-                              const StepParams& p, int parity_in, cudaStream_t st);
+                              const StepParams& p, int parity_in, int shape, cudaStream_t st);
+int batch_shape_count();
 // Every link of the entries (one condition position across the batch).
 cudaError_t launch_batch_links(int q, int storage, const BatchBc* bcs, int nbc, long long nlinks, int parity,
                                cudaStream_t st);

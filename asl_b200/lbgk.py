@@ -512,6 +512,20 @@ class Batch:
     def tiles(self) -> int:
         return int(self.lib.aslb_batch_tiles(self.h))
 
+    def setShape(self, shape: int):
+        """Launch shape of the batched step (-1: chosen by timing, the default)."""
+        L.check(self.lib.aslb_batch_set_shape(self.h, int(shape)), "Batch::setShape")
+
+    @property
+    def shape(self) -> int:
+        return int(self.lib.aslb_batch_get_shape(self.h))
+
+    @property
+    def shape_times(self) -> list:
+        buf = (C.c_float * 8)()
+        n = int(self.lib.aslb_batch_shape_times(self.h, buf, 8))
+        return [float(buf[i]) for i in range(min(n, 8))]
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.aslb_batch_destroy(self.h)

@@ -335,6 +335,8 @@ def batch_run(W, n: int, steps: int, peak: float):
     bpc = BYTES_PER_CELL[("f32", 19)]
     res = {"domains": n, "cells": cells, "steps": steps, "value": cells * steps / t / 1e6, "unit": "MLUPS",
            "ms_per_step": t / steps * 1e3, "launches_per_step": launches, "tiles_per_step": batch.tiles,
+           "layout": "packed rows", "launch_shape": {"chosen": batch.shape, "blocks_per_sm": [4, 3, 2],
+                                                     "tuning_ms_per_2_steps": batch.shape_times},
            "kernel_ms": tk * 1e3, "kernel_frac_of_peak": bpc * cells / tk / 1e9 / peak,
            "separate_launches": {"value": cells * sep_steps / t_sep / 1e6, "unit": "MLUPS", "steps": sep_steps,
                                  "launches_per_step": sum(1 + sum(b.kernels for b in bc) for bc in bcs),

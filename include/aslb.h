@@ -309,6 +309,14 @@ int aslb_batch_run(aslb_batch* b, int nsteps, aslb_bc* const* bcs, const int* nb
 int aslb_batch_sync(aslb_batch* b);
 /* Tiles (x planes) of one batched step, over all domains. */
 long long aslb_batch_tiles(aslb_batch* b);
+/* Launch shape of the batched step: resident blocks of 256 threads per SM,
+ * shape 0: 4, 1: 3, 2: 2. By default (or after shape -1) the first
+ * aslb_batch_run that records a graph first times two real steps with every
+ * shape and keeps the fastest (all shapes give identical results);
+ * aslb_batch_shape_times returns those timings (ms, up to n; the count). */
+int aslb_batch_set_shape(aslb_batch* b, int shape);
+int aslb_batch_get_shape(aslb_batch* b);
+int aslb_batch_shape_times(aslb_batch* b, float* ms_out, int n);
 int aslb_batch_destroy(aslb_batch* b);
 
 /* ---- workload geometry (host) ----------------------------------------- */

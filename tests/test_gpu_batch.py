@@ -76,3 +76,25 @@ def test_batch_rejects_mismatched_domains(gpu):
     lbs[1].close()
     with pytest.raises(A.L.ASLError):
         batch.run(2, bcs)
+
+
+def test_batch_launch_shapes_identical_and_tuned(gpu):
+    ws = small_batch(3, seed=17)
+    out = []
+    for shape in (0, 1, 2):
+        batch, lbs, bcs = W.build_batch(ws)
+        batch.setShape(shape)
+        batch.run(6, bcs)
+        batch.sync()
+        assert batch.shape == shape and batch.shape_times == []
+        out.append([lb.getF() for lb in lbs])
+    for other in out[1:]:
+        for a, b in zip(out[0], other):
+            assert np.array_equal(a, b, equal_nan=True)
+    batch, lbs, bcs = W.build_batch(ws)
+    batch.run(12, bcs)  # long enough for the tuner: 2 steps per shape first
+    batch.sync()
+    t = batch.shape_times
+    assert len(t) == 3 and batch.shape == int(np.argmin(t))
+    for lb in lbs:
+        assert lb.steps == 12
