@@ -165,7 +165,11 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, CL, FUSED>::blocks)
 // D3Q15/D3Q19 domains with fused links, at three blocks (80 registers) per
 // SM; without fused links the schedule hoists every address of both cells
 // (over 128 registers) and the one-cell kernel is faster.
-// M32: the links come from the one-word mask (p.mask32).
+// M32: the links come from the one-word mask (p.mask32). A block walks
+// kPairPlanes consecutive x planes; each thread loads the fused-link words of
+// the next plane one iteration ahead, so that the population loads, whose
+// addresses those words select, do not wait for a second memory round trip.
+constexpr int kPairPlanes = 4;
 template <int Q, class S, bool ODD, bool FUSED, bool M32>
 __global__ void __launch_bounds__(256, 3)
     k_stream_collide_pair(S* __restrict__ F, const GridDesc g, const StepParams p,
@@ -175,32 +179,55 @@ __global__ void __launch_bounds__(256, 3)
   const int za = blockIdx.x * (2 * blockDim.x) + 64 * w + lane + 1;
   const int zb = za + 32;
   const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int x = blockIdx.z + 1;
+  const int x0 = blockIdx.z * kPairPlanes + 1;
+  const int x1 = min(g.nx, x0 + kPairPlanes - 1);
   if (za > g.nz || y > g.ny) return;
   const bool has_b = zb <= g.nz;
   const unsigned ds = (unsigned)g.dstride;
-  const unsigned sa = (unsigned)sidx(g, x, y, za);
-  const unsigned sb = sa + 32u;
-  uint2 ma = make_uint2(0u, 0u), mb = make_uint2(0u, 0u);
-  if (FUSED && M32) {
-    const uint32_t wa = p.mask32[sa], wb = has_b ? p.mask32[sb] : 0u;
-    ma = (wa >> 31) ? make_uint2(0u, wa & 0x7fffffffu) : make_uint2(wa, 0u);
-    mb = (wb >> 31) ? make_uint2(0u, wb & 0x7fffffffu) : make_uint2(wb, 0u);
-  } else if (FUSED) {
-    ma = p.mask[sa];
-    if (has_b) mb = p.mask[sb];
-  }
-  int ox[3], oy[3], oza[3], ozb[3];
-  nb_offsets(g, x, y, za, ox, oy, oza);
-  ozb[0] = -1;  // zb >= 33: the lower neighbour never wraps
-  ozb[1] = 0;
-  ozb[2] = ((g.periodic & 4) && zb == g.nz) ? -(g.nz - 1) : 1;
-  C fa[Q], fb[Q];
-  cell_load<Q, S, ODD, FUSED>(F, ds, sa, ox, oy, oza, ma.x, fa);
-  if (has_b) cell_load<Q, S, ODD, FUSED>(F, ds, sb, ox, oy, ozb, mb.x, fb);
+  const unsigned pl = (unsigned)g.plane;
+  const unsigned s0 = (unsigned)sidx(g, x0, y, za);
   const C om0 = step_omega<C>(p);
-  cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, za, sa, ox, oy, oza, ma.y, fa, om0);
-  if (has_b) cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, zb, sb, ox, oy, ozb, mb.y, fb, om0);
+  // the fused-link words of the next plane are loaded one plane ahead, so the
+  // population loads (whose addresses they select) never wait for them
+  uint2 wa = make_uint2(0u, 0u), wb = make_uint2(0u, 0u);
+  if (FUSED && M32) {
+    wa.x = p.mask32[s0];
+    if (has_b) wb.x = p.mask32[s0 + 32u];
+  } else if (FUSED) {
+    wa = p.mask[s0];
+    if (has_b) wb = p.mask[s0 + 32u];
+  }
+  for (int x = x0; x <= x1; ++x) {
+    const unsigned sa = s0 + (unsigned)(x - x0) * pl;
+    const unsigned sb = sa + 32u;
+    uint2 na = make_uint2(0u, 0u), nb = make_uint2(0u, 0u);
+    if (FUSED && x < x1) {
+      if (M32) {
+        na.x = p.mask32[sa + pl];
+        if (has_b) nb.x = p.mask32[sb + pl];
+      } else {
+        na = p.mask[sa + pl];
+        if (has_b) nb = p.mask[sb + pl];
+      }
+    }
+    uint2 ma = wa, mb = wb;
+    if (FUSED && M32) {
+      ma = (wa.x >> 31) ? make_uint2(0u, wa.x & 0x7fffffffu) : make_uint2(wa.x, 0u);
+      mb = (wb.x >> 31) ? make_uint2(0u, wb.x & 0x7fffffffu) : make_uint2(wb.x, 0u);
+    }
+    int ox[3], oy[3], oza[3], ozb[3];
+    nb_offsets(g, x, y, za, ox, oy, oza);
+    ozb[0] = -1;  // zb >= 33: the lower neighbour never wraps
+    ozb[1] = 0;
+    ozb[2] = ((g.periodic & 4) && zb == g.nz) ? -(g.nz - 1) : 1;
+    C fa[Q], fb[Q];
+    cell_load<Q, S, ODD, FUSED>(F, ds, sa, ox, oy, oza, ma.x, fa);
+    if (has_b) cell_load<Q, S, ODD, FUSED>(F, ds, sb, ox, oy, ozb, mb.x, fb);
+    cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, za, sa, ox, oy, oza, ma.y, fa, om0);
+    if (has_b) cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, zb, sb, ox, oy, ozb, mb.y, fb, om0);
+    wa = na;
+    wb = nb;
+  }
 }
 
 inline void step_launch_shape(const GridDesc& g, dim3& grid, dim3& block) {
@@ -221,7 +248,7 @@ inline void pair_launch_shape(const GridDesc& g, dim3& grid, dim3& block) {
   if (tz > 128) tz = 128;
   int ty = 256 / tz;
   block = dim3(tz, ty, 1);
-  grid = dim3((g.nz + 2 * tz - 1) / (2 * tz), (g.ny + ty - 1) / ty, g.nx);
+  grid = dim3((g.nz + 2 * tz - 1) / (2 * tz), (g.ny + ty - 1) / ty, (g.nx + kPairPlanes - 1) / kPairPlanes);
 }
 
 template <int Q, class S, int CL>
