@@ -132,7 +132,11 @@ __device__ __forceinline__ void cell_finish(S* __restrict__ F, const GridDesc& g
 // (reads F[i][x - c_i], writes F[inv i][x + c_i]); EVEN: B -> A (reads
 // F[inv i][x], writes F[i][x]). Element indices are 32-bit (Q * dstride < 2^32).
 // FUSED: the domain has fused no-slip links (p.mask is read); chosen on the
-// host so domains without them run the unmasked code.
+// host so domains without them run the unmasked code. A block walks
+// kOnePlanes consecutive x planes; with fused links each thread loads the
+// next plane's link words one iteration ahead (the population addresses
+// depend on them, so they must not cost a second memory round trip).
+constexpr int kOnePlanes = 4;
 template <int Q, class S, int CL, bool ODD, bool FUSED>
 __global__ void __launch_bounds__(256, StepOccupancy<Q, S, CL, FUSED>::blocks)
     k_stream_collide(S* __restrict__ F, const GridDesc g, const StepParams p,
@@ -140,36 +144,41 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, CL, FUSED>::blocks)
   using C = typename Store<S>::C;
   const int z = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int x = blockIdx.z + 1;
+  const int x0 = blockIdx.z * kOnePlanes + 1;
+  const int x1 = min(g.nx, x0 + kOnePlanes - 1);
   if (z > g.nz || y > g.ny) return;
-  const unsigned s = (unsigned)sidx(g, x, y, z);
-  // Fused no-slip links: a fluid cell reads bounce-back populations, a solid
-  // cell skips the writes the condition would overwrite.
-  uint32_t bounce = 0, elide = 0;
-  if (FUSED) {
-    const uint2 m = p.mask[s];
-    bounce = m.x;
-    elide = m.y;
+  const unsigned pl = (unsigned)g.plane;
+  const unsigned s0 = (unsigned)sidx(g, x0, y, z);
+  // fused no-slip links: a fluid cell reads bounce-back populations, a solid
+  // cell skips the writes the condition would overwrite
+  uint2 m = make_uint2(0u, 0u);
+  if (FUSED) m = p.mask[s0];
+  for (int x = x0; x <= x1; ++x) {
+    const unsigned s = s0 + (unsigned)(x - x0) * pl;
+    uint2 mn = make_uint2(0u, 0u);
+    if (FUSED && x < x1) mn = p.mask[s + pl];
+    int ox[3], oy[3], oz[3];
+    nb_offsets(g, x, y, z, ox, oy, oz);
+    C f[Q];
+    cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, s, ox, oy, oz, m.x, f);
+    cell_finish<Q, S, CL, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, z, s, ox, oy, oz, m.y, f, step_omega<C>(p));
+    m = mn;
   }
-  int ox[3], oy[3], oz[3];
-  nb_offsets(g, x, y, z, ox, oy, oz);
-  C f[Q];
-  cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, s, ox, oy, oz, bounce, f);
-  cell_finish<Q, S, CL, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, z, s, ox, oy, oz, elide, f, step_omega<C>(p));
 }
 
 // Two cells per thread, z and z + 32 of the same row: a warp covers 64
 // consecutive cells, and each thread has the loads of both cells in flight
 // before it collides the first, which doubles the bytes in flight per
-// register-limited warp. Used for the plain (no closure) FP32/FP16 step of
+// register-limited warp. Used for the plain (no closure) FP32 step of
 // D3Q15/D3Q19 domains with fused links, at three blocks (80 registers) per
 // SM; without fused links the schedule hoists every address of both cells
-// (over 128 registers) and the one-cell kernel is faster.
+// (over 128 registers), and with FP16 storage (fewer bytes, more
+// instructions) the one-cell kernel is faster.
 // M32: the links come from the one-word mask (p.mask32). A block walks
 // kPairPlanes consecutive x planes; each thread loads the fused-link words of
 // the next plane one iteration ahead, so that the population loads, whose
 // addresses those words select, do not wait for a second memory round trip.
-constexpr int kPairPlanes = 4;
+constexpr int kPairPlanes = 2;
 template <int Q, class S, bool ODD, bool FUSED, bool M32>
 __global__ void __launch_bounds__(256, 3)
     k_stream_collide_pair(S* __restrict__ F, const GridDesc g, const StepParams p,
@@ -238,6 +247,12 @@ inline void step_launch_shape(const GridDesc& g, dim3& grid, dim3& block) {
   grid = dim3((g.nz + tz - 1) / tz, (g.ny + ty - 1) / ty, g.nx);
 }
 
+// The one-cell stream-collide: the same blocks, kOnePlanes x planes each.
+inline void plane_launch_shape(const GridDesc& g, dim3& grid, dim3& block) {
+  step_launch_shape(g, grid, block);
+  grid.z = (g.nx + kOnePlanes - 1) / kOnePlanes;
+}
+
 // Launch of the TMA-staged variant (stream_collide_tma.cuh).
 template <int Q, class S, int CL>
 cudaError_t step_tma(const DomainDev& d, const StepParams& p, int parity_in, cudaStream_t st);
@@ -257,7 +272,7 @@ cudaError_t step_q_s_cl(const DomainDev& d, const StepParams& p, int parity_in, 
   dim3 grid, block;
   using M = typename MacroT<S>::T;
   const bool fused = p.mask != nullptr;
-  if constexpr (CL == CL_NONE && Q != 27 && !std::is_same<S, double>::value) {
+  if constexpr (CL == CL_NONE && Q != 27 && std::is_same<S, float>::value) {
     if (d.variant == 0 && fused) {
       pair_launch_shape(d.g, grid, block);
       const bool m32 = p.mask32 != nullptr;
@@ -271,7 +286,7 @@ cudaError_t step_q_s_cl(const DomainDev& d, const StepParams& p, int parity_in, 
       return cudaGetLastError();
     }
   }
-  step_launch_shape(d.g, grid, block);
+  plane_launch_shape(d.g, grid, block);
   if (parity_in == 0) {
     if (fused)
       k_stream_collide<Q, S, CL, true, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
