@@ -30,6 +30,25 @@ struct MlpNet {
 };
 
 // Features of a cell. p_ab = Pi_neq_ab / rho (standard normalisation).
+// Cube root and logarithm of the features. The features are the network's
+// inputs (the same function feeds training and inference), so in FP32 they
+// use the hardware's fast base-2 exponential and logarithm (__expf, __logf):
+// cbrt(v) = sign(v) 2^(log2|v| / 3).
+template <class C>
+__host__ __device__ inline C feat_cbrt(C v) {
+#ifdef __CUDA_ARCH__
+  if constexpr (sizeof(C) == 4) return copysignf(__expf(__logf(fabsf(v)) * (1.0f / 3.0f)), v);
+#endif
+  return cbrt(v);
+}
+template <class C>
+__host__ __device__ inline C feat_log(C v) {
+#ifdef __CUDA_ARCH__
+  if constexpr (sizeof(C) == 4) return __logf(v);
+#endif
+  return log(v);
+}
+
 template <class C>
 __host__ __device__ inline void mlp_features(C rho, C ux, C uy, C uz, C P00, C P11, C P22, C P01, C P12, C P02,
                                              float (&x)[kMlpIn]) {
@@ -48,9 +67,9 @@ __host__ __device__ inline void mlp_features(C rho, C ux, C uy, C uz, C P00, C P
   x[0] = float(tr);
   x[1] = float(sqrt(n2));
   x[2] = float(sqrt(dn2));
-  x[3] = float(cbrt(C(3) * ddet));      // tr(A^3) = 3 det(A) for traceless A
-  x[4] = float(cbrt(det));
-  x[5] = float(log(sqrt(dn2) + eps));
+  x[3] = float(feat_cbrt(C(3) * ddet));  // tr(A^3) = 3 det(A) for traceless A
+  x[4] = float(feat_cbrt(det));
+  x[5] = float(feat_log(sqrt(dn2) + eps));
   x[6] = float(sqrt(a * a + b * b + c * c));
   x[7] = float(sqrt(C(2) * off2));
   x[8] = float(sqrt(ux * ux + uy * uy + uz * uz));
