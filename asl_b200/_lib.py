@@ -64,6 +64,9 @@ PROTOTYPES = {
     "aslb_lbgk_steps": (C.c_longlong, [_vp]),
     "aslb_lbgk_read": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "aslb_lbgk_write": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
+    "aslb_lbgk_state_bytes": (C.c_size_t, [_vp]),
+    "aslb_lbgk_save_state": (C.c_int, [_vp, _vp, C.c_size_t, _vp]),
+    "aslb_lbgk_load_state": (C.c_int, [_vp, _vp, C.c_size_t, _vp]),
     "aslb_lbgk_device_field": (_vp, [_vp, C.c_int]),
     "aslb_lbgk_moments": (C.c_int, [_vp, _pd]),
     "aslb_bc_slice_create": (C.c_int, [_vp, C.c_int, C.c_uint, C.c_double, _pd, C.POINTER(_vp)]),

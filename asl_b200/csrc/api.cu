@@ -846,6 +846,43 @@ int aslb_lbgk_write(aslb_lbgk* h, int field, int dtype, const void* host_in) {
   return ASLB_OK;
 }
 
+// ---- restart dump: the population array as stored ---------------------------
+size_t aslb_lbgk_state_bytes(aslb_lbgk* h) {
+  return h ? (size_t)h->d.q * h->d.g.dstride * storage_bytes(h->d.storage) : 0;
+}
+
+int aslb_lbgk_save_state(aslb_lbgk* h, void* host_out, size_t bytes, long long meta[4]) {
+  ASLB_CHECK_HANDLE(h);
+  if (!host_out || !meta || bytes != aslb_lbgk_state_bytes(h))
+    return fail(ASLB_ERR_ARG, "aslb_lbgk_save_state: the buffer must hold aslb_lbgk_state_bytes() bytes");
+  cudaError_t e = cudaMemcpyAsync(host_out, h->d.F, bytes, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_save_state: ") + cudaGetErrorString(e));
+  meta[0] = h->steps;
+  meta[1] = h->parity;
+  meta[2] = h->fresh ? 0 : 1;
+  meta[3] = h->d.storage;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_load_state(aslb_lbgk* h, const void* host_in, size_t bytes, const long long meta[4]) {
+  ASLB_CHECK_HANDLE(h);
+  if (!host_in || !meta || bytes != aslb_lbgk_state_bytes(h))
+    return fail(ASLB_ERR_ARG, "aslb_lbgk_load_state: the dump is of another domain size or lattice");
+  if (meta[3] != h->d.storage || (meta[1] != 0 && meta[1] != 1) || meta[0] < 0)
+    return fail(ASLB_ERR_ARG, "aslb_lbgk_load_state: the dump is of another storage or is damaged");
+  cudaError_t e = cudaMemcpyAsync(h->d.F, host_in, bytes, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_load_state: ") + cudaGetErrorString(e));
+  h->steps = meta[0];
+  h->parity = (int)meta[1];
+  h->fresh = meta[2] == 0;
+  h->mlp_last = -1;
+  h->macro_once = true;
+  h->version++;
+  return ASLB_OK;
+}
+
 void* aslb_lbgk_device_field(aslb_lbgk* h, int field) {
   if (!h) return nullptr;
   if (field == ASLB_FIELD_RHO) return h->d.rho;

@@ -256,6 +256,21 @@ class LBGK:
             raise L.ASLError("ASL ERROR: setF: wrong shape")
         L.check(self.lib.aslb_lbgk_write(self.h, L.FIELD_F, L.F64, f.ctypes.data_as(C.c_void_p)), "LBGK::setF")
 
+    def saveState(self):
+        """Restart dump: (population array bytes as stored, meta = [steps,
+        parity, fused links active, storage])."""
+        n = int(self.lib.aslb_lbgk_state_bytes(self.h))
+        buf = np.empty(n, dtype=np.uint8)
+        meta = (C.c_longlong * 4)()
+        L.check(self.lib.aslb_lbgk_save_state(self.h, buf.ctypes.data_as(C.c_void_p), n, meta), "LBGK::saveState")
+        return buf, np.array(meta[:], dtype=np.int64)
+
+    def loadState(self, data: np.ndarray, meta):
+        data = np.ascontiguousarray(data, dtype=np.uint8)
+        m = (C.c_longlong * 4)(*[int(v) for v in meta])
+        L.check(self.lib.aslb_lbgk_load_state(self.h, data.ctypes.data_as(C.c_void_p), data.nbytes, m),
+                "LBGK::loadState")
+
     def moments(self) -> np.ndarray:
         out = (C.c_double * 4)()
         L.check(self.lib.aslb_lbgk_moments(self.h, out), "LBGK::moments")

@@ -187,6 +187,17 @@ long long aslb_lbgk_steps(aslb_lbgk* h);
 int aslb_lbgk_read(aslb_lbgk* h, int field, int dtype, void* host_out);
 /* Load populations (field F only), ASL layout; used for restart. */
 int aslb_lbgk_write(aslb_lbgk* h, int field, int dtype, const void* host_in);
+/* Restart dump (the role of ASL's ABD dumps, src/writers/aslABDFormat.h:45-137;
+ * ASL itself keeps the population pools protected): the population array
+ * exactly as stored (storage format, current AA representation, padding),
+ * aslb_lbgk_state_bytes(h) bytes, plus meta = {steps, parity, fused-links
+ * active, storage}. Loading it into a domain of the same size, lattice,
+ * storage and conditions continues bit for bit where the dumped domain
+ * stood. A learned-closure domain recomputes its Cs^2 field at the first
+ * step after a load. */
+size_t aslb_lbgk_state_bytes(aslb_lbgk* h);
+int aslb_lbgk_save_state(aslb_lbgk* h, void* host_out, size_t bytes, long long meta[4]);
+int aslb_lbgk_load_state(aslb_lbgk* h, const void* host_in, size_t bytes, const long long meta[4]);
 /* Device pointer of RHO or VELOCITY (ASL layout; float, double for F64). */
 void* aslb_lbgk_device_field(aslb_lbgk* h, int field);
 /* Extension (no ASL analogue): x-slab decomposition across GPUs. A domain
