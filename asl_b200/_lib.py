@@ -64,6 +64,9 @@ PROTOTYPES = {
     "aslb_lbgk_steps": (C.c_longlong, [_vp]),
     "aslb_lbgk_read": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "aslb_lbgk_write": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
+    "aslb_read_stl": (C.c_int, [C.c_char_p, _vp, C.c_longlong, _vp]),
+    "aslb_surface_map": (C.c_int, [_vp, C.c_longlong, C.c_int, C.c_int, C.c_int, _pd, C.c_double, C.c_double,
+                                   C.c_int, C.c_double, C.c_double, _vp]),
     "aslb_lbgk_state_bytes": (C.c_size_t, [_vp]),
     "aslb_lbgk_save_state": (C.c_int, [_vp, _vp, C.c_size_t, _vp]),
     "aslb_lbgk_load_state": (C.c_int, [_vp, _vp, C.c_size_t, _vp]),

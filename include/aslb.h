@@ -342,6 +342,25 @@ int aslb_geom_pack_spheres(int nx, int ny, int nz, double rmin, double rmax, dou
                            unsigned long long seed, int periodic_x, int attempts, int max_spheres, double* centers,
                            double* radii, int* count);
 
+/* ---- surfaces (readSurface) -------------------------------------------- */
+
+/* Triangles of an STL file, binary or ASCII (the STL branch of ASL's
+ * readSurface, src/readers/aslVTKFormatReaders.cxx:266-345, which reads it with
+ * vtkSTLReader): *ntri triangles of 9 floats (x0 y0 z0 x1 ... z2, file
+ * coordinates) into tri when tri is not NULL and cap >= *ntri. */
+int aslb_read_stl(const char* path, float* tri, long long cap, long long* ntri);
+/* Distance map of a triangle surface on a gx x gy x gz grid whose cell
+ * (i, j, k) sits at pos0 + (i, j, k) dx (x slowest, z fastest): d = distance
+ * to the nearest triangle, exact within `band` of the surface, `band` beyond;
+ * with solid_interior, cells inside the closed surface take -d. Writes
+ * map = (d - offset) / scale (FP32, gx*gy*gz). ASL's surfaceToData
+ * (src/readers/aslVTKFormatReaders.cxx:136-210, VTK's implicit modeller)
+ * samples the unsigned distance and maps it with offset 1.2 dx, scale 1.8 dx
+ * (block overload) or 1.8 dx, 1.8 dx (spacing overloads): solid_interior = 0.
+ * Runs on the current device. */
+int aslb_surface_map(const float* tri, long long ntri, int gx, int gy, int gz, const double pos0[3], double dx,
+                     double band, int solid_interior, double offset, double scale, float* map_host);
+
 #ifdef __cplusplus
 }
 #endif
