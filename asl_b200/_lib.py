@@ -19,6 +19,7 @@ PACKED_ROWS = 64
 CLOSURE_NONE, CLOSURE_ASL_INTENT, CLOSURE_SMAGORINSKY, CLOSURE_MLP = 0, 1, 2, 3
 BC_NOSLIP, BC_VELOCITY, BC_PRESSURE, BC_PRESSURE_VELOCITY = 0, 1, 2, 3
 BC_MAP_NOSLIP, BC_MAP_VELOCITY, BC_MAP_VELOCITY_ROTATION, BC_MAP_PRESSURE_VELOCITY = 10, 11, 12, 13
+BC_MAP_TRANSPORT_DEPOSITION, BC_MAP_KINETICS_DEPOSITION = 14, 15
 FIELD_RHO, FIELD_VELOCITY, FIELD_F, FIELD_CS2 = 0, 1, 2, 3
 
 
@@ -64,6 +65,10 @@ PROTOTYPES = {
     "aslb_lbgk_steps": (C.c_longlong, [_vp]),
     "aslb_lbgk_read": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "aslb_lbgk_write": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
+    "aslb_bc_deposition_create": (C.c_int, [_vp, C.c_int, _vp, C.c_double, C.c_double, C.c_double, _vp]),
+    "aslb_flux_create": (C.c_int, [_vp, _vp, _vp]),
+    "aslb_flux_compute": (C.c_int, [_vp, _vp, _vp]),
+    "aslb_flux_destroy": (C.c_int, [_vp]),
     "aslb_read_stl": (C.c_int, [C.c_char_p, _vp, C.c_longlong, _vp]),
     "aslb_surface_map": (C.c_int, [_vp, C.c_longlong, C.c_int, C.c_int, C.c_int, _pd, C.c_double, C.c_double,
                                    C.c_int, C.c_double, C.c_double, _vp]),

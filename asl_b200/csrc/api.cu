@@ -94,6 +94,7 @@ struct aslb_bc {
 
 struct aslb_force {
   aslb_lbgk* h = nullptr;
+  bool flux = false;  // ComputeSurfaceFlux object (one value per cell)
   int4* cells = nullptr;
   uint32_t* mask_in = nullptr;
   int n = 0;
@@ -1038,18 +1039,12 @@ int aslb_bc_slice_create(aslb_lbgk* h, int kind, unsigned wallmask, double p, co
   return ASLB_OK;
 }
 
-int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const double u[3], const double omega[3],
-                       const double center[3], aslb_bc** out) {
-  ASLB_CHECK_HANDLE(h);
-  if (!out || !map) return fail(ASLB_ERR_ARG, "aslb_bc_map_create: null argument");
-  *out = nullptr;
-  if (kind < ASLB_BC_MAP_NOSLIP || kind > ASLB_BC_MAP_PRESSURE_VELOCITY)
-    return fail(ASLB_ERR_ARG, "aslb_bc_map_create: unknown map kind");
+namespace {
+// Cell x is processed iff -0.9999 < map(x) <= 0; link k iff map(x + c_k) > 0
+// (src/num/aslLBGKBC.cxx:235-251), counted when x + c_k is an interior cell.
+void map_candidates(const aslb_lbgk* h, const float* map, std::vector<Cand>& cand) {
   const GridDesc& g = h->d.g;
   const int q = h->d.q;
-  std::vector<Cand> cand;
-  // Cell x is processed iff -0.9999 < map(x) <= 0; link k iff map(x + c_k) > 0
-  // (src/num/aslLBGKBC.cxx:235-251), counted when x + c_k is an interior cell.
   for (int x = 0; x < g.gx; ++x)
     for (int y = 0; y < g.gy; ++y)
       for (int z = 0; z < g.gz; ++z) {
@@ -1063,6 +1058,52 @@ int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const
           if (map_at(g, map, qx, qy, qz) > 0.f) cand.push_back({x, y, z, k});
         }
       }
+}
+}  // namespace
+
+int aslb_bc_deposition_create(aslb_lbgk* h, int kind, const float* map, double p0, double limiting_factor,
+                              double beta, aslb_bc** out) {
+  ASLB_CHECK_HANDLE(h);
+  if (!out || !map) return fail(ASLB_ERR_ARG, "aslb_bc_deposition_create: null argument");
+  *out = nullptr;
+  if (kind != ASLB_BC_MAP_TRANSPORT_DEPOSITION && kind != ASLB_BC_MAP_KINETICS_DEPOSITION)
+    return fail(ASLB_ERR_ARG, "aslb_bc_deposition_create: unknown deposition kind");
+  std::vector<Cand> cand;
+  map_candidates(h, map, cand);
+  if (cand.size() >= (size_t)(1u << 31))
+    return fail(ASLB_ERR_ARG, "aslb_bc_deposition_create: too many boundary links");
+  auto* bc = new aslb_bc();
+  bc->h = h;
+  bc->bp.kind = kind;
+  bc->bp.compressible = h->p.compressible;
+  bc->bp.p = p0;
+  bc->bp.lf = limiting_factor;
+  bc->bp.beta = beta;
+  bc->bp.dx = h->dx;
+  for (int d = 0; d < 3; ++d) bc->bp.pos0[d] = h->pos0[d];
+  bc->bp.scale = h->p.scale;
+  bc->bp.inv_scale = h->p.inv_scale;
+  fill_link_values(h, bc);
+  // every link of an anchor together: the value depends on all of them
+  int r = finalize_links(h, bc, cand, true);
+  if (r) {
+    aslb_bc_destroy(bc);
+    return r;
+  }
+  h->bcs.push_back(bc);
+  *out = bc;
+  return ASLB_OK;
+}
+
+int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const double u[3], const double omega[3],
+                       const double center[3], aslb_bc** out) {
+  ASLB_CHECK_HANDLE(h);
+  if (!out || !map) return fail(ASLB_ERR_ARG, "aslb_bc_map_create: null argument");
+  *out = nullptr;
+  if (kind < ASLB_BC_MAP_NOSLIP || kind > ASLB_BC_MAP_PRESSURE_VELOCITY)
+    return fail(ASLB_ERR_ARG, "aslb_bc_map_create: unknown map kind");
+  std::vector<Cand> cand;
+  map_candidates(h, map, cand);
   if (cand.size() >= (size_t)(1u << 31)) return fail(ASLB_ERR_ARG, "aslb_bc_map_create: too many boundary links");
   auto* bc = new aslb_bc();
   bc->h = h;
@@ -1180,17 +1221,13 @@ int aslb_bc_kernels(aslb_bc* bc) { return !bc || bc->fused ? 0 : (bc->nd > 0) + 
 
 // ---- surface force ---------------------------------------------------------
 
-int aslb_force_create(aslb_lbgk* h, const float* map, aslb_force** out) {
-  ASLB_CHECK_HANDLE(h);
-  if (!out || !map) return fail(ASLB_ERR_ARG, "aslb_force_create: null argument");
-  *out = nullptr;
+namespace {
+// Cells with |map| < 0.9999 (src/num/aslLBGKBC.cxx:730-733, 659-661); mask0
+// links from a solid cell to a fluid interior neighbour, mask_in links from a
+// fluid interior cell to a solid neighbour (src/num/aslLBGKBC.cxx:713-726, 643-656).
+void surface_cells(const aslb_lbgk* h, const float* map, std::vector<int4>& cells, std::vector<uint32_t>& mask_in) {
   const GridDesc& g = h->d.g;
   const int q = h->d.q;
-  std::vector<int4> cells;
-  std::vector<uint32_t> mask_in;
-  // Cells with |map| < 0.9999 (src/num/aslLBGKBC.cxx:730-733); mask0 links from
-  // a solid cell to a fluid interior neighbour, mask_in links from a fluid
-  // interior cell to a solid neighbour (src/num/aslLBGKBC.cxx:713-726).
   for (int x = 0; x < g.gx; ++x)
     for (int y = 0; y < g.gy; ++y)
       for (int z = 0; z < g.gz; ++z) {
@@ -1211,8 +1248,22 @@ int aslb_force_create(aslb_lbgk* h, const float* map, aslb_force** out) {
           mask_in.push_back(ki);
         }
       }
+}
+
+// A force (3 values per cell) or flux (1 value per cell) object on the
+// surface of map.
+int surface_object(aslb_lbgk* h, const float* map, bool flux, aslb_force** out, const char* what) {
+  ASLB_CHECK_HANDLE(h);
+  if (!out || !map) return fail(ASLB_ERR_ARG, std::string(what) + ": null argument");
+  *out = nullptr;
+  const GridDesc& g = h->d.g;
+  std::vector<int4> cells;
+  std::vector<uint32_t> mask_in;
+  surface_cells(h, map, cells, mask_in);
+  const int width = flux ? 1 : 6, comps = flux ? 1 : 3;
   auto* fc = new aslb_force();
   fc->h = h;
+  fc->flux = flux;
   fc->n = (int)cells.size();
   int r = upload(&fc->cells, cells);
   if (!r) r = upload(&fc->mask_in, mask_in);
@@ -1220,23 +1271,51 @@ int aslb_force_create(aslb_lbgk* h, const float* map, aslb_force** out) {
     aslb_force_destroy(fc);
     return r;
   }
-  cudaError_t e = cudaMalloc((void**)&fc->field, 3 * (size_t)g.L * sizeof(float));
-  if (e == cudaSuccess) e = cudaMemsetAsync(fc->field, 0, 3 * (size_t)g.L * sizeof(float), h->stream);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&fc->partials, (size_t)force_blocks(fc->n) * 6 * sizeof(double));
+  cudaError_t e = cudaMalloc((void**)&fc->field, comps * (size_t)g.L * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemsetAsync(fc->field, 0, comps * (size_t)g.L * sizeof(float), h->stream);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&fc->partials, (size_t)force_blocks(fc->n) * width * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc((void**)&fc->out, 6 * sizeof(double));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&fc->host_out, 6 * sizeof(double));
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
     aslb_force_destroy(fc);
-    return fail(ASLB_ERR_CUDA, std::string("aslb_force_create: ") + cudaGetErrorString(e));
+    return fail(ASLB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
   }
   h->forces.push_back(fc);
   *out = fc;
   return ASLB_OK;
 }
+}  // namespace
+
+int aslb_force_create(aslb_lbgk* h, const float* map, aslb_force** out) {
+  return surface_object(h, map, false, out, "aslb_force_create");
+}
+
+int aslb_flux_create(aslb_lbgk* h, const float* map, aslb_flux** out) {
+  return surface_object(h, map, true, out, "aslb_flux_create");
+}
+
+int aslb_flux_compute(aslb_flux* fc, float* field_host, double* total) {
+  if (!fc) return fail(ASLB_ERR_ARG, "aslb_flux_compute: null argument");
+  if (!fc->flux) return fail(ASLB_ERR_ARG, "aslb_flux_compute: a force object, not a flux object");
+  if (!fc->h) return fail(ASLB_ERR_STATE, "aslb_flux_compute: its domain was destroyed");
+  aslb_lbgk* h = fc->h;
+  cudaError_t e = launch_flux(h->d, fc->cells, fc->mask_in, fc->n, fc->field, h->p.inv_scale,
+                              h->fresh ? nullptr : h->mask_dev, h->parity, fc->partials, fc->out, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(fc->host_out, fc->out, sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess && field_host)
+    e = cudaMemcpyAsync(field_host, fc->field, (size_t)h->d.g.L * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_flux_compute: ") + cudaGetErrorString(e));
+  if (total) *total = fc->host_out[0];
+  return ASLB_OK;
+}
+
+int aslb_flux_destroy(aslb_flux* fc) { return aslb_force_destroy(fc); }
 
 int aslb_force_compute(aslb_force* fc, const double r0[3], float* field_host, double out6[6]) {
   if (!fc || !out6) return fail(ASLB_ERR_ARG, "aslb_force_compute: null argument");
+  if (fc->flux) return fail(ASLB_ERR_ARG, "aslb_force_compute: a flux object, not a force object");
   if (!fc->h) return fail(ASLB_ERR_STATE, "aslb_force_compute: its domain was destroyed");
   aslb_lbgk* h = fc->h;
   const double zero[3] = {0, 0, 0};
@@ -1298,6 +1377,7 @@ double* g_force_scratch_dev[64] = {nullptr};
 
 extern "C" int aslb_force_compute_noalloc(aslb_force* fc, const double r0[3], double out6[6]) {
   if (!fc || !out6) return fail(ASLB_ERR_ARG, "aslb_force_compute_noalloc: null argument");
+  if (fc->flux) return fail(ASLB_ERR_ARG, "aslb_force_compute_noalloc: a flux object, not a force object");
   if (!fc->h) return fail(ASLB_ERR_STATE, "aslb_force_compute_noalloc: its domain was destroyed");
   aslb_lbgk* h = fc->h;
   if (force_blocks(fc->n) > kNoAllocForceBlocks)

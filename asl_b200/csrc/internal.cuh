@@ -154,6 +154,8 @@ enum BcKind {
   BCK_MAP_VELOCITY = 11,
   BCK_MAP_VELOCITY_ROTATION = 12,
   BCK_MAP_PRESSURE_VELOCITY = 13,
+  BCK_MAP_TRANSPORT_DEPOSITION = 14,
+  BCK_MAP_KINETICS_DEPOSITION = 15,
 };
 
 struct BcParams {
@@ -165,6 +167,7 @@ struct BcParams {
   double cen[3];
   double pos0[3];
   double dx;
+  double lf, beta;  // deposition: limiting factor, kinetic coefficient
   float scale, inv_scale;
 };
 

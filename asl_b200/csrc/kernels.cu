@@ -236,6 +236,26 @@ __global__ void __launch_bounds__(256) k_bc(S* __restrict__ F, const GridDesc g,
       vel[2] = C(bp.om[0] * r1 - bp.om[1] * r0);
     }
   }
+  C dep = C(0);
+  if (kind == BCK_MAP_TRANSPORT_DEPOSITION || kind == BCK_MAP_KINETICS_DEPOSITION) {
+    // rho = sum_k w_k f_inv(k)(a + c_k), coef = sum_k w_k over fluid neighbours;
+    // transport limited j = rho - (rho - coef p0) / (1 + coef lF), kinetics
+    // limited j = rho - beta (rho / coef - p0) / (1 + lF); every link of the
+    // anchor gets j / coef (aslLBGKBC.cxx:477-500, 546-569)
+    C coef = C(0), rs = C(0);
+#pragma unroll
+    for (int k = 1; k < Q; ++k)
+      if (mask >> k & 1u) {
+        const S* out = parity == 0 ? F + (size_t)Lt::inv(k) * g.dstride + sq[k] : F + (size_t)k * g.dstride + sa;
+        coef += C(Lt::w(k));
+        rs += A::get(out, bp) * C(Lt::w(k));
+      }
+    const C rho = A::kDev ? rs + coef : rs;  // deviations summed: add sum_k w_k * 1
+    const C p0 = C(bp.p), lf = C(bp.lf);
+    const C j = kind == BCK_MAP_TRANSPORT_DEPOSITION ? rho - (rho - coef * p0) / (C(1) + coef * lf)
+                                                     : rho - C(bp.beta) * (rho / coef - p0) / (C(1) + lf);
+    dep = j / coef;
+  }
   const C P = C(bp.p);
   const C vv = vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2];
 #pragma unroll
@@ -280,6 +300,10 @@ __global__ void __launch_bounds__(256) k_bc(S* __restrict__ F, const GridDesc g,
         A::put(in, A::rep(fe), bp);
         break;
       }
+      case BCK_MAP_TRANSPORT_DEPOSITION:
+      case BCK_MAP_KINETICS_DEPOSITION:
+        A::put(in, A::rep(dep), bp);
+        break;
     }
   }
 }
@@ -452,6 +476,68 @@ static cudaError_t force_impl(const DomainDev& d, const int4* cells, const uint3
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return launch_reduce_rows(partials, nb, 6, out6, st);
+}
+
+// ComputeSurfaceFluxMap (aslLBGKBC.cxx:623-665): per cell with |map| < 0.9999,
+// flux = sum_k w_k s_k (f*_k(x) - f*_inv(k)(x + c_k)), s_k = +1 for links from a
+// solid x (mask0), -1 from a fluid x (mask_in). The two populations of a link
+// swap slots between the AA representations. A fused no-slip link carries no
+// flux: bounce-back makes its two populations equal, as the separate
+// condition does before the flux is taken.
+template <int Q, class S>
+__global__ void __launch_bounds__(kForceThreads)
+    k_flux(const S* __restrict__ F, const GridDesc g, const int4* __restrict__ cells,
+           const uint32_t* __restrict__ mask_in, int n, float* __restrict__ field, float inv_scale,
+           const uint2* __restrict__ fused, int parity, double* __restrict__ partials) {
+  using Lt = Lattice<Q>;
+  using C = typename Store<S>::C;
+  constexpr bool kDev = std::is_same<S, __half>::value;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[1] = {0};
+  if (t < n) {
+    const int4 an = cells[t];
+    const unsigned m0 = (unsigned)an.w, mi = mask_in[t];
+    const bool px = g.periodic & 1, py = g.periodic & 2, pz = g.periodic & 4;
+    const long long sa = sidx(g, an.x, an.y, an.z);
+    C flux = C(0);
+#pragma unroll
+    for (int k = 1; k < Q; ++k) {
+      const bool b0 = m0 >> k & 1u, bi = mi >> k & 1u;
+      if (!(b0 || bi)) continue;
+      const long long sq = sidx(g, wrap_axis(an.x + Lt::c(k, 0), g.nx, px), wrap_axis(an.y + Lt::c(k, 1), g.ny, py),
+                                wrap_axis(an.z + Lt::c(k, 2), g.nz, pz));
+      if (fused && (((b0 ? fused[sq].x : fused[sa].x) >> (b0 ? k : Lt::inv(k))) & 1u)) continue;
+      const S* pa = F + (size_t)k * g.dstride + sa;
+      const S* pq = F + (size_t)Lt::inv(k) * g.dstride + sq;
+      const S* p0 = parity == 0 ? pa : pq;  // f*_k(x)
+      const S* pI = parity == 0 ? pq : pa;  // f*_inv(k)(x + c_k)
+      C d = kDev ? Store<S>::dev(p0, inv_scale) - Store<S>::dev(pI, inv_scale)
+                 : Store<S>::val(p0, inv_scale) - Store<S>::val(pI, inv_scale);
+      if (bi) d = -d;
+      flux += d * C(Lt::w(k));
+    }
+    if (field) field[aidx(g, an.x, an.y, an.z)] = float(flux);
+    v[0] = double(flux);
+  }
+  block_reduce_rows<1>(v, partials);
+}
+
+template <int Q, class S>
+static cudaError_t flux_impl(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,
+                             float inv_scale, const uint2* fused, int parity, double* partials, double* out1,
+                             cudaStream_t st) {
+  const int nb = force_blocks(n);
+  k_flux<Q, S><<<nb, kForceThreads, 0, st>>>((const S*)d.F, d.g, cells, mask_in, n, field, inv_scale, fused, parity,
+                                             partials);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_reduce_rows(partials, nb, 1, out1, st);
+}
+
+cudaError_t launch_flux(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,
+                        float inv_scale, const uint2* fused, int parity, double* partials, double* out1,
+                        cudaStream_t st) {
+  ASLB_DISPATCH(d, flux_impl, d, cells, mask_in, n, field, inv_scale, fused, parity, partials, out1, st)
 }
 
 cudaError_t launch_force(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,

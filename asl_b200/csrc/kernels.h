@@ -47,6 +47,11 @@ cudaError_t launch_bc_links(const DomainDev& d, const int* links, int n, const L
 // Surface force: per-cell field (ASL layout, optional) and per-block FP64
 // partial sums of (F, (r - r0) x F), then a fixed-order final sum into out6.
 int force_blocks(int n);
+// Surface flux (ComputeSurfaceFluxMap): same cell lists as the force, one
+// value per cell (field, optional) and its FP64 total (out1).
+cudaError_t launch_flux(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,
+                        float inv_scale, const uint2* fused, int parity, double* partials, double* out1,
+                        cudaStream_t st);
 cudaError_t launch_force(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,
                          const double* r0, const double* pos0, double dx, float inv_scale, const uint2* fused,
                          int parity, double* partials, double* out6, cudaStream_t st);

@@ -455,6 +455,61 @@ def generateBCVelocity(lbgk: LBGK, velocity, m) -> BC:
     return _map_bc(lbgk, L.BC_MAP_VELOCITY, m, u=velocity)
 
 
+def _deposition_bc(lbgk: LBGK, kind: int, m, p0: float, lf: float, beta: float) -> BC:
+    arr = _map_array(lbgk, m)
+    h = C.c_void_p()
+    L.check(lbgk.lib.aslb_bc_deposition_create(lbgk.h, kind, arr.ctypes.data_as(L._pf), float(p0), float(lf),
+                                               float(beta), C.byref(h)), "generateBCDeposition")
+    return BC(lbgk, h)
+
+
+def generateBCTransportLimitedDeposition(lbgk: LBGK, p0: float, limitingFactor: float, m) -> BC:
+    """BCTransportLimitedDepositionMap (src/num/aslLBGKBC.cxx:440-506, 878-888)."""
+    return _deposition_bc(lbgk, L.BC_MAP_TRANSPORT_DEPOSITION, m, p0, limitingFactor, 0.0)
+
+
+def generateBCKineticsLimitedDeposition(lbgk: LBGK, p0: float, limitingFactor: float, beta: float, m) -> BC:
+    """BCKineticsLimitedDepositionMap (src/num/aslLBGKBC.cxx:508-575, 891-903);
+    the arguments in the order of the definition (the header names them
+    beta, p0, limitingFactor, but binds them positionally as here)."""
+    return _deposition_bc(lbgk, L.BC_MAP_KINETICS_DEPOSITION, m, p0, limitingFactor, beta)
+
+
+class ComputeSurfaceFlux:
+    """ComputeSurfaceFluxMap (src/num/aslLBGKBC.cxx:623-665): ``execute()``
+    returns the flux field (ghosted, FP32; cells off the surface 0) and its
+    FP64 total."""
+
+    def __init__(self, lbgk: LBGK, m: np.ndarray):
+        self.num = lbgk
+        arr = _map_array(lbgk, m)
+        h = C.c_void_p()
+        L.check(lbgk.lib.aslb_flux_create(lbgk.h, arr.ctypes.data_as(L._pf), C.byref(h)), "ComputeSurfaceFlux")
+        self.h = h
+
+    def init(self):
+        pass
+
+    def execute(self):
+        fld = np.zeros(self.num.block.ghosted, dtype=np.float32)
+        tot = C.c_double()
+        L.check(self.num.lib.aslb_flux_compute(self.h, fld.ctypes.data_as(L._pf), C.byref(tot)),
+                "ComputeSurfaceFlux::execute")
+        return fld, tot.value
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.num.lib.aslb_flux_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def generateComputeSurfaceFlux(lbgk: LBGK, m: np.ndarray) -> ComputeSurfaceFlux:
+    return ComputeSurfaceFlux(lbgk, m)
+
+
 class ComputeSurfaceForce:
     """ComputeSurfaceForceMap (src/num/aslLBGKBC.cxx:674-742) plus an FP64
     reduction to total force and torque about ``r0``."""

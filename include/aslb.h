@@ -71,6 +71,8 @@ extern "C" {
 #define ASLB_BC_MAP_VELOCITY 11
 #define ASLB_BC_MAP_VELOCITY_ROTATION 12
 #define ASLB_BC_MAP_PRESSURE_VELOCITY 13
+#define ASLB_BC_MAP_TRANSPORT_DEPOSITION 14
+#define ASLB_BC_MAP_KINETICS_DEPOSITION 15
 
 /* walls for slice BCs: bit w for asl::SlicesNames {X0,XE,Y0,YE,Z0,ZE}
  * (src/num/aslBCond.h:309) */
@@ -85,6 +87,7 @@ extern "C" {
 typedef struct aslb_lbgk aslb_lbgk;
 typedef struct aslb_bc aslb_bc;
 typedef struct aslb_force aslb_force;
+typedef struct aslb_force aslb_flux;
 typedef struct aslb_batch aslb_batch;
 
 /* Last error message of the calling thread ("" if none). */
@@ -231,6 +234,18 @@ int aslb_bc_slice_create(aslb_lbgk* h, int kind, unsigned wallmask, double p, co
  * generateBCConstantPressureVelocity(map) (src/num/aslLBGKBC.cxx:205-438). */
 int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const double u[3], const double omega[3],
                        const double center[3], aslb_bc** out);
+/* Deposition on a map surface (generateBCTransportLimitedDeposition(nm, p0,
+ * limitingFactor, map) and generateBCKineticsLimitedDeposition(nm, p0,
+ * limitingFactor, beta, map) in the argument order of their definitions,
+ * src/num/aslLBGKBC.cxx:878-903; BCTransportLimitedDepositionMap /
+ * BCKineticsLimitedDepositionMap :440-598). Per solid cell x with fluid
+ * neighbours: rho = sum_k w_k f_inv(k)(x + c_k), coef = sum_k w_k; transport
+ * limited j = rho - (rho - coef p0) / (1 + coef lF), kinetics limited
+ * j = rho - beta (rho / coef - p0) / (1 + lF); f_k(x) = j / coef on every
+ * link. kind: ASLB_BC_MAP_TRANSPORT_DEPOSITION (beta unused) or
+ * ASLB_BC_MAP_KINETICS_DEPOSITION. */
+int aslb_bc_deposition_create(aslb_lbgk* h, int kind, const float* map, double p0, double limiting_factor,
+                              double beta, aslb_bc** out);
 /* Extension (no ASL analogue): fold a no-slip condition (walls or map) into
  * the stream-collide kernel, removing its separate launch. Fluid cells read
  * bounce-back populations inline and solid cells skip the writes the
@@ -272,6 +287,18 @@ int aslb_force_destroy(aslb_force* fc);
  * first call before any stream capture. All calls share the array: calls
  * whose work overlaps on the GPU (different streams) race. Synchronises. */
 int aslb_force_compute_noalloc(aslb_force* fc, const double r0[3], double out6[6]);
+
+/* ---- surface flux -------------------------------------------------------- */
+
+/* generateComputeSurfaceFlux(lbgk, fluxField, map) (src/num/aslLBGKBC.cxx:
+ * 623-665, 906-912): per cell with |map| < 0.9999, flux = sum_k w_k
+ * (f_k(x) - f_inv(k)(x + c_k)) over links from a solid x to fluid neighbours
+ * minus the same over links from a fluid x to solid neighbours. field_host
+ * (L floats, optional) receives the flux field (cells off the surface hold
+ * 0), total (optional) its FP64 sum. Synchronises. */
+int aslb_flux_create(aslb_lbgk* h, const float* map, aslb_flux** out);
+int aslb_flux_compute(aslb_flux* fx, float* field_host, double* total);
+int aslb_flux_destroy(aslb_flux* fx);
 
 /* ---- learned closure: training (extension, no ASL analogue) ------------ */
 

@@ -26,6 +26,9 @@
 //   src/num/aslBCond.cxx:373-510               slice point lists
 //   src/num/aslLBGKBC.cxx:91-202               slice BC values
 //   src/num/aslLBGKBC.cxx:219-432              map BCs and their guards
+//   src/num/aslLBGKBC.cxx:440-598              deposition map BCs (transport
+//                                              and kinetics limited)
+//   src/num/aslLBGKBC.cxx:623-665              ComputeSurfaceFluxMap
 //   src/num/aslLBGKBC.cxx:691-736              ComputeSurfaceForceMap
 //   src/acl/aclMath/aclVectorOfElementsOperations.cxx:249-258
 //                                              component-sequential `+=`
@@ -103,6 +106,8 @@ enum BcKind {
   MAP_VELOCITY = 11,          // constant velocity field
   MAP_VELOCITY_ROTATION = 12, // u = Omega x (r - c)
   MAP_PRESSURE_VELOCITY = 13,
+  MAP_TRANSPORT_DEPOSITION = 14,
+  MAP_KINETICS_DEPOSITION = 15,
 };
 
 struct Bc {
@@ -110,6 +115,7 @@ struct Bc {
   double p;
   double u[3];
   double om[3], cen[3];  // rotation field
+  double lf = 0, beta = 0;  // deposition: limiting factor, kinetic coefficient
   // Slice: (point, direction) pairs in the reference's addSlice order.
   std::vector<long> pts;
   std::vector<int> dirs;
@@ -415,6 +421,21 @@ void bc_execute(Sim<T>& s, Bc& bc) {
           T mc = mom[0] * T(lat.c[k][0]) + mom[1] * T(lat.c[k][1]) + mom[2] * T(lat.c[k][2]);
           f[(long)k * L + cell] = rb + mc * T(3);
         }
+    } else if (bc.kind == MAP_TRANSPORT_DEPOSITION || bc.kind == MAP_KINETICS_DEPOSITION) {
+      // aslLBGKBC.cxx:477-500, 546-569: rho = sum_k w_k f_kbar(x+c_k), coef = sum_k w_k,
+      // transport: j = rho - (rho - coef p0) / (1 + coef lF); kinetics:
+      // j = rho - beta (rho / coef - p0) / (1 + lF); f_k(x) = j / coef
+      T coef = T(0), rho = T(0);
+      for (int k = 1; k < lat.q; ++k)
+        if (mask >> k & 1u) {
+          coef += T(lat.w[k]);
+          rho += f[(long)lat.inv[k] * L + nb(k)] * T(lat.w[k]);
+        }
+      const T p0 = T(bc.p), lf = T(bc.lf);
+      const T j = bc.kind == MAP_TRANSPORT_DEPOSITION ? rho - (rho - coef * p0) / (T(1) + coef * lf)
+                                                      : rho - T(bc.beta) * (rho / coef - p0) / (T(1) + lf);
+      for (int k = 1; k < lat.q; ++k)
+        if (mask >> k & 1u) f[(long)k * L + cell] = j / coef;
     } else if (bc.kind == MAP_PRESSURE_VELOCITY) {
       // aslLBGKBC.cxx:400-423
       T P = T(bc.p), uu[3] = {T(bc.u[0]), T(bc.u[1]), T(bc.u[2])};
@@ -511,6 +532,46 @@ Sim<T>* make_sim(int nx, int ny, int nz, int q, double nu, int flags) {
     else { auto& S = *(h)->sd; call; }         \
   } while (0)
 
+// ComputeSurfaceFluxMap (aslLBGKBC.cxx:623-665), per cell with |map| < 0.9999:
+// flux = sum_k w_k (f_k(x) - f_kbar(x + c_k)) over links from a solid x to a
+// fluid interior neighbour, minus the same over links from a fluid interior x
+// to a solid neighbour. field (L floats) optional; returns the FP64 total.
+template <class T>
+double flux(Sim<T>& s, const float* map, float* field) {
+  const Lattice& lat = s.lat;
+  const long L = s.L;
+  double tot = 0;
+#pragma omp parallel for collapse(2) reduction(+ : tot) schedule(static)
+  for (int x = 0; x < s.G[0]; ++x)
+    for (int y = 0; y < s.G[1]; ++y)
+      for (int z = 0; z < s.G[2]; ++z) {
+        if ((s.periodic[0] && (x < 1 || x > s.N[0])) || (s.periodic[1] && (y < 1 || y > s.N[1])) ||
+            (s.periodic[2] && (z < 1 || z > s.N[2])))
+          continue;
+        long n = s.idx(x, y, z);
+        float m0 = map[n];
+        if (!(std::fabs(m0) < 0.9999f)) continue;
+        T fl = T(0);
+        bool in0 = s.interior(x, y, z), any = false;
+        for (int k = 1; k < lat.q; ++k) {
+          int q[3] = {s.wrapc(x + lat.c[k][0], 0), s.wrapc(y + lat.c[k][1], 1), s.wrapc(z + lat.c[k][2], 2)};
+          double mk = map_at(s, map, q[0], q[1], q[2]);
+          bool b0 = (m0 <= 0.f) && (mk > 0.0) && s.interior(q[0], q[1], q[2]);
+          bool bI = (mk <= 0.0) && (m0 > 0.f) && in0;
+          if (!b0 && !bI) continue;
+          any = true;
+          long nq = s.idx(q[0], q[1], q[2]);
+          T f0 = s.f[(long)k * L + n];
+          T fI = s.f[(long)lat.inv[k] * L + nq];
+          fl += (b0 ? (f0 - fI) : (fI - f0)) * T(lat.w[k]);
+        }
+        if (!any) continue;
+        if (field) field[n] = float(fl);
+        tot += double(fl);
+      }
+  return tot;
+}
+
 extern "C" {
 
 // flags: bit0 no velocity output, bit1 no density output, bit2 incompressible,
@@ -601,6 +662,30 @@ int orc_bc_map(void* p, int kind, const float* map, double pr, const double* u, 
     id = (int)S.bcs.size() - 1;
   });
   return id;
+}
+
+int orc_bc_deposition(void* p, int kind, const float* map, double p0, double lf, double beta) {
+  auto* h = (Handle*)p;
+  int id = -1;
+  DISPATCH(h, {
+    Bc bc;
+    bc.kind = kind;
+    bc.p = p0;
+    bc.lf = lf;
+    bc.beta = beta;
+    for (int d = 0; d < 3; ++d) bc.u[d] = bc.om[d] = bc.cen[d] = 0.0;
+    build_map_links(S, bc, map);
+    S.bcs.push_back(std::move(bc));
+    id = (int)S.bcs.size() - 1;
+  });
+  return id;
+}
+
+double orc_flux(void* p, const float* map, float* field) {
+  auto* h = (Handle*)p;
+  double t = 0;
+  DISPATCH(h, t = flux(S, map, field));
+  return t;
 }
 
 long orc_bc_size(void* p, int id) {

@@ -61,6 +61,8 @@ def load():
             "orc_bc_size": (C.c_long, [vp, C.c_int]),
             "orc_bc_execute": (None, [vp, C.c_int]),
             "orc_force": (None, [vp, pf, pf, pd, pd]),
+            "orc_bc_deposition": (C.c_int, [vp, C.c_int, pf, d, d, d]),
+            "orc_flux": (C.c_double, [vp, pf, pf]),
             "orc_size": (C.c_long, [vp]),
             "orc_get_f": (None, [vp, pd]),
             "orc_set_f": (None, [vp, pd]),
@@ -153,6 +155,17 @@ class Oracle:
 
     def bc_size(self, bid) -> int:
         return int(self.lib.orc_bc_size(self.h, int(bid)))
+
+    def bc_deposition(self, kind, m, p0, lf, beta=0.0) -> int:
+        mm = np.ascontiguousarray(m, dtype=np.float32)
+        return self.lib.orc_bc_deposition(self.h, int(kind), _fp(mm), float(p0), float(lf), float(beta))
+
+    def flux(self, m):
+        """(flux field, FP64 total) of ComputeSurfaceFluxMap."""
+        mm = np.ascontiguousarray(m, dtype=np.float32)
+        fld = np.zeros(self.g, dtype=np.float32)
+        tot = self.lib.orc_flux(self.h, _fp(mm), _fp(fld))
+        return fld, float(tot)
 
     def force(self, m, r0=(0.0, 0.0, 0.0), field=False):
         mm = np.ascontiguousarray(m, dtype=np.float32)

@@ -167,7 +167,7 @@ class NumpyLBGK:
     def _skip(self, x):
         return any(self.periodic[a] and not (1 <= x[a] <= self.N[a]) for a in range(3))
 
-    def apply_map(self, kind, m, p=0.0, u=(0, 0, 0)):
+    def apply_map(self, kind, m, p=0.0, u=(0, 0, 0), lf=0.0, beta=0.0):
         m = np.asarray(m, np.float32)
         u = np.asarray(u, float)
         writes = []
@@ -192,8 +192,37 @@ class NumpyLBGK:
                     cu = u @ self.c[k]
                     fe = p + 3 * p * cu + 4.5 * p * cu * cu - 1.5 * p * (u @ u)
                     writes.append((k, x, fe))
+            elif kind in ("transport_deposition", "kinetics_deposition"):
+                # p is p0: transport limited j = rho - (rho - coef p0) / (1 + coef lf),
+                # kinetics limited j = rho - beta (rho / coef - p0) / (1 + lf)
+                coef = sum(self.w[k] for k in ks)
+                rho = sum(self.f[self.inv[k]][self._nb(x, k)] * self.w[k] for k in ks)
+                if kind == "transport_deposition":
+                    j = rho - (rho - coef * p) / (1 + coef * lf)
+                else:
+                    j = rho - beta * (rho / coef - p) / (1 + lf)
+                for k in ks:
+                    writes.append((k, x, j / coef))
         for k, x, v in writes:
             self.f[k][x] = v
+
+    def flux(self, m):
+        """Surface flux field and total (ComputeSurfaceFluxMap)."""
+        m = np.asarray(m, np.float32)
+        F = np.zeros(self.G)
+        for x in np.ndindex(*self.G):
+            if self._skip(x) or not (abs(m[x]) < np.float32(0.9999)):
+                continue
+            for k in range(1, self.q):
+                nb = self._nb(x, k)
+                mk = self._map(m, nb)
+                b0 = m[x] <= 0 and mk > 0 and self._interior(nb)
+                bi = mk <= 0 and m[x] > 0 and self._interior(x)
+                if b0:
+                    F[x] += (self.f[k][x] - self.f[self.inv[k]][nb]) * self.w[k]
+                elif bi:
+                    F[x] += (self.f[self.inv[k]][nb] - self.f[k][x]) * self.w[k]
+        return F, F.sum()
 
     def force(self, m, r0=(0, 0, 0)):
         m = np.asarray(m, np.float32)

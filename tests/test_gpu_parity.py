@@ -460,3 +460,69 @@ def test_fused_cells_with_both_link_kinds(gpu):
         out.append(lb.getF())
     assert np.array_equal(out[0], out[1], equal_nan=True)
     assert np.array_equal(out[0], out[2], equal_nan=True)
+
+
+@pytest.mark.parametrize("kind", [14, 15])
+@pytest.mark.parametrize("storage,prec,tol", [("f64", 8, 1e-12), ("f32", 4, 1e-5)])
+def test_deposition_and_flux_match_oracle(gpu, oracle_mod, kind, storage, prec, tol):
+    """Deposition on a sphere map inside a closed box, after odd and even step
+    counts: populations against the oracle, then the surface flux field and
+    total (ComputeSurfaceFlux) on the same map. beta = 0.03 keeps the kinetics
+    limited condition contracting (1 - beta / ((1 + lF) coef) > -1 for the
+    smallest coef = 1/36); larger values make it amplify rounding step by step."""
+    size = (14, 10, 12)
+    g = tuple(s + 2 for s in size)
+    rho, u = smooth_field(g, 70 + kind, amp=0.02)
+    sphere = sphere_map(g, (6.5, 4.5, 5.5), 2.6)
+    lb = A.LBGK(A.Block(size), 0.04, A.d3q19(), storage=storage)
+    A.LBGKUtilities(lb).initF(rho, u)
+    if kind == 14:
+        dep = A.generateBCTransportLimitedDeposition(lb, 0.97, 0.4, sphere)
+    else:
+        dep = A.generateBCKineticsLimitedDeposition(lb, 0.97, 0.4, 0.03, sphere)
+    bcs = [A.generateBCNoSlip(lb, [A.X0, A.XE, A.Y0, A.YE, A.Z0, A.ZE]), dep]
+    flux = A.generateComputeSurfaceFlux(lb, sphere)
+    o = oracle_mod.Oracle(size, 19, prec, 0.04)
+    o.init_f_fields(rho, u)
+    ids = [o.bc_slice(0, 63), o.bc_deposition(kind, sphere, 0.97, 0.4, 0.03)]
+    for n in (5, 6):
+        lb.run(n, bcs)
+        for _ in range(n):
+            o.step(1)
+            for i in ids:
+                o.bc_execute(i)
+        assert np.abs(lb.getF()[I4] - o.get_f()[I4]).max() <= tol
+        fld, tot = flux.execute()
+        ofld, otot = o.flux(sphere)
+        assert np.abs(fld - ofld).max() <= max(tol, 1e-6) * 10
+        assert abs(tot - otot) <= max(tol, 1e-9) * 100 * max(1.0, abs(otot))
+        assert np.abs(ofld).max() > 1e-4
+
+
+@pytest.mark.parametrize("fuse", [False, True])
+def test_flux_of_no_slip_map(gpu, oracle_mod, fuse):
+    """The flux through a no-slip surface is zero link by link once the
+    condition has run; with the condition fused into the stream-collide
+    kernel the flux object must see the same (its links carry none)."""
+    w = W.channel_cylinder(size=(32, 16, 16), radius=3.0, center=(10.0, 8.0))
+    lb, bcs = W.build_lbgk(w, "f64", fuse=fuse)
+    lb.run(9, bcs)
+    fld, tot = A.generateComputeSurfaceFlux(lb, w.map).execute()
+    assert np.abs(fld).max() <= 1e-15 and abs(tot) <= 1e-13
+
+
+def test_deposition_f16_close_to_f32(gpu):
+    size = (14, 10, 12)
+    g = tuple(s + 2 for s in size)
+    rho, u = smooth_field(g, 90, amp=0.02)
+    sphere = sphere_map(g, (6.5, 4.5, 5.5), 2.6)
+    out = []
+    for storage in ("f32", "f16"):
+        lb = A.LBGK(A.Block(size), 0.04, A.d3q19(), storage=storage)
+        A.LBGKUtilities(lb).initF(rho, u)
+        bcs = [A.generateBCNoSlip(lb, [A.X0, A.XE, A.Y0, A.YE, A.Z0, A.ZE]),
+               A.generateBCTransportLimitedDeposition(lb, 0.97, 0.4, sphere)]
+        lb.run(20, bcs)
+        out.append((lb.getF()[I4], A.generateComputeSurfaceFlux(lb, sphere).execute()[1]))
+    assert np.abs(out[0][0] - out[1][0]).max() <= 2e-3
+    assert abs(out[0][1] - out[1][1]) <= 2e-3 * max(1.0, abs(out[0][1]))

@@ -137,6 +137,60 @@ def test_oracle_matches_numpy_boundaries(oracle_mod, q):
     assert np.allclose(out, ref_out, rtol=1e-10, atol=1e-12)
 
 
+@pytest.mark.parametrize("kind,name", [(14, "transport_deposition"), (15, "kinetics_deposition")])
+def test_oracle_deposition_and_flux_match_numpy(oracle_mod, kind, name):
+    """Deposition conditions on a sphere map (p0 = 0.97, limiting factor 0.4,
+    beta 0.03) and the surface flux, against the numpy restatement."""
+    size = (8, 6, 7)
+    g = tuple(s + 2 for s in size)
+    rho, u = _smooth_field(g, 23, amp=0.02)
+    pos = np.stack(np.meshgrid(*[np.arange(n) - 1.0 for n in g], indexing="ij"))
+    sphere = np.clip((np.sqrt(((pos - np.array([4.0, 3.0, 3.5]).reshape(3, 1, 1, 1)) ** 2).sum(0)) - 1.7) / 1.8,
+                     -1, 1).astype(np.float32)
+    o = oracle_mod.Oracle(size, 19, 8, 0.04)
+    o.init_f_fields(rho, u)
+    ref = NumpyLBGK(size, 19, 0.04)
+    ref.init_f(rho, u)
+    ids = [o.bc_slice(SLICE["noslip"], 63), o.bc_deposition(kind, sphere, 0.97, 0.4, 0.03)]
+    for _ in range(3):
+        o.step(1)
+        ref.step()
+        for bid in ids:
+            o.bc_execute(bid)
+        ref.apply_slice("noslip", ("X0", "XE", "Y0", "YE", "Z0", "ZE"))
+        ref.apply_map(name, sphere, 0.97, lf=0.4, beta=0.03)
+    assert np.allclose(o.get_f(), ref.f, rtol=0, atol=1e-13)
+    fld, tot = o.flux(sphere)
+    ref_fld, ref_tot = ref.flux(sphere)
+    assert np.allclose(fld, ref_fld, atol=1e-6)
+    assert abs(tot - ref_tot) <= 1e-12 * max(1.0, abs(ref_tot))
+    assert np.abs(ref_fld).max() > 1e-4  # the condition makes a flux
+
+
+def test_deposition_single_cell_by_hand(oracle_mod):
+    """One solid cell with known fluid neighbours: f_k = j / coef with the
+    formulas of aslLBGKBC.cxx:477-500 evaluated by hand."""
+    size = (5, 5, 5)
+    g = tuple(s + 2 for s in size)
+    m = np.ones(g, dtype=np.float32)
+    m[3, 3, 3] = -0.5  # interior cell (2, 2, 2) in ghosted coordinates (3, 3, 3)
+    o = oracle_mod.Oracle(size, 19, 8, 0.04)
+    rng = np.random.default_rng(4)
+    f = 1.0 + 0.1 * rng.standard_normal((19, *g))
+    o.set_f(f)
+    lat = NumpyLBGK(size, 19, 0.04)
+    w, c, inv = lat.w, lat.c, lat.inv
+    rho = sum(w[k] * f[inv[k], 3 + c[k][0], 3 + c[k][1], 3 + c[k][2]] for k in range(1, 19))
+    coef = sum(w[k] for k in range(1, 19))
+    for kind, j in ((14, rho - (rho - coef * 0.9) / (1 + coef * 0.3)), (15, rho - 0.7 * (rho / coef - 0.9) / (1 + 0.3))):
+        o.set_f(f)
+        o.bc_execute(o.bc_deposition(kind, m, 0.9, 0.3, 0.7))
+        got = o.get_f()
+        for k in range(1, 19):
+            assert abs(got[k, 3, 3, 3] - j / coef) < 1e-14
+        assert got[0, 3, 3, 3] == f[0, 3, 3, 3]
+
+
 def test_force_at_rest_is_zero(oracle_mod):
     size = (10, 8, 8)
     g = tuple(s + 2 for s in size)
