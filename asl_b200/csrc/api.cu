@@ -1042,7 +1042,9 @@ int aslb_bc_slice_create(aslb_lbgk* h, int kind, unsigned wallmask, double p, co
 namespace {
 // Cell x is processed iff -0.9999 < map(x) <= 0; link k iff map(x + c_k) > 0
 // (src/num/aslLBGKBC.cxx:235-251), counted when x + c_k is an interior cell.
-void map_candidates(const aslb_lbgk* h, const float* map, std::vector<Cand>& cand) {
+// With a computational-domain map cd, a neighbour also needs cd > 0 to be a
+// computation node (src/num/aslBCond.cxx:204-211; cd reads -1 off the grid).
+void map_candidates(const aslb_lbgk* h, const float* map, std::vector<Cand>& cand, const float* cd = nullptr) {
   const GridDesc& g = h->d.g;
   const int q = h->d.q;
   for (int x = 0; x < g.gx; ++x)
@@ -1055,7 +1057,7 @@ void map_candidates(const aslb_lbgk* h, const float* map, std::vector<Cand>& can
           const int qx = wrapc(h, x + lattice_c(q, k, 0), 0), qy = wrapc(h, y + lattice_c(q, k, 1), 1),
                     qz = wrapc(h, z + lattice_c(q, k, 2), 2);
           if (!interior(g, qx, qy, qz)) continue;
-          if (map_at(g, map, qx, qy, qz) > 0.f) cand.push_back({x, y, z, k});
+          if (map_at(g, map, qx, qy, qz) > 0.f && (!cd || cd[aidx(g, qx, qy, qz)] > 0.f)) cand.push_back({x, y, z, k});
         }
       }
 }
@@ -1097,13 +1099,18 @@ int aslb_bc_deposition_create(aslb_lbgk* h, int kind, const float* map, double p
 
 int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const double u[3], const double omega[3],
                        const double center[3], aslb_bc** out) {
+  return aslb_bc_map_create_cd(h, kind, map, nullptr, p, u, omega, center, out);
+}
+
+int aslb_bc_map_create_cd(aslb_lbgk* h, int kind, const float* map, const float* cdomain, double p, const double u[3],
+                          const double omega[3], const double center[3], aslb_bc** out) {
   ASLB_CHECK_HANDLE(h);
   if (!out || !map) return fail(ASLB_ERR_ARG, "aslb_bc_map_create: null argument");
   *out = nullptr;
   if (kind < ASLB_BC_MAP_NOSLIP || kind > ASLB_BC_MAP_PRESSURE_VELOCITY)
     return fail(ASLB_ERR_ARG, "aslb_bc_map_create: unknown map kind");
   std::vector<Cand> cand;
-  map_candidates(h, map, cand);
+  map_candidates(h, map, cand, cdomain);
   if (cand.size() >= (size_t)(1u << 31)) return fail(ASLB_ERR_ARG, "aslb_bc_map_create: too many boundary links");
   auto* bc = new aslb_bc();
   bc->h = h;

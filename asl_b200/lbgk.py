@@ -394,11 +394,14 @@ def _slice_bc(lbgk: LBGK, kind: int, slices, p: float = 0.0, u=(0.0, 0.0, 0.0)) 
     return BC(lbgk, h)
 
 
-def _map_bc(lbgk: LBGK, kind: int, m, p=0.0, u=(0.0, 0.0, 0.0), omega=(0.0, 0.0, 0.0), center=(0.0, 0.0, 0.0)) -> BC:
+def _map_bc(lbgk: LBGK, kind: int, m, p=0.0, u=(0.0, 0.0, 0.0), omega=(0.0, 0.0, 0.0), center=(0.0, 0.0, 0.0),
+            cdomain=None) -> BC:
     arr = _map_array(lbgk, m)
+    cd = None if cdomain is None else _map_array(lbgk, cdomain)
     h = C.c_void_p()
-    L.check(lbgk.lib.aslb_bc_map_create(lbgk.h, kind, arr.ctypes.data_as(L._pf), float(p), L.dvec(u), L.dvec(omega),
-                                        L.dvec(center), C.byref(h)), "generateBC")
+    L.check(lbgk.lib.aslb_bc_map_create_cd(lbgk.h, kind, arr.ctypes.data_as(L._pf),
+                                           None if cd is None else cd.ctypes.data_as(L._pf), float(p), L.dvec(u),
+                                           L.dvec(omega), L.dvec(center), C.byref(h)), "generateBC")
     return BC(lbgk, h)
 
 
@@ -446,13 +449,16 @@ def generatePFRotationField(omega, center) -> PFRotationField:
     return PFRotationField(tuple(float(a) for a in omega), tuple(float(a) for a in center))
 
 
-def generateBCVelocity(lbgk: LBGK, velocity, m) -> BC:
-    """BCVelocityMap (src/num/aslLBGKBC.cxx:262-354) with a constant or rotation field."""
+def generateBCVelocity(lbgk: LBGK, velocity, m, computationalDomain=None) -> BC:
+    """BCVelocityMap (src/num/aslLBGKBC.cxx:262-354) with a constant or rotation
+    field; with ``computationalDomain`` only neighbours where that map is
+    positive are fluid ends (the four-argument overload, :837-844)."""
     if isinstance(velocity, PFRotationField):
-        return _map_bc(lbgk, L.BC_MAP_VELOCITY_ROTATION, m, omega=velocity.omega, center=velocity.center)
+        return _map_bc(lbgk, L.BC_MAP_VELOCITY_ROTATION, m, omega=velocity.omega, center=velocity.center,
+                       cdomain=computationalDomain)
     if isinstance(velocity, PFConstant):
         velocity = velocity.value
-    return _map_bc(lbgk, L.BC_MAP_VELOCITY, m, u=velocity)
+    return _map_bc(lbgk, L.BC_MAP_VELOCITY, m, u=velocity, cdomain=computationalDomain)
 
 
 def _deposition_bc(lbgk: LBGK, kind: int, m, p0: float, lf: float, beta: float) -> BC:

@@ -234,6 +234,12 @@ int aslb_bc_slice_create(aslb_lbgk* h, int kind, unsigned wallmask, double p, co
  * generateBCConstantPressureVelocity(map) (src/num/aslLBGKBC.cxx:205-438). */
 int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const double u[3], const double omega[3],
                        const double center[3], aslb_bc** out);
+/* The same with a computational-domain map (L floats, host; NULL for none):
+ * a neighbour is a fluid end only where map > 0 and cdomain > 0, as in
+ * generateBCVelocity(nm, v, map, computationalDomain)
+ * (src/num/aslLBGKBC.cxx:273-282, 837-844; src/num/aslBCond.cxx:204-211). */
+int aslb_bc_map_create_cd(aslb_lbgk* h, int kind, const float* map, const float* cdomain, double p, const double u[3],
+                          const double omega[3], const double center[3], aslb_bc** out);
 /* Deposition on a map surface (generateBCTransportLimitedDeposition(nm, p0,
  * limitingFactor, map) and generateBCKineticsLimitedDeposition(nm, p0,
  * limitingFactor, beta, map) in the argument order of their definitions,

@@ -323,8 +323,10 @@ double map_at(const Sim<T>& s, const float* map, int x, int y, int z) {
 
 // Map BC guard and links (aslLBGKBC.cxx:219-254): a cell x is processed iff
 // -0.9999 < map(x) <= 0; link k iff map(x + c_k) > 0 (fluid end interior).
+// With a computational-domain map cd, a neighbour also needs cd > 0
+// (src/num/aslBCond.cxx:204-211).
 template <class T>
-void build_map_links(Sim<T>& s, Bc& bc, const float* map) {
+void build_map_links(Sim<T>& s, Bc& bc, const float* map, const float* cd = nullptr) {
   const Lattice& lat = s.lat;
   for (int x = 0; x < s.G[0]; ++x)
     for (int y = 0; y < s.G[1]; ++y)
@@ -338,7 +340,7 @@ void build_map_links(Sim<T>& s, Bc& bc, const float* map) {
         for (int k = 1; k < lat.q; ++k) {
           int q[3] = {s.wrapc(x + lat.c[k][0], 0), s.wrapc(y + lat.c[k][1], 1), s.wrapc(z + lat.c[k][2], 2)};
           if (!s.interior(q[0], q[1], q[2])) continue;
-          if (map_at(s, map, q[0], q[1], q[2]) > 0.0) mask |= 1u << k;
+          if (map_at(s, map, q[0], q[1], q[2]) > 0.0 && (!cd || cd[s.idx(q[0], q[1], q[2])] > 0.f)) mask |= 1u << k;
         }
         if (mask) {
           bc.cells.push_back(s.idx(x, y, z));
@@ -638,6 +640,26 @@ int orc_bc_slice(void* p, int kind, int wallmask, double pr, double ux, double u
     bc.p = pr;
     bc.u[0] = ux; bc.u[1] = uy; bc.u[2] = uz;
     add_slices(S, bc, wallmask);
+    S.bcs.push_back(std::move(bc));
+    id = (int)S.bcs.size() - 1;
+  });
+  return id;
+}
+
+int orc_bc_map_cd(void* p, int kind, const float* map, const float* cd, double pr, const double* u,
+                  const double* om, const double* cen) {
+  auto* h = (Handle*)p;
+  int id = -1;
+  DISPATCH(h, {
+    Bc bc;
+    bc.kind = kind;
+    bc.p = pr;
+    for (int d = 0; d < 3; ++d) {
+      bc.u[d] = u ? u[d] : 0.0;
+      bc.om[d] = om ? om[d] : 0.0;
+      bc.cen[d] = cen ? cen[d] : 0.0;
+    }
+    build_map_links(S, bc, map, cd);
     S.bcs.push_back(std::move(bc));
     id = (int)S.bcs.size() - 1;
   });

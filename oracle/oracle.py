@@ -62,6 +62,7 @@ def load():
             "orc_bc_execute": (None, [vp, C.c_int]),
             "orc_force": (None, [vp, pf, pf, pd, pd]),
             "orc_bc_deposition": (C.c_int, [vp, C.c_int, pf, d, d, d]),
+            "orc_bc_map_cd": (C.c_int, [vp, C.c_int, pf, pf, d, pd, pd, pd]),
             "orc_flux": (C.c_double, [vp, pf, pf]),
             "orc_size": (C.c_long, [vp]),
             "orc_get_f": (None, [vp, pd]),
@@ -145,9 +146,13 @@ class Oracle:
     def bc_slice(self, kind, wallmask, p=0.0, u=(0.0, 0.0, 0.0)) -> int:
         return self.lib.orc_bc_slice(self.h, int(kind), int(wallmask), float(p), *map(float, u))
 
-    def bc_map(self, kind, m, p=0.0, u=(0.0, 0.0, 0.0), omega=(0.0, 0.0, 0.0), center=(0.0, 0.0, 0.0)) -> int:
+    def bc_map(self, kind, m, p=0.0, u=(0.0, 0.0, 0.0), omega=(0.0, 0.0, 0.0), center=(0.0, 0.0, 0.0),
+               cdomain=None) -> int:
         mm = np.ascontiguousarray(m, dtype=np.float32)
         uu, om, ce = (np.asarray(v, dtype=np.float64) for v in (u, omega, center))
+        if cdomain is not None:
+            cd = np.ascontiguousarray(cdomain, dtype=np.float32)
+            return self.lib.orc_bc_map_cd(self.h, int(kind), _fp(mm), _fp(cd), float(p), _dp(uu), _dp(om), _dp(ce))
         return self.lib.orc_bc_map(self.h, int(kind), _fp(mm), float(p), _dp(uu), _dp(om), _dp(ce))
 
     def bc_execute(self, bid):

@@ -167,7 +167,7 @@ class NumpyLBGK:
     def _skip(self, x):
         return any(self.periodic[a] and not (1 <= x[a] <= self.N[a]) for a in range(3))
 
-    def apply_map(self, kind, m, p=0.0, u=(0, 0, 0), lf=0.0, beta=0.0):
+    def apply_map(self, kind, m, p=0.0, u=(0, 0, 0), lf=0.0, beta=0.0, cd=None):
         m = np.asarray(m, np.float32)
         u = np.asarray(u, float)
         writes = []
@@ -176,7 +176,8 @@ class NumpyLBGK:
                 continue
             if not (m[x] <= 0 and m[x] > np.float32(-0.9999)):
                 continue
-            ks = [k for k in range(1, self.q) if self._interior(self._nb(x, k)) and self._map(m, self._nb(x, k)) > 0]
+            ks = [k for k in range(1, self.q) if self._interior(self._nb(x, k)) and self._map(m, self._nb(x, k)) > 0
+                  and (cd is None or cd[self._nb(x, k)] > 0)]
             if not ks:
                 continue
             if kind == "noslip":

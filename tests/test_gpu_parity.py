@@ -526,3 +526,38 @@ def test_deposition_f16_close_to_f32(gpu):
         out.append((lb.getF()[I4], A.generateComputeSurfaceFlux(lb, sphere).execute()[1]))
     assert np.abs(out[0][0] - out[1][0]).max() <= 2e-3
     assert abs(out[0][1] - out[1][1]) <= 2e-3 * max(1.0, abs(out[0][1]))
+
+
+@pytest.mark.parametrize("field", ["constant", "rotation"])
+def test_velocity_map_with_computational_domain(gpu, oracle_mod, field):
+    """generateBCVelocity(nm, v, map, computationalDomain) against the oracle:
+    only neighbours inside the computational domain are fluid ends."""
+    size = (16, 12, 10)
+    g = tuple(s + 2 for s in size)
+    rho, u = smooth_field(g, 41, amp=0.02)
+    vmap = sphere_map(g, (7.5, 5.5, 4.5), 2.4)
+    pos = np.stack(np.meshgrid(*[np.arange(n) - 1.0 for n in g], indexing="ij"))
+    cd = np.where(pos[0] + 0.5 * pos[1] < 11.0, 1.0, -0.5).astype(np.float32)
+    lb = A.LBGK(A.Block(size), 0.03, A.d3q19(), storage="f64")
+    A.LBGKUtilities(lb).initF(rho, u)
+    if field == "constant":
+        v = A.generatePFConstant((0.01, 0.02, -0.01))
+        kw = dict(u=(0.01, 0.02, -0.01))
+        kind = MAPK["velocity"]
+    else:
+        v = A.generatePFRotationField((0.0, 0.0, 0.01), (7.5, 5.5, 4.5))
+        kw = dict(omega=(0.0, 0.0, 0.01), center=(7.5, 5.5, 4.5))
+        kind = 12
+    bcs = [A.generateBCNoSlip(lb, [A.X0, A.XE, A.Y0, A.YE, A.Z0, A.ZE]), A.generateBCVelocity(lb, v, vmap, cd)]
+    full = A.generateBCVelocity(lb, v, vmap)
+    assert 0 < bcs[1].num_links < full.num_links
+    o = oracle_mod.Oracle(size, 19, 8, 0.03)
+    o.init_f_fields(rho, u)
+    ids = [o.bc_slice(0, 63), o.bc_map(kind, vmap, 0.0, cdomain=cd, **kw)]
+    for n in (3, 4):
+        lb.run(n, bcs)
+        for _ in range(n):
+            o.step(1)
+            for i in ids:
+                o.bc_execute(i)
+        assert np.abs(lb.getF()[I4] - o.get_f()[I4]).max() <= 1e-12

@@ -167,6 +167,31 @@ def test_oracle_deposition_and_flux_match_numpy(oracle_mod, kind, name):
     assert np.abs(ref_fld).max() > 1e-4  # the condition makes a flux
 
 
+def test_oracle_velocity_map_with_computational_domain(oracle_mod):
+    """generateBCVelocity(nm, v, map, computationalDomain): neighbours outside
+    the computational domain (cd <= 0) are not fluid ends."""
+    size = (8, 7, 6)
+    g = tuple(s + 2 for s in size)
+    rho, u = _smooth_field(g, 31, amp=0.02)
+    pos = np.stack(np.meshgrid(*[np.arange(n) - 1.0 for n in g], indexing="ij"))
+    vmap = np.clip((np.sqrt(((pos - np.array([4.0, 3.0, 2.5]).reshape(3, 1, 1, 1)) ** 2).sum(0)) - 1.5) / 1.8,
+                   -1, 1).astype(np.float32)
+    cd = np.where(pos[1] < 3.0, 1.0, -1.0).astype(np.float32)  # only y < 3 computes
+    o = oracle_mod.Oracle(size, 19, 8, 0.03)
+    o.init_f_fields(rho, u)
+    ref = NumpyLBGK(size, 19, 0.03)
+    ref.init_f(rho, u)
+    full = o.bc_map(MAPK["velocity"], vmap, 0.0, (0.01, 0.02, 0.0))
+    part = o.bc_map(MAPK["velocity"], vmap, 0.0, (0.01, 0.02, 0.0), cdomain=cd)
+    assert 0 < o.bc_size(part) < o.bc_size(full)
+    for _ in range(2):
+        o.step(1)
+        ref.step()
+        o.bc_execute(part)
+        ref.apply_map("velocity", vmap, 0.0, (0.01, 0.02, 0.0), cd=cd)
+    assert np.allclose(o.get_f(), ref.f, rtol=0, atol=1e-13)
+
+
 def test_deposition_single_cell_by_hand(oracle_mod):
     """One solid cell with known fluid neighbours: f_k = j / coef with the
     formulas of aslLBGKBC.cxx:477-500 evaluated by hand."""
