@@ -70,6 +70,16 @@ PROTOTYPES = {
     "aslb_flux_create": (C.c_int, [_vp, _vp, _vp]),
     "aslb_flux_compute": (C.c_int, [_vp, _vp, _vp]),
     "aslb_flux_destroy": (C.c_int, [_vp]),
+    "aslb_fd_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _vp]),
+    "aslb_fd_set_velocity": (C.c_int, [_vp, _vp, C.c_int]),
+    "aslb_fd_set_diffusion": (C.c_int, [_vp, C.c_double]),
+    "aslb_fd_write": (C.c_int, [_vp, C.c_int, _vp]),
+    "aslb_fd_read": (C.c_int, [_vp, C.c_int, _vp]),
+    "aslb_fd_set_face_value": (C.c_int, [_vp, C.c_uint, C.c_double]),
+    "aslb_fd_step": (C.c_int, [_vp, C.c_int]),
+    "aslb_fd_sync": (C.c_int, [_vp]),
+    "aslb_fd_device_field": (_vp, [_vp]),
+    "aslb_fd_destroy": (C.c_int, [_vp]),
     "aslb_read_stl": (C.c_int, [C.c_char_p, _vp, C.c_longlong, _vp]),
     "aslb_surface_map": (C.c_int, [_vp, C.c_longlong, C.c_int, C.c_int, C.c_int, _pd, C.c_double, C.c_double,
                                    C.c_int, C.c_double, C.c_double, _vp]),

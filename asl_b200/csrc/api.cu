@@ -76,7 +76,30 @@ struct aslb_lbgk {
   std::vector<aslb_bc*> bcs;
   std::vector<aslb_force*> forces;
   std::vector<aslb_batch*> batches;  // batches this domain belongs to
+  std::vector<aslb_fd*> fds;         // FD solvers reading its velocity
 };
+
+namespace aslb {
+int lbgk_velocity_binding(aslb_lbgk* h, int n[3], int* storage, void** u, cudaStream_t* st) {
+  if (!h) {
+    set_last_error("aslb_fd_set_velocity: null domain");
+    return ASLB_ERR_ARG;
+  }
+  if (!h->comp_vel) {
+    set_last_error("aslb_fd_set_velocity: the domain does not write its velocity (created with ASLB_NO_VELOCITY)");
+    return ASLB_ERR_ARG;
+  }
+  n[0] = h->d.g.nx;
+  n[1] = h->d.g.ny;
+  n[2] = h->d.g.nz;
+  *storage = h->d.storage;
+  *u = h->d.u;
+  *st = h->stream;
+  return ASLB_OK;
+}
+void lbgk_attach_fd(aslb_lbgk* h, aslb_fd* f) { h->fds.push_back(f); }
+void lbgk_detach_fd(aslb_lbgk* h, aslb_fd* f) { h->fds.erase(std::remove(h->fds.begin(), h->fds.end(), f), h->fds.end()); }
+}  // namespace aslb
 
 struct aslb_bc {
   aslb_lbgk* h = nullptr;
@@ -429,6 +452,8 @@ int aslb_lbgk_destroy(aslb_lbgk* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   drop_graph(h);
   for (aslb_batch* b : std::vector<aslb_batch*>(h->batches)) batch_detach(b, h);
+  for (aslb_fd* f : h->fds) fd_detached(f);
+  h->fds.clear();
   for (aslb_bc* bc : h->bcs) {
     cudaFree(bc->anchors);
     cudaFree(bc->dlinks);

@@ -1,0 +1,298 @@
+// Finite-difference advection-diffusion coupled to the LBGK velocity field:
+// ASL's FDAdvectionDiffusion (src/num/aslFDAdvectionDiffusion.cxx:88-180,
+// 209-226) for one component with a constant diffusion coefficient D,
+//   c' = D lap(c) + c - divProduct(u, c)
+//   (compressibility correction: c' /= 1 - div(u); c' += lap(c) |u(x)|^2 / 2)
+// with the stencil operators of src/math/aslTemplateVE.cxx:164-267 on the
+// templates d3q7 / d3q15 / d3q19 (laplacian and gradient coefficients of
+// src/math/aslTemplates.cxx:134-186):
+//   lap(c)            = sum_i LC_i c(x + e_i)
+//   div(u)            = sum_d sum_i GC_i e_i,d u_d(x + e_i)
+//   divProduct(u, c)  = sum_d sum_i GC_i e_i,d (u_d(x + e_i) + u_d(x)) (c(x + e_i) + c(x)) / 2
+// The update writes the interior of a second buffer and the buffers swap
+// (postProcessing), so ghost values persist in both: they are the
+// boundary values (BCConstantValue on faces, src/num/aslBasicBC.cxx:51-57).
+// The velocity is the bound LBGK's device velocity field (ASL layout, FP32,
+// FP64 for FP64 storage), read on that domain's stream after its step.
+#include <cstring>
+#include <string>
+#include <vector>
+#include "aslb.h"
+#include "kernels.h"
+#include "lattice.cuh"
+
+namespace aslb {
+namespace {
+
+// Template vectors: d3q7, d3q15 and d3q19 list their vectors in the order of
+// the lattice tables (d3q7 is the first seven of d3q19). Coefficients by
+// vector class: rest, axis, diagonal.
+template <int Q>
+struct FdTemplate {
+  __host__ __device__ static constexpr int e(int i, int d) { return Q == 15 ? lat_c15(i, d) : lat_c27(i, d); }
+  __host__ __device__ static constexpr double lc(int i) {
+    return i == 0 ? (Q == 7 ? -6.0 : Q == 15 ? -14.0 / 3.0 : -4.0)
+                  : (i <= 6 ? (Q == 7 ? 1.0 : Q == 15 ? 2.0 / 3.0 : 1.0 / 3.0) : (Q == 15 ? 1.0 / 12.0 : 1.0 / 6.0));
+  }
+  __host__ __device__ static constexpr double gc(int i) {
+    return i == 0 ? 0.0
+                  : (i <= 6 ? (Q == 7 ? 0.5 : Q == 15 ? 1.0 / 3.0 : 1.0 / 6.0) : (Q == 15 ? 1.0 / 24.0 : 1.0 / 12.0));
+  }
+};
+
+struct FdGrid {
+  int nx, ny, nz, gx, gy, gz;
+  long long L;
+};
+
+// One interior cell per thread (z fastest), neighbours through L1/L2.
+template <int Q, class T>
+__global__ void __launch_bounds__(256) k_fd_step(const T* __restrict__ c, T* __restrict__ cn,
+                                                 const T* __restrict__ u, FdGrid g, T D, int cc) {
+  using Tp = FdTemplate<Q>;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int y = blockIdx.y + 1;
+  const int x = blockIdx.z + 1;
+  if (z > g.nz) return;
+  const long long a = ((long long)x * g.gy + y) * g.gz + z;
+  T cv[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) cv[i] = c[a + ((long long)Tp::e(i, 0) * g.gy + Tp::e(i, 1)) * g.gz + Tp::e(i, 2)];
+  T lap = T(0);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) lap += T(Tp::lc(i)) * cv[i];
+  T cnew = D * lap + cv[0];
+  if (u) {
+    T dp[3], dv[3];
+    T u0[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) u0[d] = u[d * g.L + a];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      T s = T(0), v = T(0);
+#pragma unroll
+      for (int i = 1; i < Q; ++i) {
+        if (Tp::e(i, d) == 0) continue;
+        const T ui = u[d * g.L + a + ((long long)Tp::e(i, 0) * g.gy + Tp::e(i, 1)) * g.gz + Tp::e(i, 2)];
+        const T coef = T(Tp::gc(i) * Tp::e(i, d));
+        s += T(0.5) * ((ui + u0[d]) * (cv[i] + cv[0])) * coef;
+        v += coef * ui;
+      }
+      dp[d] = s;
+      dv[d] = v;
+    }
+    cnew -= dp[0] + dp[1] + dp[2];
+    if (cc) {
+      cnew /= T(1) - (dv[0] + dv[1] + dv[2]);
+      cnew += lap * (u0[0] * u0[0] + u0[1] * u0[1] + u0[2] * u0[2]) * T(0.5);
+    }
+  }
+  cn[a] = cnew;
+}
+
+// Face ghost layers (cells of the face with interior tangential indices).
+template <class T>
+__global__ void k_fd_face_value(T* __restrict__ c, FdGrid g, int axis, int layer, T value) {
+  const int n1 = axis == 0 ? g.ny : g.nx, n2 = axis == 2 ? g.ny : g.nz;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n1 * n2) return;
+  const int i = t / n2 + 1, j = t % n2 + 1;
+  int x, y, z;
+  if (axis == 0) { x = layer; y = i; z = j; }
+  else if (axis == 1) { x = i; y = layer; z = j; }
+  else { x = i; y = j; z = layer; }
+  c[((long long)x * g.gy + y) * g.gz + z] = value;
+}
+
+}  // namespace
+}  // namespace aslb
+
+using namespace aslb;
+
+struct aslb_fd {
+  FdGrid g{};
+  int q = 7;
+  int dtype = ASLB_F32;
+  double D = 0;
+  void* c[2] = {nullptr, nullptr};
+  int cur = 0;
+  const void* u = nullptr;  // bound velocity field (device), or none
+  int cc = 0;
+  cudaStream_t stream = nullptr, own = nullptr;
+  aslb_lbgk* bound = nullptr;  // domain whose velocity and stream are used
+  long long steps = 0;
+};
+
+namespace aslb {
+// The bound domain is being destroyed: fall back to no velocity.
+void fd_detached(aslb_fd* f) {
+  f->u = nullptr;
+  f->stream = f->own;
+  f->cc = 0;
+  f->bound = nullptr;
+}
+}  // namespace aslb
+
+namespace {
+int fd_err(const char* what, cudaError_t e) {
+  set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return ASLB_ERR_CUDA;
+}
+int fd_arg(const char* what) {
+  set_last_error(std::string(what));
+  return ASLB_ERR_ARG;
+}
+size_t fd_elem(const aslb_fd* f) { return f->dtype == ASLB_F64 ? 8 : 4; }
+
+template <int Q, class T>
+cudaError_t fd_launch(aslb_fd* f) {
+  dim3 block(256), grid((f->g.nz + 255) / 256, f->g.ny, f->g.nx);
+  k_fd_step<Q, T><<<grid, block, 0, f->stream>>>((const T*)f->c[f->cur], (T*)f->c[1 - f->cur], (const T*)f->u, f->g,
+                                                T(f->D), f->cc);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t fd_step_t(aslb_fd* f) {
+  switch (f->q) {
+    case 7: return fd_launch<7, T>(f);
+    case 15: return fd_launch<15, T>(f);
+    case 19: return fd_launch<19, T>(f);
+  }
+  return cudaErrorInvalidValue;
+}
+}  // namespace
+
+extern "C" {
+
+int aslb_fd_create(int nx, int ny, int nz, int q, int dtype, double D, aslb_fd** out) {
+  if (!out) return fd_arg("aslb_fd_create: null argument");
+  *out = nullptr;
+  if (nx < 1 || ny < 1 || nz < 1) return fd_arg("aslb_fd_create: sizes must be positive");
+  if (q != 7 && q != 15 && q != 19) return fd_arg("aslb_fd_create: template must be d3q7, d3q15 or d3q19");
+  if (dtype != ASLB_F32 && dtype != ASLB_F64) return fd_arg("aslb_fd_create: dtype must be F32 or F64");
+  auto* f = new aslb_fd();
+  f->g = FdGrid{nx, ny, nz, nx + 2, ny + 2, nz + 2, (long long)(nx + 2) * (ny + 2) * (nz + 2)};
+  f->q = q;
+  f->dtype = dtype;
+  f->D = D;
+  cudaError_t e = cudaStreamCreateWithFlags(&f->own, cudaStreamNonBlocking);
+  f->stream = f->own;
+  for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+    e = cudaMalloc(&f->c[b], f->g.L * fd_elem(f));
+    if (e == cudaSuccess) e = cudaMemsetAsync(f->c[b], 0, f->g.L * fd_elem(f), f->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
+  if (e != cudaSuccess) {
+    aslb_fd_destroy(f);
+    return fd_err("aslb_fd_create", e);
+  }
+  *out = f;
+  return ASLB_OK;
+}
+
+int aslb_fd_set_velocity(aslb_fd* f, aslb_lbgk* h, int compressibility_correction) {
+  if (!f) return fd_arg("aslb_fd_set_velocity: null argument");
+  if (f->bound) {
+    cudaStreamSynchronize(f->stream);
+    lbgk_detach_fd(f->bound, f);
+    fd_detached(f);
+  }
+  if (!h) return ASLB_OK;
+  int n[3], storage;
+  void* u;
+  cudaStream_t st;
+  int r = lbgk_velocity_binding(h, n, &storage, &u, &st);
+  if (r) return r;
+  if (n[0] != f->g.nx || n[1] != f->g.ny || n[2] != f->g.nz)
+    return fd_arg("aslb_fd_set_velocity: the domain has another size");
+  if ((storage == ASLB_F64) != (f->dtype == ASLB_F64))
+    return fd_arg("aslb_fd_set_velocity: the velocity field is FP64 only for FP64 storage; match the FD dtype");
+  cudaStreamSynchronize(f->stream);
+  f->u = u;
+  f->stream = st;  // after the domain's step, in order
+  f->cc = compressibility_correction ? 1 : 0;
+  f->bound = h;
+  lbgk_attach_fd(h, f);
+  return ASLB_OK;
+}
+
+int aslb_fd_set_diffusion(aslb_fd* f, double D) {
+  if (!f) return fd_arg("aslb_fd_set_diffusion: null argument");
+  f->D = D;
+  return ASLB_OK;
+}
+
+int aslb_fd_write(aslb_fd* f, int dtype, const void* host) {
+  if (!f || !host || dtype != f->dtype) return fd_arg("aslb_fd_write: null argument or dtype differs from the FD's");
+  const size_t bytes = f->g.L * fd_elem(f);
+  cudaError_t e = cudaMemcpyAsync(f->c[0], host, bytes, cudaMemcpyHostToDevice, f->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(f->c[1], f->c[0], bytes, cudaMemcpyDeviceToDevice, f->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
+  if (e != cudaSuccess) return fd_err("aslb_fd_write", e);
+  f->cur = 0;
+  return ASLB_OK;
+}
+
+int aslb_fd_read(aslb_fd* f, int dtype, void* host) {
+  if (!f || !host || dtype != f->dtype) return fd_arg("aslb_fd_read: null argument or dtype differs from the FD's");
+  cudaError_t e = cudaMemcpyAsync(host, f->c[f->cur], f->g.L * fd_elem(f), cudaMemcpyDeviceToHost, f->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
+  if (e != cudaSuccess) return fd_err("aslb_fd_read", e);
+  return ASLB_OK;
+}
+
+int aslb_fd_set_face_value(aslb_fd* f, unsigned wallmask, double value) {
+  if (!f) return fd_arg("aslb_fd_set_face_value: null argument");
+  cudaError_t e = cudaSuccess;
+  for (int w = 0; w < 6 && e == cudaSuccess; ++w) {
+    if (!(wallmask >> w & 1u)) continue;
+    const int axis = w / 2;
+    const int n[3] = {f->g.nx, f->g.ny, f->g.nz};
+    const int layer = (w & 1) ? n[axis] + 1 : 0;
+    const int cnt = (axis == 0 ? f->g.ny * f->g.nz : axis == 1 ? f->g.nx * f->g.nz : f->g.nx * f->g.ny);
+    for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+      if (f->dtype == ASLB_F64)
+        k_fd_face_value<double><<<(cnt + 255) / 256, 256, 0, f->stream>>>((double*)f->c[b], f->g, axis, layer, value);
+      else
+        k_fd_face_value<float><<<(cnt + 255) / 256, 256, 0, f->stream>>>((float*)f->c[b], f->g, axis, layer,
+                                                                         (float)value);
+      e = cudaGetLastError();
+    }
+  }
+  if (e != cudaSuccess) return fd_err("aslb_fd_set_face_value", e);
+  return ASLB_OK;
+}
+
+int aslb_fd_step(aslb_fd* f, int n) {
+  if (!f || n < 0) return fd_arg("aslb_fd_step: null argument or negative count");
+  for (int s = 0; s < n; ++s) {
+    cudaError_t e = f->dtype == ASLB_F64 ? fd_step_t<double>(f) : fd_step_t<float>(f);
+    if (e != cudaSuccess) return fd_err("aslb_fd_step", e);
+    f->cur = 1 - f->cur;
+    f->steps++;
+  }
+  return ASLB_OK;
+}
+
+int aslb_fd_sync(aslb_fd* f) {
+  if (!f) return fd_arg("aslb_fd_sync: null argument");
+  cudaError_t e = cudaStreamSynchronize(f->stream);
+  if (e != cudaSuccess) return fd_err("aslb_fd_sync", e);
+  return ASLB_OK;
+}
+
+void* aslb_fd_device_field(aslb_fd* f) { return f ? f->c[f->cur] : nullptr; }
+
+int aslb_fd_destroy(aslb_fd* f) {
+  if (!f) return ASLB_OK;
+  if (f->stream) cudaStreamSynchronize(f->stream);
+  if (f->bound) lbgk_detach_fd(f->bound, f);
+  for (void* p : f->c)
+    if (p) cudaFree(p);
+  if (f->own) cudaStreamDestroy(f->own);
+  delete f;
+  return ASLB_OK;
+}
+
+}  // extern "C"

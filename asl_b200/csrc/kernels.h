@@ -5,12 +5,22 @@
 #include <string>
 #include "internal.cuh"
 
+struct aslb_lbgk;
+struct aslb_fd;
+
 namespace aslb {
 
 enum StorageKind { ST_F32 = 0, ST_F16 = 1, ST_F64 = 2 };
 
 // Message returned by aslb_last_error() on the calling thread.
 void set_last_error(const std::string& msg);
+// Velocity field of a domain for a coupled FD solver (fd.cu): interior
+// sizes, storage, device pointer (ASL layout, 3 L values) and stream. Fails
+// when the domain does not write its velocity every step.
+int lbgk_velocity_binding(aslb_lbgk* h, int n[3], int* storage, void** u, cudaStream_t* st);
+void lbgk_attach_fd(aslb_lbgk* h, aslb_fd* f);
+void lbgk_detach_fd(aslb_lbgk* h, aslb_fd* f);
+void fd_detached(aslb_fd* f);
 
 struct DomainDev {
   GridDesc g;

@@ -1,0 +1,94 @@
+"""FD advection-diffusion coupled to an LBGK velocity field (ASL's
+FDAdvectionDiffusion, src/num/aslFDAdvectionDiffusion.cxx:88-180, 209-226).
+
+``generateFDAdvectionDiffusion(c, D, v, vt, compressibilityCorrection)``
+builds the solver on the GPU (``aslb_fd_*``): ``c`` is the ghosted initial
+field (ASL layout, FP32 or FP64), ``v`` an LBGK whose velocity the solver
+reads on the device (or None), ``vt`` the stencil template (d3q7, d3q15 or
+d3q19). ``execute()`` advances one step on the LBGK's stream, after its
+steps; ``generateBCConstantValue(fd, value, walls)`` fixes face ghost
+layers (ghost values are never written by a step, as in ASL).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Iterable, Optional, Union
+
+import numpy as np
+
+from . import _lib as L
+from .lbgk import LBGK, VectorTemplate
+
+
+def _q(vt) -> int:
+    q = vt.q if isinstance(vt, VectorTemplate) else int(vt)
+    if q not in (7, 15, 19):
+        raise L.ASLError("ASL ERROR: FDAdvectionDiffusion: template must be d3q7, d3q15 or d3q19")
+    return q
+
+
+class FDAdvectionDiffusion:
+    def __init__(self, c: np.ndarray, D: float, vt: Union[VectorTemplate, int], velocity: Optional[LBGK] = None,
+                 compressibilityCorrection: bool = False):
+        self.lib = L.load()
+        c = np.asarray(c)
+        self.dtype = np.float64 if c.dtype == np.float64 else np.float32
+        self.code = L.F64 if self.dtype == np.float64 else L.F32
+        self.shape = c.shape
+        nx, ny, nz = (s - 2 for s in c.shape)
+        h = C.c_void_p()
+        L.check(self.lib.aslb_fd_create(nx, ny, nz, _q(vt), self.code, float(D), C.byref(h)), "FDAdvectionDiffusion")
+        self.h = h
+        self.velocity = velocity
+        self._c0 = np.ascontiguousarray(c, dtype=self.dtype)
+        if velocity is not None:
+            L.check(self.lib.aslb_fd_set_velocity(self.h, velocity.h, int(bool(compressibilityCorrection))),
+                    "FDAdvectionDiffusion::setVelocity")
+        self.setC(self._c0)
+
+    def init(self):
+        pass
+
+    def setC(self, c: np.ndarray):
+        c = np.ascontiguousarray(c, dtype=self.dtype)
+        if c.shape != self.shape:
+            raise L.ASLError("ASL ERROR: FDAdvectionDiffusion: field of another shape")
+        L.check(self.lib.aslb_fd_write(self.h, self.code, c.ctypes.data_as(C.c_void_p)), "FDAdvectionDiffusion")
+
+    def getC(self) -> np.ndarray:
+        out = np.empty(self.shape, dtype=self.dtype)
+        L.check(self.lib.aslb_fd_read(self.h, self.code, out.ctypes.data_as(C.c_void_p)), "FDAdvectionDiffusion")
+        return out
+
+    def setDiffusionCoefficient(self, D: float):
+        L.check(self.lib.aslb_fd_set_diffusion(self.h, float(D)), "FDAdvectionDiffusion")
+
+    def execute(self, n: int = 1):
+        L.check(self.lib.aslb_fd_step(self.h, int(n)), "FDAdvectionDiffusion::execute")
+
+    def sync(self):
+        L.check(self.lib.aslb_fd_sync(self.h), "FDAdvectionDiffusion")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.aslb_fd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def generateFDAdvectionDiffusion(c, D: float, v=None, vt=7, compressibilityCorrection: bool = False):
+    return FDAdvectionDiffusion(c, D, vt, v, compressibilityCorrection)
+
+
+def generateBCConstantValue(fd: FDAdvectionDiffusion, value: float, walls: Iterable):
+    """BCConstantValue on faces (src/num/aslBasicBC.cxx:51-57): the ghost
+    layers of the given faces hold ``value``."""
+    mask = 0
+    for w in walls:
+        mask |= 1 << int(w)
+    L.check(fd.lib.aslb_fd_set_face_value(fd.h, mask, float(value)), "generateBCConstantValue")

@@ -88,6 +88,7 @@ typedef struct aslb_lbgk aslb_lbgk;
 typedef struct aslb_bc aslb_bc;
 typedef struct aslb_force aslb_force;
 typedef struct aslb_force aslb_flux;
+typedef struct aslb_fd aslb_fd;
 typedef struct aslb_batch aslb_batch;
 
 /* Last error message of the calling thread ("" if none). */
@@ -374,6 +375,38 @@ int aslb_batch_destroy(aslb_batch* b);
 int aslb_geom_pack_spheres(int nx, int ny, int nz, double rmin, double rmax, double solid_fraction,
                            unsigned long long seed, int periodic_x, int attempts, int max_spheres, double* centers,
                            double* radii, int* count);
+
+/* ---- FD advection-diffusion coupled to the flow -------------------------- */
+
+/* generateFDAdvectionDiffusion(c, D, v, template[, compressibilityCorrection])
+ * (src/num/aslFDAdvectionDiffusion.cxx:88-180, 209-226), one component, no
+ * electric field: per interior cell
+ *   c' = D lap(c) + c - divProduct(v, c)
+ * and, with the correction, c' /= 1 - div(v); c' += lap(c) |v(x)|^2 / 2,
+ * with the template operators of src/math/aslTemplateVE.cxx:164-267 on
+ * q = 7, 15 or 19 (d3q7 / d3q15 / d3q19). c is an (nx+2)(ny+2)(nz+2) field
+ * in ASL layout (dtype ASLB_F32 or ASLB_F64); ghost values are never
+ * written by a step, so they act as fixed boundary values. */
+int aslb_fd_create(int nx, int ny, int nz, int q, int dtype, double D, aslb_fd** out);
+/* setVelocity(lbgk->getVelocity(), compressibilityCorrection): reads the
+ * domain's device velocity field and runs on the domain's stream (after its
+ * steps, in order). Same size; dtype ASLB_F64 for FP64 storage, ASLB_F32
+ * otherwise. NULL unbinds. Destroying the domain unbinds it. */
+int aslb_fd_set_velocity(aslb_fd* fd, aslb_lbgk* h, int compressibility_correction);
+int aslb_fd_set_diffusion(aslb_fd* fd, double D);
+/* Host copies of c (ghosted, L values of dtype); writing resets both buffers. */
+int aslb_fd_write(aslb_fd* fd, int dtype, const void* host_in);
+int aslb_fd_read(aslb_fd* fd, int dtype, void* host_out);
+/* generateBCConstantValue(c, value, {faces}) (src/num/aslBasicBC.cxx:51-57;
+ * faces as ASLB_WALL bits): the face ghost layers (interior tangential
+ * indices) hold value from now on. */
+int aslb_fd_set_face_value(aslb_fd* fd, unsigned wallmask, double value);
+/* execute() n times (asynchronous on the FD's stream). */
+int aslb_fd_step(aslb_fd* fd, int n);
+int aslb_fd_sync(aslb_fd* fd);
+/* Device pointer of the current c (valid until the next step). */
+void* aslb_fd_device_field(aslb_fd* fd);
+int aslb_fd_destroy(aslb_fd* fd);
 
 /* ---- surfaces (readSurface) -------------------------------------------- */
 
