@@ -45,35 +45,29 @@ struct FdGrid {
   long long L;
 };
 
-// One interior cell per thread (z fastest), neighbours through L1/L2.
-template <int Q, class T>
-__global__ void __launch_bounds__(256) k_fd_step(const T* __restrict__ c, T* __restrict__ cn,
-                                                 const T* __restrict__ u, FdGrid g, T D, int cc) {
+// The update of one cell from its stencil values: cv(i) = c(x + e_i),
+// uv(d, i) = u_d(x + e_i).
+template <int Q, class T, bool U, class CV, class UV>
+__device__ __forceinline__ T fd_cell(CV cvf, UV uvf, T D, int cc) {
   using Tp = FdTemplate<Q>;
-  const int z = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int y = blockIdx.y + 1;
-  const int x = blockIdx.z + 1;
-  if (z > g.nz) return;
-  const long long a = ((long long)x * g.gy + y) * g.gz + z;
   T cv[Q];
 #pragma unroll
-  for (int i = 0; i < Q; ++i) cv[i] = c[a + ((long long)Tp::e(i, 0) * g.gy + Tp::e(i, 1)) * g.gz + Tp::e(i, 2)];
+  for (int i = 0; i < Q; ++i) cv[i] = cvf(i);
   T lap = T(0);
 #pragma unroll
   for (int i = 0; i < Q; ++i) lap += T(Tp::lc(i)) * cv[i];
   T cnew = D * lap + cv[0];
-  if (u) {
-    T dp[3], dv[3];
-    T u0[3];
+  if (U) {
+    T dp[3], dv[3], u0[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) u0[d] = u[d * g.L + a];
+    for (int d = 0; d < 3; ++d) u0[d] = uvf(d, 0);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       T s = T(0), v = T(0);
 #pragma unroll
       for (int i = 1; i < Q; ++i) {
         if (Tp::e(i, d) == 0) continue;
-        const T ui = u[d * g.L + a + ((long long)Tp::e(i, 0) * g.gy + Tp::e(i, 1)) * g.gz + Tp::e(i, 2)];
+        const T ui = uvf(d, i);
         const T coef = T(Tp::gc(i) * Tp::e(i, d));
         s += T(0.5) * ((ui + u0[d]) * (cv[i] + cv[0])) * coef;
         v += coef * ui;
@@ -87,7 +81,77 @@ __global__ void __launch_bounds__(256) k_fd_step(const T* __restrict__ c, T* __r
       cnew += lap * (u0[0] * u0[0] + u0[1] * u0[1] + u0[2] * u0[2]) * T(0.5);
     }
   }
-  cn[a] = cnew;
+  return cnew;
+}
+
+// 2.5-D tiling: a block of 64 x 4 threads owns a 64 (z) x 4 (y) column of
+// cells and walks kFdPlanes x planes, keeping three planes of c (and u) with
+// a one-cell halo in shared memory, so every value is read from HBM about
+// once (the y/z halos of neighbouring tiles come from L2) and every
+// neighbour read of the stencil is a shared-memory load.
+constexpr int kFdTZ = 64, kFdTY = 4, kFdPlanes = 32;
+
+template <int Q, class T, bool U>
+__global__ void __launch_bounds__(kFdTZ * kFdTY) k_fd_step(const T* __restrict__ c, T* __restrict__ cn,
+                                                          const T* __restrict__ u, FdGrid g, T D, int cc) {
+  using Tp = FdTemplate<Q>;
+  constexpr int W = kFdTZ + 2, H = kFdTY + 2, P = W * H, NF = U ? 4 : 1;
+  __shared__ T sm[3][NF][P];
+  const int tz = threadIdx.x, ty = threadIdx.y, t = ty * kFdTZ + tz;
+  const int z0 = blockIdx.x * kFdTZ, y0 = blockIdx.y * kFdTY;  // ghosted origin of the tile
+  const int x0 = blockIdx.z * kFdPlanes + 1, x1 = min(g.nx, x0 + kFdPlanes - 1);
+  const int z = z0 + tz + 1, y = y0 + ty + 1;
+  const bool active = z <= g.nz && y <= g.ny;
+  // each thread owns tile entries t and t + 256 (P <= 512): a plane is
+  // fetched into registers one iteration ahead, so its HBM latency overlaps
+  // the arithmetic of the current plane
+  constexpr int NT = kFdTZ * kFdTY;
+  static_assert(P <= 2 * NT, "two tile entries per thread");
+  T r[2][NF];
+  auto fetch = [&](int xp) {
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int e = t + k * NT;
+      const int yy = y0 + e / W, zz = z0 + e % W;
+      if (e < P && yy < g.gy && zz < g.gz) {
+        const long long a = ((long long)xp * g.gy + yy) * g.gz + zz;
+        r[k][0] = c[a];
+        if (U) {
+          r[k][1 % NF] = u[a];
+          r[k][2 % NF] = u[g.L + a];
+          r[k][3 % NF] = u[2 * g.L + a];
+        }
+      }
+    }
+  };
+  auto stash = [&](int xp) {
+    const int slot = xp % 3;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int e = t + k * NT;
+      if (e < P)
+#pragma unroll
+        for (int f = 0; f < NF; ++f) sm[slot][f][e] = r[k][f];
+    }
+  };
+  fetch(x0 - 1);
+  stash(x0 - 1);
+  fetch(x0);
+  stash(x0);
+  fetch(x0 + 1);
+  for (int x = x0; x <= x1; ++x) {
+    stash(x + 1);  // into the slot plane x - 2 used; everyone passed the barrier below
+    __syncthreads();
+    if (x < x1) fetch(x + 2);
+    if (active) {
+      const int sl[3] = {(x + 2) % 3, x % 3, (x + 1) % 3};
+      const int base = (ty + 1) * W + tz + 1;
+      auto cvf = [&](int i) { return sm[sl[1 + Tp::e(i, 0)]][0][base + Tp::e(i, 1) * W + Tp::e(i, 2)]; };
+      auto uvf = [&](int d, int i) { return sm[sl[1 + Tp::e(i, 0)]][U ? 1 + d : 0][base + Tp::e(i, 1) * W + Tp::e(i, 2)]; };
+      cn[((long long)x * g.gy + y) * g.gz + z] = fd_cell<Q, T, U>(cvf, uvf, D, cc);
+    }
+    __syncthreads();
+  }
 }
 
 // Face ghost layers (cells of the face with interior tangential indices).
@@ -146,9 +210,14 @@ size_t fd_elem(const aslb_fd* f) { return f->dtype == ASLB_F64 ? 8 : 4; }
 
 template <int Q, class T>
 cudaError_t fd_launch(aslb_fd* f) {
-  dim3 block(256), grid((f->g.nz + 255) / 256, f->g.ny, f->g.nx);
-  k_fd_step<Q, T><<<grid, block, 0, f->stream>>>((const T*)f->c[f->cur], (T*)f->c[1 - f->cur], (const T*)f->u, f->g,
-                                                T(f->D), f->cc);
+  dim3 block(kFdTZ, kFdTY),
+      grid((f->g.nz + kFdTZ - 1) / kFdTZ, (f->g.ny + kFdTY - 1) / kFdTY, (f->g.nx + kFdPlanes - 1) / kFdPlanes);
+  const T* c = (const T*)f->c[f->cur];
+  T* cn = (T*)f->c[1 - f->cur];
+  if (f->u)
+    k_fd_step<Q, T, true><<<grid, block, 0, f->stream>>>(c, cn, (const T*)f->u, f->g, T(f->D), f->cc);
+  else
+    k_fd_step<Q, T, false><<<grid, block, 0, f->stream>>>(c, cn, nullptr, f->g, T(f->D), 0);
   return cudaGetLastError();
 }
 

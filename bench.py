@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--batch-steps", type=int, default=2000,
                     help="timed steps of the 256-domain batch (0: skip)")
     ap.add_argument("--batch-domains", type=int, default=256)
+    ap.add_argument("--fd-steps", type=int, default=100,
+                    help="steps of the FD advection-diffusion leg (0 skips it)")
     ap.add_argument("--closure-size", type=int, default=256,
                     help="coarse grid of the learned-closure study (fine = 2x; 0: skip)")
     return ap.parse_args()
@@ -291,6 +293,40 @@ def closure_run(n: int):
     return res
 
 
+def fd_run(W, w, steps: int, peak: float):
+    """FD advection-diffusion (aslb_fd) on the porous grid, reading the
+    velocity field of the FP32 domain on its stream: device time per step of
+    the FD kernel alone, d3q7 and d3q19 stencils. Algorithmic bytes per cell:
+    read c (4) and the three velocity components (12), write c (4)."""
+    import numpy as np
+    import torch
+    from asl_b200 import fd as FD
+    lb, bcs = W.build_lbgk(w, storage="f32", fuse=True)
+    lb.run(2, bcs)
+    lb.sync()
+    st = torch.cuda.ExternalStream(lb.stream)
+    g = tuple(s + 2 for s in w.size)
+    c = np.full(g, 0.5, dtype=np.float32)
+    out = {}
+    for q in (7, 19):
+        fd = FD.generateFDAdvectionDiffusion(c, 0.05, lb, q)
+        fd.execute(3)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fd.execute(steps)
+        e1.record(st)
+        e1.synchronize()
+        tk = e0.elapsed_time(e1) / 1e3 / steps
+        gbs = 20 * w.cells / tk / 1e9
+        out["d3q%d" % q] = {"kernel_ms": tk * 1e3, "value": w.cells / tk / 1e6, "unit": "MLUPS",
+                            "achieved_gbs": gbs, "frac_of_peak": gbs / peak, "steps": steps}
+        fd.close()
+    out["bytes_per_cell"] = 20
+    out["note"] = "k_fd_step, one interior cell per thread, FP32, velocity read from the LBGK's device field"
+    del lb, bcs
+    return out
+
+
 def batch_run(W, n: int, steps: int, peak: float):
     """Many small domains (seeded channels of random size, viscosity, obstacle
     and inlet velocity): the batch (one persistent stream-collide launch per
@@ -479,6 +515,9 @@ def run_ours(args):
     vehicle = None
     if world == 1 and args.q27_steps > 0:
         vehicle = vehicle_run(W, parse_size(args.q27_size), args.q27_steps, peak)
+    fdad = None
+    if world == 1 and args.fd_steps > 0:
+        fdad = fd_run(W, w, args.fd_steps, peak)
 
     bpc = BYTES_PER_CELL[(args.storage, w.q)]
     achieved = bpc * w.cells / tk / 1e9
@@ -509,6 +548,7 @@ def run_ours(args):
                 "gpu_launches": K * head["launches_per_step"],
                 "separate_conditions": sep, "tma_kernel": direct, "fp16": fp16, "accuracy": accuracy,
                 "d3q27_vehicle": vehicle, "batched_domains": batched, "learned_closure": learned,
+                "fd_advection_diffusion": fdad,
                 "finite": finite, "mass": mom[0]}
         print(json.dumps(line), flush=True)
     if world > 1:
