@@ -20,6 +20,7 @@ CLOSURE_NONE, CLOSURE_ASL_INTENT, CLOSURE_SMAGORINSKY, CLOSURE_MLP = 0, 1, 2, 3
 BC_NOSLIP, BC_VELOCITY, BC_PRESSURE, BC_PRESSURE_VELOCITY = 0, 1, 2, 3
 BC_MAP_NOSLIP, BC_MAP_VELOCITY, BC_MAP_VELOCITY_ROTATION, BC_MAP_PRESSURE_VELOCITY = 10, 11, 12, 13
 BC_MAP_TRANSPORT_DEPOSITION, BC_MAP_KINETICS_DEPOSITION = 14, 15
+BC_FIELD_NOSLIP_VEL, BC_FIELD_NOSLIP_RHO, BC_FIELD_VELOCITY_VEL, BC_FIELD_VELOCITY_VEL_ROTATION = 20, 21, 22, 23
 FIELD_RHO, FIELD_VELOCITY, FIELD_F, FIELD_CS2 = 0, 1, 2, 3
 
 
@@ -66,6 +67,7 @@ PROTOTYPES = {
     "aslb_lbgk_read": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "aslb_lbgk_write": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "aslb_bc_map_create_cd": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_double, _pd, _pd, _pd, _vp]),
+    "aslb_bc_field_create": (C.c_int, [_vp, C.c_int, _vp, _pd, _pd, _pd, _vp]),
     "aslb_bc_deposition_create": (C.c_int, [_vp, C.c_int, _vp, C.c_double, C.c_double, C.c_double, _vp]),
     "aslb_flux_create": (C.c_int, [_vp, _vp, _vp]),
     "aslb_flux_compute": (C.c_int, [_vp, _vp, _vp]),

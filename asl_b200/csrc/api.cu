@@ -113,6 +113,8 @@ struct aslb_bc {
   BcParams bp{};
   std::vector<int> host_links;     // host copies, kept for fusing
   std::vector<int4> host_anchors;
+  double* fweights = nullptr;      // field condition on rho: per-cell direction weights
+  bool field() const { return bp.kind >= BCK_FIELD_NOSLIP_VEL; }
 };
 
 struct aslb_force {
@@ -185,6 +187,11 @@ int do_step(aslb_lbgk* h) {
 
 int do_bc(aslb_bc* bc) {
   aslb_lbgk* h = bc->h;
+  if (bc->field()) {
+    cudaError_t e = launch_field_bc(h->d, bc->anchors, bc->n, bc->fweights, bc->bp, h->stream);
+    if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("field condition launch: ") + cudaGetErrorString(e));
+    return ASLB_OK;
+  }
   if (bc->fused) {
     // The condition takes effect inside the next steps (bounce-back reads).
     if (h->fresh) {
@@ -684,7 +691,7 @@ int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int us
   // A fused condition takes effect inside the next step, after every separate
   // condition of this step: it must be the last writer of its links.
   for (int b = 1; b < nbc; ++b)
-    if (bcs[b - 1]->fused && !bcs[b]->fused)
+    if (bcs[b - 1]->fused && !bcs[b]->fused && !bcs[b]->field())
       return fail(ASLB_ERR_ARG, "aslb_lbgk_run: fused conditions must come after all separate ones");
   auto eager = [&](int n) -> int {
     for (int i = 0; i < n; ++i) {
@@ -1088,6 +1095,84 @@ void map_candidates(const aslb_lbgk* h, const float* map, std::vector<Cand>& can
 }
 }  // namespace
 
+int aslb_bc_field_create(aslb_lbgk* h, int kind, const float* map, const double u[3], const double omega[3],
+                         const double center[3], aslb_bc** out) {
+  ASLB_CHECK_HANDLE(h);
+  if (!out || !map) return fail(ASLB_ERR_ARG, "aslb_bc_field_create: null argument");
+  *out = nullptr;
+  if (kind < ASLB_BC_FIELD_NOSLIP_VEL || kind > ASLB_BC_FIELD_VELOCITY_VEL_ROTATION)
+    return fail(ASLB_ERR_ARG, "aslb_bc_field_create: unknown field condition kind");
+  const int q = h->d.q;
+  if (q == 27)
+    return fail(ASLB_ERR_ARG,
+                "aslb_bc_field_create: ASL's d3q27 template has no laplacian or gradient coefficients");
+  const bool vel = kind == ASLB_BC_FIELD_NOSLIP_VEL || kind >= ASLB_BC_FIELD_VELOCITY_VEL;
+  if ((vel && !h->comp_vel) || (kind == ASLB_BC_FIELD_NOSLIP_RHO && !h->comp_rho))
+    return fail(ASLB_ERR_ARG, "aslb_bc_field_create: the domain does not write that output field");
+  const GridDesc& g = h->d.g;
+  // guard cells -0.9999 < map <= 0 (aslBasicBC.cxx:223-226, 343-346, 137-141);
+  // fluid neighbours map > 0, interior (the same restatement as the map conditions)
+  std::vector<int4> cells;
+  std::vector<double> wts;
+  const double gcax = q == 15 ? 1.0 / 3.0 : 1.0 / 6.0, gcdg = q == 15 ? 1.0 / 24.0 : 1.0 / 12.0;
+  for (int x = 0; x < g.gx; ++x)
+    for (int y = 0; y < g.gy; ++y)
+      for (int z = 0; z < g.gz; ++z) {
+        if (on_periodic_ghost(h, x, y, z)) continue;
+        const float m0 = map[aidx(g, x, y, z)];
+        if (!(m0 <= 0.f && m0 > -0.9999f)) continue;
+        unsigned mask = 0;
+        double nrm[3] = {0, 0, 0};
+        for (int k = 1; k < q; ++k) {
+          const int qx = wrapc(h, x + lattice_c(q, k, 0), 0), qy = wrapc(h, y + lattice_c(q, k, 1), 1),
+                    qz = wrapc(h, z + lattice_c(q, k, 2), 2);
+          const float mk = map_at(g, map, qx, qy, qz);
+          if (mk > 0.f && interior(g, qx, qy, qz)) mask |= 1u << k;
+          // map gradient with the template's gradient coefficients (aslTemplateVE.cxx:210-222)
+          const int n2 = lattice_c(q, k, 0) * lattice_c(q, k, 0) + lattice_c(q, k, 1) * lattice_c(q, k, 1) +
+                         lattice_c(q, k, 2) * lattice_c(q, k, 2);
+          const double gc = n2 == 1 ? gcax : gcdg;
+          for (int d = 0; d < 3; ++d) nrm[d] += gc * lattice_c(q, k, d) * (double)mk;
+        }
+        if (kind == ASLB_BC_FIELD_NOSLIP_RHO) {
+          const double len = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+          if (!(len > 0.0) || !mask) continue;  // no normal or no fluid neighbour: the value stays
+          std::vector<double> w(q, 0.0);
+          for (int k = 1; k < q; ++k) {
+            if (!(mask >> k & 1u)) continue;
+            const int c0 = lattice_c(q, k, 0), c1 = lattice_c(q, k, 1), c2 = lattice_c(q, k, 2);
+            const double cl = std::sqrt((double)(c0 * c0 + c1 * c1 + c2 * c2));
+            const double dc = (nrm[0] * c0 + nrm[1] * c1 + nrm[2] * c2) / len / cl + 1.0;
+            w[k] = dc * dc;
+          }
+          wts.insert(wts.end(), w.begin(), w.end());
+        }
+        cells.push_back(make_int4(x, y, z, (int)mask));
+      }
+  auto* bc = new aslb_bc();
+  bc->h = h;
+  bc->bp.kind = kind;
+  for (int d = 0; d < 3; ++d) {
+    bc->bp.u[d] = u ? u[d] : 0.0;
+    bc->bp.om[d] = omega ? omega[d] : 0.0;
+    bc->bp.cen[d] = center ? center[d] : 0.0;
+    bc->bp.pos0[d] = h->pos0[d];
+  }
+  bc->bp.dx = h->dx;
+  bc->n = (int)cells.size();
+  bc->links = bc->n;
+  int r = upload(&bc->anchors, cells);
+  if (!r && !wts.empty()) r = upload(&bc->fweights, wts);
+  if (r) {
+    aslb_bc_destroy(bc);
+    return r;
+  }
+  bc->host_anchors.swap(cells);
+  h->bcs.push_back(bc);
+  *out = bc;
+  return ASLB_OK;
+}
+
 int aslb_bc_deposition_create(aslb_lbgk* h, int kind, const float* map, double p0, double limiting_factor,
                               double beta, aslb_bc** out) {
   ASLB_CHECK_HANDLE(h);
@@ -1243,6 +1328,7 @@ int aslb_bc_destroy(aslb_bc* bc) {
   }
   cudaFree(bc->anchors);
   cudaFree(bc->dlinks);
+  cudaFree(bc->fweights);
   delete bc;
   return ASLB_OK;
 }
@@ -1651,7 +1737,9 @@ int aslb_batch_run(aslb_batch* b, int nsteps, aslb_bc* const* bcs, const int* nb
       if (c > 0 && bcs[total + c - 1]->fused && !bc->fused)
         return fail(ASLB_ERR_ARG, "aslb_batch_run: fused conditions must come after all separate ones");
       if (!bc->fused && bc->n > 0)
-        return fail(ASLB_ERR_ARG, "aslb_batch_run: velocity maps and links across periodic faces are not batched");
+        return fail(ASLB_ERR_ARG,
+                    "aslb_batch_run: per-cell conditions (velocity, deposition and field maps, links across periodic "
+                    "faces) are not batched");
     }
     total += nbc[i];
   }

@@ -156,6 +156,11 @@ enum BcKind {
   BCK_MAP_PRESSURE_VELOCITY = 13,
   BCK_MAP_TRANSPORT_DEPOSITION = 14,
   BCK_MAP_KINETICS_DEPOSITION = 15,
+  // conditions on the rho / u output fields (visualisation)
+  BCK_FIELD_NOSLIP_VEL = 20,
+  BCK_FIELD_NOSLIP_RHO = 21,
+  BCK_FIELD_VELOCITY_VEL = 22,
+  BCK_FIELD_VELOCITY_VEL_ROTATION = 23,
 };
 
 struct BcParams {

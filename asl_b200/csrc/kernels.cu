@@ -321,6 +321,91 @@ cudaError_t launch_bc(const DomainDev& d, const int4* anchors, int n, const BcPa
   ASLB_DISPATCH(d, bc_impl, d, anchors, n, bp, parity, st)
 }
 
+// Conditions on the output fields near a map (aslBasicBC.cxx:152-230, 300-350
+// through generateBCNoSlipVel / NoSlipRho / VelocityVel, aslLBGKBC.cxx:808-852).
+// Thread t takes guard cell t (x, y, z, mask of fluid-neighbour directions):
+//   NOSLIP_VEL   u(x) = sum_k LC_k (0 - u(x + c_k)) / max(sum_k LC_k, 0.01)
+//                (the middle-point value 0 between the cell and each fluid neighbour)
+//   NOSLIP_RHO   rho(x) = sum_k W_k rho(x + c_k) / sum_k W_k when sum_k W_k > 0.1,
+//                W_k = (n . c_k / |c_k| + 1)^2 from the map's unit normal n (the
+//                weights come precomputed per cell, wt[t * Q + k]; zero gradient)
+//   VELOCITY_VEL u(x) = v(position of x): constant, or omega x (r - center)
+// LC_k: laplacian coefficients of the lattice's template (D3Q15: 2/3 axis,
+// 1/12 diagonal; D3Q19: 1/3 axis, 1/6 diagonal).
+template <int Q, class S>
+__global__ void __launch_bounds__(256) k_field_bc(typename MacroT<S>::T* __restrict__ rho,
+                                                  typename MacroT<S>::T* __restrict__ u, const GridDesc g,
+                                                  const int4* __restrict__ cells, int n,
+                                                  const double* __restrict__ wt, const BcParams bp) {
+  using Lt = Lattice<Q>;
+  using M = typename MacroT<S>::T;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int4 an = cells[t];
+  const unsigned mask = (unsigned)an.w;
+  const bool px = g.periodic & 1, py = g.periodic & 2, pz = g.periodic & 4;
+  const long long a = aidx(g, an.x, an.y, an.z);
+  auto nb = [&](int k) {
+    return aidx(g, wrap_axis(an.x + Lt::c(k, 0), g.nx, px), wrap_axis(an.y + Lt::c(k, 1), g.ny, py),
+                wrap_axis(an.z + Lt::c(k, 2), g.nz, pz));
+  };
+  if (bp.kind == BCK_FIELD_NOSLIP_VEL) {
+    M v[3] = {M(0), M(0), M(0)}, counter = M(0);
+#pragma unroll
+    for (int k = 1; k < Q; ++k) {
+      if (!(mask >> k & 1u)) continue;
+      const M lc = M(Lt::norm2(k) == 1 ? (Q == 15 ? 2.0 / 3.0 : 1.0 / 3.0) : (Q == 15 ? 1.0 / 12.0 : 1.0 / 6.0));
+      const long long q = nb(k);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) v[d] += (M(0) - u[d * g.L + q]) * lc;
+      counter += lc;
+    }
+    const M c = counter > M(0.01) ? counter : M(0.01);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) u[d * g.L + a] = v[d] / c;
+  } else if (bp.kind == BCK_FIELD_NOSLIP_RHO) {
+    M s = M(0), counter = M(0);
+#pragma unroll
+    for (int k = 1; k < Q; ++k) {
+      if (!(mask >> k & 1u)) continue;
+      const M w = M(wt[(size_t)t * Q + k]);
+      s += rho[nb(k)] * w;
+      counter += w;
+    }
+    if (counter > M(0.1)) rho[a] = s / counter;
+  } else {
+    M v[3] = {M(bp.u[0]), M(bp.u[1]), M(bp.u[2])};
+    if (bp.kind == BCK_FIELD_VELOCITY_VEL_ROTATION) {
+      const double r0 = bp.pos0[0] + (an.x - 1) * bp.dx - bp.cen[0];
+      const double r1 = bp.pos0[1] + (an.y - 1) * bp.dx - bp.cen[1];
+      const double r2 = bp.pos0[2] + (an.z - 1) * bp.dx - bp.cen[2];
+      v[0] = M(bp.om[1] * r2 - bp.om[2] * r1);
+      v[1] = M(bp.om[2] * r0 - bp.om[0] * r2);
+      v[2] = M(bp.om[0] * r1 - bp.om[1] * r0);
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) u[d * g.L + a] = v[d];
+  }
+}
+
+template <int Q, class S>
+static cudaError_t field_bc_impl(const DomainDev& d, const int4* cells, int n, const double* wt, const BcParams& bp,
+                                 cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  if constexpr (Q == 27) {
+    return cudaErrorNotSupported;
+  } else {
+    using M = typename MacroT<S>::T;
+    k_field_bc<Q, S><<<(n + 255) / 256, 256, 0, st>>>((M*)d.rho, (M*)d.u, d.g, cells, n, wt, bp);
+    return cudaGetLastError();
+  }
+}
+
+cudaError_t launch_field_bc(const DomainDev& d, const int4* cells, int n, const double* wt, const BcParams& bp,
+                            cudaStream_t st) {
+  ASLB_DISPATCH(d, field_bc_impl, d, cells, n, wt, bp, st)
+}
+
 // Direction-sorted links: thread t handles link t, whose direction k comes from
 // the segment table (warp-uniform except at segment ends). IN and OUT slots as
 // above; the fluid end is anchor + off[k].

@@ -48,6 +48,10 @@ cudaError_t launch_init_f(const DomainDev& d, const StepParams& p, double rho0, 
 cudaError_t launch_export_f(const DomainDev& d, const StepParams& p, int parity, void* out, cudaStream_t st);
 cudaError_t launch_import_f(const DomainDev& d, const StepParams& p, const void* in, cudaStream_t st);
 // Boundary links: anchors (x, y, z, direction mask) in ghosted coordinates.
+// Conditions on the rho / u output fields (visualisation): guard cells with
+// their fluid-neighbour masks, per-cell weights for the rho condition.
+cudaError_t launch_field_bc(const DomainDev& d, const int4* cells, int n, const double* wt, const BcParams& bp,
+                            cudaStream_t st);
 cudaError_t launch_bc(const DomainDev& d, const int4* anchors, int n, const BcParams& bp, int parity,
                       cudaStream_t st);
 // Direction-sorted links (one thread per link), the common case of every

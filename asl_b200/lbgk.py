@@ -461,6 +461,36 @@ def generateBCVelocity(lbgk: LBGK, velocity, m, computationalDomain=None) -> BC:
     return _map_bc(lbgk, L.BC_MAP_VELOCITY, m, u=velocity, cdomain=computationalDomain)
 
 
+def _field_bc(lbgk: LBGK, kind: int, m, u=(0.0, 0.0, 0.0), omega=(0.0, 0.0, 0.0), center=(0.0, 0.0, 0.0)) -> BC:
+    arr = _map_array(lbgk, m)
+    h = C.c_void_p()
+    L.check(lbgk.lib.aslb_bc_field_create(lbgk.h, kind, arr.ctypes.data_as(L._pf), L.dvec(u), L.dvec(omega),
+                                          L.dvec(center), C.byref(h)), "generateBC")
+    return BC(lbgk, h)
+
+
+def generateBCNoSlipVel(lbgk: LBGK, m) -> BC:
+    """Velocity output zero at the map surface, for visualisation
+    (src/num/aslLBGKBC.cxx:808-816: BCConstantValueMiddlePointMap on u)."""
+    return _field_bc(lbgk, L.BC_FIELD_NOSLIP_VEL, m)
+
+
+def generateBCNoSlipRho(lbgk: LBGK, m) -> BC:
+    """Zero normal gradient of the density output at the map surface
+    (src/num/aslLBGKBC.cxx:819-827: BCConstantGradientMap on rho)."""
+    return _field_bc(lbgk, L.BC_FIELD_NOSLIP_RHO, m)
+
+
+def generateBCVelocityVel(lbgk: LBGK, velocity, m) -> BC:
+    """Velocity output set to a position function on the map's guard cells
+    (src/num/aslLBGKBC.cxx:847-852: BCValuePFMap on u)."""
+    if isinstance(velocity, PFRotationField):
+        return _field_bc(lbgk, L.BC_FIELD_VELOCITY_VEL_ROTATION, m, omega=velocity.omega, center=velocity.center)
+    if isinstance(velocity, PFConstant):
+        velocity = velocity.value
+    return _field_bc(lbgk, L.BC_FIELD_VELOCITY_VEL, m, u=velocity)
+
+
 def _deposition_bc(lbgk: LBGK, kind: int, m, p0: float, lf: float, beta: float) -> BC:
     arr = _map_array(lbgk, m)
     h = C.c_void_p()

@@ -73,6 +73,10 @@ extern "C" {
 #define ASLB_BC_MAP_PRESSURE_VELOCITY 13
 #define ASLB_BC_MAP_TRANSPORT_DEPOSITION 14
 #define ASLB_BC_MAP_KINETICS_DEPOSITION 15
+#define ASLB_BC_FIELD_NOSLIP_VEL 20
+#define ASLB_BC_FIELD_NOSLIP_RHO 21
+#define ASLB_BC_FIELD_VELOCITY_VEL 22
+#define ASLB_BC_FIELD_VELOCITY_VEL_ROTATION 23
 
 /* walls for slice BCs: bit w for asl::SlicesNames {X0,XE,Y0,YE,Z0,ZE}
  * (src/num/aslBCond.h:309) */
@@ -241,6 +245,19 @@ int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const
  * (src/num/aslLBGKBC.cxx:273-282, 837-844; src/num/aslBCond.cxx:204-211). */
 int aslb_bc_map_create_cd(aslb_lbgk* h, int kind, const float* map, const float* cdomain, double p, const double u[3],
                           const double omega[3], const double center[3], aslb_bc** out);
+/* Conditions on the output fields near a map, for visualisation
+ * (generateBCNoSlipVel / generateBCNoSlipRho / generateBCVelocityVel,
+ * src/num/aslLBGKBC.cxx:808-852 -> src/num/aslBasicBC.cxx:110-230, 300-350),
+ * on guard cells -0.9999 < map <= 0 of the domain's velocity / density
+ * fields (the domain must write them): FIELD_NOSLIP_VEL sets u to the
+ * middle-point zero value (laplacian-weighted 2*0 - u of fluid neighbours);
+ * FIELD_NOSLIP_RHO gives rho a zero normal gradient (neighbours weighted by
+ * (n . c/|c| + 1)^2, n the map's unit normal); FIELD_VELOCITY_VEL(_ROTATION)
+ * sets u = v (constant u, or omega x (r - center)). Executed like any
+ * condition, after the step that wrote the fields. D3Q15 and D3Q19 only
+ * (ASL's d3q27 template has no laplacian or gradient coefficients). */
+int aslb_bc_field_create(aslb_lbgk* h, int kind, const float* map, const double u[3], const double omega[3],
+                         const double center[3], aslb_bc** out);
 /* Deposition on a map surface (generateBCTransportLimitedDeposition(nm, p0,
  * limitingFactor, map) and generateBCKineticsLimitedDeposition(nm, p0,
  * limitingFactor, beta, map) in the argument order of their definitions,

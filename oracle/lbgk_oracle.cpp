@@ -29,6 +29,9 @@
 //   src/num/aslLBGKBC.cxx:440-598              deposition map BCs (transport
 //                                              and kinetics limited)
 //   src/num/aslLBGKBC.cxx:623-665              ComputeSurfaceFluxMap
+//   src/num/aslLBGKBC.cxx:808-852 and           output-field conditions for
+//   src/num/aslBasicBC.cxx:110-230, 300-350     visualisation (NoSlipVel/Rho,
+//                                              VelocityVel)
 //   src/num/aslLBGKBC.cxx:691-736              ComputeSurfaceForceMap
 //   src/acl/aclMath/aclVectorOfElementsOperations.cxx:249-258
 //                                              component-sequential `+=`
@@ -108,6 +111,10 @@ enum BcKind {
   MAP_PRESSURE_VELOCITY = 13,
   MAP_TRANSPORT_DEPOSITION = 14,
   MAP_KINETICS_DEPOSITION = 15,
+  FIELD_NOSLIP_VEL = 20,
+  FIELD_NOSLIP_RHO = 21,
+  FIELD_VELOCITY_VEL = 22,
+  FIELD_VELOCITY_VEL_ROTATION = 23,
 };
 
 struct Bc {
@@ -122,6 +129,8 @@ struct Bc {
   // Map: cells passing the guard with their fluid-neighbour mask.
   std::vector<long> cells;
   std::vector<uint32_t> masks;
+  // Output-field conditions: per-cell direction weights (rho), q per cell.
+  std::vector<double> wts;
 };
 
 template <class T>
@@ -574,6 +583,99 @@ double flux(Sim<T>& s, const float* map, float* field) {
   return tot;
 }
 
+// Output-field conditions (aslBasicBC.cxx): guard cells -0.9999 < map <= 0,
+// fluid neighbours map > 0 and interior. NoSlipVel: u = sum LC_k (2*0 - u_nb) /
+// max(sum LC_k, 0.01) (BCConstantValueMiddlePointMap, :171-230). NoSlipRho:
+// rho = sum W_k rho_nb / sum W_k if sum W_k > 0.1, W_k = (n . c_k/|c_k| + 1)^2,
+// n the unit map gradient with the template's gradient coefficients
+// (BCConstantGradientMap, :300-350). VelocityVel: u = v(position) (BCValuePFMap,
+// :123-145). Template coefficients of d3q15 / d3q19 (aslTemplates.cxx:146-185).
+template <class T>
+void build_field(Sim<T>& s, Bc& bc, const float* map) {
+  const Lattice& lat = s.lat;
+  const double gcax = lat.q == 15 ? 1.0 / 3.0 : 1.0 / 6.0, gcdg = lat.q == 15 ? 1.0 / 24.0 : 1.0 / 12.0;
+  for (int x = 0; x < s.G[0]; ++x)
+    for (int y = 0; y < s.G[1]; ++y)
+      for (int z = 0; z < s.G[2]; ++z) {
+        if ((s.periodic[0] && (x < 1 || x > s.N[0])) || (s.periodic[1] && (y < 1 || y > s.N[1])) ||
+            (s.periodic[2] && (z < 1 || z > s.N[2])))
+          continue;
+        float m0 = map[s.idx(x, y, z)];
+        if (!(m0 <= 0.f && m0 > -0.9999f)) continue;
+        uint32_t mask = 0;
+        double n[3] = {0, 0, 0};
+        for (int k = 1; k < lat.q; ++k) {
+          int q[3] = {s.wrapc(x + lat.c[k][0], 0), s.wrapc(y + lat.c[k][1], 1), s.wrapc(z + lat.c[k][2], 2)};
+          double mk = map_at(s, map, q[0], q[1], q[2]);
+          if (mk > 0.0 && s.interior(q[0], q[1], q[2])) mask |= 1u << k;
+          int n2 = lat.c[k][0] * lat.c[k][0] + lat.c[k][1] * lat.c[k][1] + lat.c[k][2] * lat.c[k][2];
+          for (int d = 0; d < 3; ++d) n[d] += (n2 == 1 ? gcax : gcdg) * lat.c[k][d] * mk;
+        }
+        if (bc.kind == FIELD_NOSLIP_RHO) {
+          double len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+          if (!(len > 0.0) || !mask) continue;
+          for (int k = 0; k < lat.q; ++k) {
+            double w = 0;
+            if (k > 0 && (mask >> k & 1u)) {
+              double cl = std::sqrt(double(lat.c[k][0] * lat.c[k][0] + lat.c[k][1] * lat.c[k][1] +
+                                           lat.c[k][2] * lat.c[k][2]));
+              double dc = (n[0] * lat.c[k][0] + n[1] * lat.c[k][1] + n[2] * lat.c[k][2]) / len / cl + 1.0;
+              w = dc * dc;
+            }
+            bc.wts.push_back(w);
+          }
+        }
+        bc.cells.push_back(s.idx(x, y, z));
+        bc.masks.push_back(mask);
+      }
+}
+
+template <class T>
+void field_execute(Sim<T>& s, Bc& bc) {
+  const Lattice& lat = s.lat;
+  const long L = s.L;
+  for (size_t t = 0; t < bc.cells.size(); ++t) {
+    long cell = bc.cells[t];
+    uint32_t mask = bc.masks[t];
+    int x, y, z;
+    decode(s, cell, x, y, z);
+    auto nb = [&](int k) {
+      return s.idx(s.wrapc(x + lat.c[k][0], 0), s.wrapc(y + lat.c[k][1], 1), s.wrapc(z + lat.c[k][2], 2));
+    };
+    if (bc.kind == FIELD_NOSLIP_VEL) {
+      T v[3] = {T(0), T(0), T(0)}, counter = T(0);
+      for (int k = 1; k < lat.q; ++k) {
+        if (!(mask >> k & 1u)) continue;
+        int n2 = lat.c[k][0] * lat.c[k][0] + lat.c[k][1] * lat.c[k][1] + lat.c[k][2] * lat.c[k][2];
+        T lc = T(n2 == 1 ? (lat.q == 15 ? 2.0 / 3.0 : 1.0 / 3.0) : (lat.q == 15 ? 1.0 / 12.0 : 1.0 / 6.0));
+        for (int d = 0; d < 3; ++d) v[d] += (T(0) - s.u[d * L + nb(k)]) * lc;
+        counter += lc;
+      }
+      T c = counter > T(0.01) ? counter : T(0.01);
+      for (int d = 0; d < 3; ++d) s.u[d * L + cell] = v[d] / c;
+    } else if (bc.kind == FIELD_NOSLIP_RHO) {
+      T sum = T(0), counter = T(0);
+      for (int k = 1; k < lat.q; ++k) {
+        if (!(mask >> k & 1u)) continue;
+        T w = T(bc.wts[t * lat.q + k]);
+        sum += s.rho[nb(k)] * w;
+        counter += w;
+      }
+      if (counter > T(0.1)) s.rho[cell] = sum / counter;
+    } else {
+      T v[3] = {T(bc.u[0]), T(bc.u[1]), T(bc.u[2])};
+      if (bc.kind == FIELD_VELOCITY_VEL_ROTATION) {
+        double r[3] = {s.pos0[0] + (x - 1) * s.dx - bc.cen[0], s.pos0[1] + (y - 1) * s.dx - bc.cen[1],
+                       s.pos0[2] + (z - 1) * s.dx - bc.cen[2]};
+        v[0] = T(bc.om[1] * r[2] - bc.om[2] * r[1]);
+        v[1] = T(bc.om[2] * r[0] - bc.om[0] * r[2]);
+        v[2] = T(bc.om[0] * r[1] - bc.om[1] * r[0]);
+      }
+      for (int d = 0; d < 3; ++d) s.u[d * L + cell] = v[d];
+    }
+  }
+}
+
 extern "C" {
 
 // flags: bit0 no velocity output, bit1 no density output, bit2 incompressible,
@@ -719,7 +821,31 @@ long orc_bc_size(void* p, int id) {
 
 void orc_bc_execute(void* p, int id) {
   auto* h = (Handle*)p;
-  DISPATCH(h, bc_execute(S, S.bcs[id]));
+  DISPATCH(h, {
+    if (S.bcs[id].kind >= FIELD_NOSLIP_VEL)
+      field_execute(S, S.bcs[id]);
+    else
+      bc_execute(S, S.bcs[id]);
+  });
+}
+
+int orc_bc_field(void* p, int kind, const float* map, const double* u, const double* om, const double* cen) {
+  auto* h = (Handle*)p;
+  int id = -1;
+  DISPATCH(h, {
+    Bc bc;
+    bc.kind = kind;
+    bc.p = 0;
+    for (int d = 0; d < 3; ++d) {
+      bc.u[d] = u ? u[d] : 0.0;
+      bc.om[d] = om ? om[d] : 0.0;
+      bc.cen[d] = cen ? cen[d] : 0.0;
+    }
+    build_field(S, bc, map);
+    S.bcs.push_back(std::move(bc));
+    id = (int)S.bcs.size() - 1;
+  });
+  return id;
 }
 
 void orc_force(void* p, const float* map, float* field, const double* r0, double* out6) {

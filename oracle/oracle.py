@@ -63,6 +63,7 @@ def load():
             "orc_force": (None, [vp, pf, pf, pd, pd]),
             "orc_bc_deposition": (C.c_int, [vp, C.c_int, pf, d, d, d]),
             "orc_bc_map_cd": (C.c_int, [vp, C.c_int, pf, pf, d, pd, pd, pd]),
+            "orc_bc_field": (C.c_int, [vp, C.c_int, pf, pd, pd, pd]),
             "orc_flux": (C.c_double, [vp, pf, pf]),
             "orc_size": (C.c_long, [vp]),
             "orc_get_f": (None, [vp, pd]),
@@ -160,6 +161,11 @@ class Oracle:
 
     def bc_size(self, bid) -> int:
         return int(self.lib.orc_bc_size(self.h, int(bid)))
+
+    def bc_field(self, kind, m, u=(0.0, 0.0, 0.0), omega=(0.0, 0.0, 0.0), center=(0.0, 0.0, 0.0)) -> int:
+        mm = np.ascontiguousarray(m, dtype=np.float32)
+        uu, om, ce = (np.asarray(v, dtype=np.float64) for v in (u, omega, center))
+        return self.lib.orc_bc_field(self.h, int(kind), _fp(mm), _dp(uu), _dp(om), _dp(ce))
 
     def bc_deposition(self, kind, m, p0, lf, beta=0.0) -> int:
         mm = np.ascontiguousarray(m, dtype=np.float32)

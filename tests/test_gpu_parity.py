@@ -561,3 +561,54 @@ def test_velocity_map_with_computational_domain(gpu, oracle_mod, field):
             for i in ids:
                 o.bc_execute(i)
         assert np.abs(lb.getF()[I4] - o.get_f()[I4]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("kind", [20, 21, 22, 23])
+@pytest.mark.parametrize("storage,prec,tol", [("f64", 8, 1e-12), ("f32", 4, 1e-5)])
+def test_output_field_conditions_match_oracle(gpu, oracle_mod, kind, storage, prec, tol):
+    """generateBCNoSlipVel / NoSlipRho / VelocityVel on the density and
+    velocity outputs after each step, behind a fused no-slip map (field
+    conditions may follow fused ones: they touch no population)."""
+    size = (16, 12, 10)
+    g = tuple(s + 2 for s in size)
+    rho, u = smooth_field(g, 60 + kind, amp=0.02)
+    m = sphere_map(g, (7.5, 5.5, 4.5), 2.4)
+    lb = A.LBGK(A.Block(size), 0.03, A.d3q19(), storage=storage)
+    A.LBGKUtilities(lb).initF(rho, u)
+    nos = A.generateBCNoSlip(lb, m)
+    walls = A.generateBCNoSlip(lb, [A.X0, A.XE, A.Y0, A.YE, A.Z0, A.ZE])
+    kw = {}
+    if kind == 20:
+        fb = A.generateBCNoSlipVel(lb, m)
+    elif kind == 21:
+        fb = A.generateBCNoSlipRho(lb, m)
+    elif kind == 22:
+        fb = A.generateBCVelocityVel(lb, A.generatePFConstant((0.01, -0.02, 0.03)), m)
+        kw = dict(u=(0.01, -0.02, 0.03))
+    else:
+        fb = A.generateBCVelocityVel(lb, A.generatePFRotationField((0.0, 0.02, 0.01), (7.5, 5.5, 4.5)), m)
+        kw = dict(omega=(0.0, 0.02, 0.01), center=(7.5, 5.5, 4.5))
+    nos.fuse()
+    bcs = [walls, nos, fb]
+    o = oracle_mod.Oracle(size, 19, prec, 0.03)
+    o.init_f_fields(rho, u)
+    ids = [o.bc_slice(0, 63), o.bc_map(10, m), o.bc_field(kind, m, **kw)]
+    for n in (3, 4):
+        lb.run(n, bcs)
+        for _ in range(n):
+            o.step(1)
+            for i in ids:
+                o.bc_execute(i)
+        guard = (m <= 0) & (m > -0.9999)
+        assert np.abs(lb.getRho()[guard] - o.get_rho()[guard]).max() <= tol
+        assert np.abs(lb.getVelocity()[:, guard] - o.get_u()[:, guard]).max() <= tol
+        inner = np.zeros(g, dtype=bool)
+        inner[1:-1, 1:-1, 1:-1] = True
+        assert np.abs(lb.getVelocity()[:, inner] - o.get_u()[:, inner]).max() <= tol
+
+
+def test_output_field_conditions_reject_d3q27(gpu):
+    lb = A.LBGK(A.Block((8, 8, 8)), 0.03, A.d3q27())
+    m = np.ones((10, 10, 10), dtype=np.float32)
+    with pytest.raises(A.L.ASLError, match="d3q27"):
+        A.generateBCNoSlipVel(lb, m)

@@ -305,3 +305,88 @@ def test_single_cell_collide_by_hand(oracle_mod):
         cm = sum(c[i][d] * m[d] for d in range(3))
         feq = rho + 3 * cm + 4.5 * cm * cm / rho - 1.5 * mm / rho
         assert abs(got[i] - ((1 - om) * f0[i] + om * feq)) < 1e-14
+
+
+def _field_expect(kind, q, m, rho, u, lat, size, omega=None, center=None, U=None):
+    """Independent numpy restatement of the output-field conditions."""
+    c, w, inv = lat
+    g = m.shape
+    rho2, u2 = rho.copy(), u.copy()
+    axis_lc, diag_lc = (2 / 3, 1 / 12) if q == 15 else (1 / 3, 1 / 6)
+    axis_gc, diag_gc = (1 / 3, 1 / 24) if q == 15 else (1 / 6, 1 / 12)
+
+    def mat(p):
+        return m[p] if all(0 <= p[a] < g[a] for a in range(3)) else np.float32(-0.9)
+    for x in np.ndindex(*g):
+        if not (m[x] <= 0 and m[x] > np.float32(-0.9999)):
+            continue
+        nbs = [(k, tuple(x[a] + c[k][a] for a in range(3))) for k in range(1, q)]
+        fluid = [(k, p) for k, p in nbs if all(1 <= p[a] <= size[a] for a in range(3)) and mat(p) > 0]
+        if kind == 20:
+            lc = {k: (axis_lc if (np.abs(c[k]).sum() == 1) else diag_lc) for k, _ in fluid}
+            cnt = sum(lc.values())
+            for d in range(3):
+                u2[(d,) + x] = sum((0 - u[(d,) + p]) * lc[k] for k, p in fluid) / max(cnt, 0.01)
+        elif kind == 21:
+            n = sum((axis_gc if np.abs(c[k]).sum() == 1 else diag_gc) * np.asarray(c[k], float) * mat(p)
+                    for k, p in nbs)
+            ln = np.linalg.norm(n)
+            if ln == 0 or not fluid:
+                continue
+            ws = {k: ((n @ c[k]) / ln / np.linalg.norm(c[k]) + 1) ** 2 for k, _ in fluid}
+            if sum(ws.values()) > 0.1:
+                rho2[x] = sum(rho[p] * ws[k] for k, p in fluid) / sum(ws.values())
+        elif kind == 22:
+            u2[(slice(None),) + x] = U
+        else:
+            r = np.asarray(x, float) - 1 - np.asarray(center, float)
+            u2[(slice(None),) + x] = np.cross(np.asarray(omega, float), r)
+    return rho2, u2
+
+
+@pytest.mark.parametrize("q", [15, 19])
+@pytest.mark.parametrize("kind", [20, 21, 22, 23])
+def test_oracle_output_field_conditions(oracle_mod, q, kind):
+    size = (9, 8, 7)
+    g = tuple(s + 2 for s in size)
+    rho, u = _smooth_field(g, 50 + kind, amp=0.03)
+    pos = np.stack(np.meshgrid(*[np.arange(n) - 1.0 for n in g], indexing="ij"))
+    m = np.clip((np.sqrt(((pos - np.array([4.0, 3.5, 3.0]).reshape(3, 1, 1, 1)) ** 2).sum(0)) - 2.1) / 1.8,
+                -1, 1).astype(np.float32)
+    o = oracle_mod.Oracle(size, q, 8, 0.03)
+    o.init_f_fields(rho, u)
+    kw = {}
+    if kind == 22:
+        kw = dict(u=(0.01, -0.02, 0.03))
+    if kind == 23:
+        kw = dict(omega=(0.0, 0.02, 0.01), center=(4.0, 3.5, 3.0))
+    bid = o.bc_field(kind, m, **kw)
+    rho0, u0 = o.get_rho(), o.get_u()
+    o.bc_execute(bid)
+    want_rho, want_u = _field_expect(kind, q, m, rho0, u0, oracle_mod.lattice(q), size,
+                                     omega=kw.get("omega"), center=kw.get("center"), U=kw.get("u"))
+    assert np.allclose(o.get_rho(), want_rho, rtol=0, atol=1e-14)
+    assert np.allclose(o.get_u(), want_u, rtol=0, atol=1e-14)
+    assert not (np.array_equal(o.get_rho(), rho0) and np.array_equal(o.get_u(), u0))
+
+
+def test_oracle_noslip_vel_known_answer(oracle_mod):
+    """A uniform flow U around the guard cells: the middle-point condition
+    sets u = -U there (the mean of cell and neighbour vanishes)."""
+    size = (8, 8, 8)
+    g = tuple(s + 2 for s in size)
+    pos = np.stack(np.meshgrid(*[np.arange(n) - 1.0 for n in g], indexing="ij"))
+    m = np.clip((np.sqrt(((pos - 3.5) ** 2).sum(0)) - 2.0) / 1.8, -1, 1).astype(np.float32)
+    U = np.array([0.02, 0.01, -0.03])
+    o = oracle_mod.Oracle(size, 19, 8, 0.03)
+    o.init_f(1.0, U)
+    bid = o.bc_field(20, m)
+    o.bc_execute(bid)
+    got = o.get_u()
+    guard = (m <= 0) & (m > -0.9999)
+    with_fluid = guard & (m > -0.6)  # guard cells next to fluid (the deepest ones have no fluid neighbour)
+    assert with_fluid.any()
+    for d in range(3):
+        vals = got[d][guard]
+        assert np.all((np.abs(vals + U[d]) < 1e-15) | (vals == 0.0))
+        assert np.allclose(got[d][with_fluid & (np.abs(got[0]) > 0)], -U[d], atol=1e-15)
