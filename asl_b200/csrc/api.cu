@@ -1095,6 +1095,16 @@ void map_candidates(const aslb_lbgk* h, const float* map, std::vector<Cand>& can
 }
 }  // namespace
 
+int aslb_lattice(int q, int* c, double* w, int* inv) {
+  if ((q != 15 && q != 19 && q != 27) || !c || !w || !inv) return fail(ASLB_ERR_ARG, "aslb_lattice: bad arguments");
+  for (int i = 0; i < q; ++i) {
+    for (int d = 0; d < 3; ++d) c[3 * i + d] = lattice_c(q, i, d);
+    w[i] = q == 15 ? Lattice<15>::w(i) : q == 19 ? Lattice<19>::w(i) : Lattice<27>::w(i);
+    inv[i] = lattice_inv(q, i);
+  }
+  return ASLB_OK;
+}
+
 int aslb_bc_field_create(aslb_lbgk* h, int kind, const float* map, const double u[3], const double omega[3],
                          const double center[3], aslb_bc** out) {
   ASLB_CHECK_HANDLE(h);

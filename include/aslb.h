@@ -245,6 +245,11 @@ int aslb_bc_map_create(aslb_lbgk* h, int kind, const float* map, double p, const
  * (src/num/aslLBGKBC.cxx:273-282, 837-844; src/num/aslBCond.cxx:204-211). */
 int aslb_bc_map_create_cd(aslb_lbgk* h, int kind, const float* map, const float* cdomain, double p, const double u[3],
                           const double omega[3], const double center[3], aslb_bc** out);
+/* The velocity set the kernels use (host copy, no device needed):
+ * VectorTemplate::vectors, quasiparticlesCoefs and invertVectors of d3q15 /
+ * d3q19 / d3q27 (src/math/aslTemplates.cxx:30-83, 146-200; D3Q27 with the
+ * standard weights, the reference's d3q27 has none). c: 3q ints, w: q, inv: q. */
+int aslb_lattice(int q, int* c, double* w, int* inv);
 /* Conditions on the output fields near a map, for visualisation
  * (generateBCNoSlipVel / generateBCNoSlipRho / generateBCVelocityVel,
  * src/num/aslLBGKBC.cxx:808-852 -> src/num/aslBasicBC.cxx:110-230, 300-350),
