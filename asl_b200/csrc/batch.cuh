@@ -43,17 +43,33 @@ __global__ void __launch_bounds__(256, BLOCKS)
     S* F = (S*)D.F;
     const uint2* mask = D.mask;
     const C om0 = std::is_same<C, double>::value ? C(D.om0d) : C(D.om0f);
-    for (unsigned l = threadIdx.x; l < plane_cells; l += 256u) {
+    // storage index of plane cell l (y rows of nz cells, z fastest)
+    auto cell_index = [&](unsigned l, int& y, int& z) {
       unsigned yq = __umulhi(l, nz_inv);
       if (yq * nz > l) --yq;  // exact quotient for l < 2^32 / nz
-      const int y = (int)yq + 1;
-      const int z = (int)(l - yq * nz) + 1;
-      const unsigned s = (unsigned)sidx(g, x, y, z);
+      y = (int)yq + 1;
+      z = (int)(l - yq * nz) + 1;
+      return (unsigned)sidx(g, x, y, z);
+    };
+    // the fused-link words of a thread's next cell are loaded one iteration
+    // ahead: the population addresses depend on them, so they must not cost
+    // a second memory round trip
+    uint2 mnext = make_uint2(0u, 0u);
+    if (FUSED && mask && threadIdx.x < plane_cells) {
+      int y1, z1;
+      mnext = mask[cell_index(threadIdx.x, y1, z1)];
+    }
+    for (unsigned l = threadIdx.x; l < plane_cells; l += 256u) {
+      int y, z;
+      const unsigned s = cell_index(l, y, z);
       uint32_t bounce = 0, elide = 0;
       if (FUSED && mask) {
-        const uint2 m = mask[s];
-        bounce = m.x;
-        elide = m.y;
+        bounce = mnext.x;
+        elide = mnext.y;
+        if (l + 256u < plane_cells) {
+          int y1, z1;
+          mnext = mask[cell_index(l + 256u, y1, z1)];
+        }
       }
       int ox[3], oy[3], oz[3];
       nb_offsets(g, x, y, z, ox, oy, oz);
