@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kTmaThreads, TmaOccupancy<S, CL>::blocks)
     const int rg = tile / sh.nseg, seg = tile % sh.nseg;
     const int row = rg * sh.rows + lr;
     const int z = 1 + seg * sh.tz + lz;
-    const bool valid = row < g.nx * g.ny && z <= g.nz;
+    const bool valid = lr < sh.rows && row < g.nx * g.ny && z <= g.nz;
     const int x = valid ? row / g.ny + 1 : 1, y = valid ? row % g.ny + 1 : 1;
 
     C f[Q];
@@ -214,8 +214,10 @@ __global__ void __launch_bounds__(kTmaThreads, TmaOccupancy<S, CL>::blocks)
 template <int Q, class S>
 inline TmaShape tma_shape(const GridDesc& g, bool fused, int blocks_per_sm) {
   TmaShape sh{};
-  int tz = ((g.nz + 31) / 32) * 32;
-  if (tz > 256) tz = 256;
+  // tz divides the 256 consumer threads (32, 64, 128 or 256), so that rows * tz
+  // is exactly 256 and no consumer thread maps past the tile's staged rows
+  int tz = 32;
+  while (tz < g.nz && tz < 256) tz *= 2;
   sh.tz = tz;
   sh.rows = 256 / tz;
   sh.nseg = (g.nz + tz - 1) / tz;

@@ -342,7 +342,9 @@ def test_destroy_domain_before_its_conditions(gpu):
 @pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
 @pytest.mark.parametrize("shape,periodic", [((6, 5, 300), (True, True, True)),    # two z segments, z wrap
                                             ((9, 7, 40), (False, True, True)),    # 4 rows per tile, partial group
-                                            ((5, 3, 17), (True, False, False))])  # short rows
+                                            ((5, 3, 17), (True, False, False)),   # short rows
+                                            ((4, 3, 192), (False, True, False)),  # rows of 192: 256-cell segments
+                                            ((4, 5, 96), (True, False, True))])   # rows of 96, z wrap
 def test_kernel_variants_bitwise_equal(gpu, q, storage, shape, periodic):
     g = tuple(s + 2 for s in shape)
     rho, u = smooth_field(g, 3 + q)
