@@ -79,6 +79,10 @@ PROTOTYPES = {
     "aslb_fd_write": (C.c_int, [_vp, C.c_int, _vp]),
     "aslb_fd_read": (C.c_int, [_vp, C.c_int, _vp]),
     "aslb_fd_set_face_value": (C.c_int, [_vp, C.c_uint, C.c_double]),
+    "aslb_fd_bc_create": (C.c_int, [_vp, C.c_int, _vp, C.c_double, _vp]),
+    "aslb_fd_bc_execute": (C.c_int, [_vp]),
+    "aslb_fd_bc_cells": (C.c_longlong, [_vp]),
+    "aslb_fd_bc_destroy": (C.c_int, [_vp]),
     "aslb_fd_step": (C.c_int, [_vp, C.c_int]),
     "aslb_fd_sync": (C.c_int, [_vp]),
     "aslb_fd_device_field": (_vp, [_vp]),

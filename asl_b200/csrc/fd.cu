@@ -14,6 +14,8 @@
 // boundary values (BCConstantValue on faces, src/num/aslBasicBC.cxx:51-57).
 // The velocity is the bound LBGK's device velocity field (ASL layout, FP32,
 // FP64 for FP64 storage), read on that domain's stream after its step.
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -168,10 +170,42 @@ __global__ void k_fd_face_value(T* __restrict__ c, FdGrid g, int axis, int layer
   c[((long long)x * g.gy + y) * g.gz + z] = value;
 }
 
+// Conditions on c at a map (aslBasicBC.cxx:71-108, 271-350), thread t per
+// guard cell (x, y, z, mask of fluid-neighbour directions of the template):
+//   VALUE     c(x) = value
+//   GRADIENT  c(x) = sum_k W_k (c(x + e_k) - (n . e_k / |e_k|) value) / sum_k W_k
+//             when sum_k W_k > 0.1; W_k = (n . e_k / |e_k| + 1)^2 and
+//             n . e_k / |e_k| precomputed per cell and direction (wt, nd).
+template <int Q, class T>
+__global__ void k_fd_map_bc(T* __restrict__ c, FdGrid g, const int4* __restrict__ cells, int n,
+                            const double* __restrict__ wt, const double* __restrict__ nd, int gradient, T value) {
+  using Tp = FdTemplate<Q>;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int4 an = cells[t];
+  const long long a = ((long long)an.x * g.gy + an.y) * g.gz + an.z;
+  if (!gradient) {
+    c[a] = value;
+    return;
+  }
+  T sum = T(0), counter = T(0);
+#pragma unroll
+  for (int k = 1; k < Q; ++k) {
+    if (!((unsigned)an.w >> k & 1u)) continue;
+    const long long q = ((long long)(an.x + Tp::e(k, 0)) * g.gy + an.y + Tp::e(k, 1)) * g.gz + an.z + Tp::e(k, 2);
+    const T w = T(wt[(size_t)t * Q + k]);
+    sum += (c[q] - T(nd[(size_t)t * Q + k]) * value) * w;
+    counter += w;
+  }
+  if (counter > T(0.1)) c[a] = sum / counter;
+}
+
 }  // namespace
 }  // namespace aslb
 
 using namespace aslb;
+
+struct aslb_fd_bc;
 
 struct aslb_fd {
   FdGrid g{};
@@ -185,6 +219,17 @@ struct aslb_fd {
   cudaStream_t stream = nullptr, own = nullptr;
   aslb_lbgk* bound = nullptr;  // domain whose velocity and stream are used
   long long steps = 0;
+  std::vector<aslb_fd_bc*> bcs;  // map conditions on c (detached on destroy)
+};
+
+struct aslb_fd_bc {
+  aslb_fd* fd = nullptr;
+  int gradient = 0;
+  double value = 0;
+  int n = 0;
+  int4* cells = nullptr;
+  double* wt = nullptr;
+  double* nd = nullptr;
 };
 
 namespace aslb {
@@ -353,10 +398,127 @@ int aslb_fd_sync(aslb_fd* f) {
 
 void* aslb_fd_device_field(aslb_fd* f) { return f ? f->c[f->cur] : nullptr; }
 
+int aslb_fd_bc_create(aslb_fd* f, int kind, const float* map, double value, aslb_fd_bc** out) {
+  if (!f || !map || !out) return fd_arg("aslb_fd_bc_create: null argument");
+  *out = nullptr;
+  if (kind != ASLB_FD_BC_VALUE_MAP && kind != ASLB_FD_BC_GRADIENT_MAP)
+    return fd_arg("aslb_fd_bc_create: kind must be ASLB_FD_BC_VALUE_MAP or ASLB_FD_BC_GRADIENT_MAP");
+  const FdGrid& g = f->g;
+  const int q = f->q;
+  auto e = [&](int k, int d) { return q == 15 ? lat_c15(k, d) : lat_c27(k, d); };
+  auto gc = [&](int k) {
+    return q == 7 ? FdTemplate<7>::gc(k) : q == 15 ? FdTemplate<15>::gc(k) : FdTemplate<19>::gc(k);
+  };
+  auto mat = [&](int x, int y, int z) -> double {  // the map, -0.9 off the grid (generateDCFullSafe)
+    if (x < 0 || y < 0 || z < 0 || x >= g.gx || y >= g.gy || z >= g.gz) return -0.9;
+    return map[((long long)x * g.gy + y) * g.gz + z];
+  };
+  std::vector<int4> cells;
+  std::vector<double> wt, nd;
+  for (int x = 0; x < g.gx; ++x)
+    for (int y = 0; y < g.gy; ++y)
+      for (int z = 0; z < g.gz; ++z) {
+        const float m0 = map[((long long)x * g.gy + y) * g.gz + z];
+        if (!(m0 <= 0.f && m0 > -0.9999f)) continue;
+        unsigned mask = 0;
+        double nrm[3] = {0, 0, 0};
+        for (int k = 1; k < q; ++k) {
+          const int qx = x + e(k, 0), qy = y + e(k, 1), qz = z + e(k, 2);
+          const double mk = mat(qx, qy, qz);
+          const bool in = qx >= 1 && qx <= g.nx && qy >= 1 && qy <= g.ny && qz >= 1 && qz <= g.nz;
+          if (mk > 0.0 && in) mask |= 1u << k;
+          for (int d = 0; d < 3; ++d) nrm[d] += gc(k) * e(k, d) * (float)mk;
+        }
+        if (kind == ASLB_FD_BC_GRADIENT_MAP) {
+          const double len = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+          if (!(len > 0.0) || !mask) continue;  // no normal or no fluid neighbour: c stays
+          for (int k = 0; k < q; ++k) {
+            double w = 0, dn = 0;
+            if (k > 0 && (mask >> k & 1u)) {
+              const double cl = std::sqrt((double)(e(k, 0) * e(k, 0) + e(k, 1) * e(k, 1) + e(k, 2) * e(k, 2)));
+              dn = (nrm[0] * e(k, 0) + nrm[1] * e(k, 1) + nrm[2] * e(k, 2)) / len / cl;
+              w = (dn + 1.0) * (dn + 1.0);
+            }
+            wt.push_back(w);
+            nd.push_back(dn);
+          }
+        }
+        cells.push_back(make_int4(x, y, z, (int)mask));
+      }
+  auto* b = new aslb_fd_bc();
+  b->fd = f;
+  b->gradient = kind == ASLB_FD_BC_GRADIENT_MAP;
+  b->value = value;
+  b->n = (int)cells.size();
+  cudaError_t err = cudaSuccess;
+  if (b->n) {
+    err = cudaMalloc((void**)&b->cells, cells.size() * sizeof(int4));
+    if (err == cudaSuccess)
+      err = cudaMemcpy(b->cells, cells.data(), cells.size() * sizeof(int4), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess && !wt.empty()) {
+      err = cudaMalloc((void**)&b->wt, wt.size() * sizeof(double));
+      if (err == cudaSuccess) err = cudaMalloc((void**)&b->nd, nd.size() * sizeof(double));
+      if (err == cudaSuccess) err = cudaMemcpy(b->wt, wt.data(), wt.size() * sizeof(double), cudaMemcpyHostToDevice);
+      if (err == cudaSuccess) err = cudaMemcpy(b->nd, nd.data(), nd.size() * sizeof(double), cudaMemcpyHostToDevice);
+    }
+  }
+  if (err != cudaSuccess) {
+    aslb_fd_bc_destroy(b);
+    return fd_err("aslb_fd_bc_create", err);
+  }
+  f->bcs.push_back(b);
+  *out = b;
+  return ASLB_OK;
+}
+
+int aslb_fd_bc_execute(aslb_fd_bc* b) {
+  if (!b) return fd_arg("aslb_fd_bc_execute: null argument");
+  if (!b->fd) {
+    set_last_error("aslb_fd_bc_execute: its FD solver was destroyed");
+    return ASLB_ERR_STATE;
+  }
+  aslb_fd* f = b->fd;
+  if (!b->n) return ASLB_OK;
+  const unsigned blocks = (unsigned)((b->n + 255) / 256);
+  const int q = f->q;
+  if (f->dtype == ASLB_F64) {
+    double* c = (double*)f->c[f->cur];
+    if (q == 7) k_fd_map_bc<7, double><<<blocks, 256, 0, f->stream>>>(c, f->g, b->cells, b->n, b->wt, b->nd, b->gradient, b->value);
+    else if (q == 15) k_fd_map_bc<15, double><<<blocks, 256, 0, f->stream>>>(c, f->g, b->cells, b->n, b->wt, b->nd, b->gradient, b->value);
+    else k_fd_map_bc<19, double><<<blocks, 256, 0, f->stream>>>(c, f->g, b->cells, b->n, b->wt, b->nd, b->gradient, b->value);
+  } else {
+    float* c = (float*)f->c[f->cur];
+    const float v = (float)b->value;
+    if (q == 7) k_fd_map_bc<7, float><<<blocks, 256, 0, f->stream>>>(c, f->g, b->cells, b->n, b->wt, b->nd, b->gradient, v);
+    else if (q == 15) k_fd_map_bc<15, float><<<blocks, 256, 0, f->stream>>>(c, f->g, b->cells, b->n, b->wt, b->nd, b->gradient, v);
+    else k_fd_map_bc<19, float><<<blocks, 256, 0, f->stream>>>(c, f->g, b->cells, b->n, b->wt, b->nd, b->gradient, v);
+  }
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return fd_err("aslb_fd_bc_execute", err);
+  return ASLB_OK;
+}
+
+long long aslb_fd_bc_cells(aslb_fd_bc* b) { return b ? b->n : -1; }
+
+int aslb_fd_bc_destroy(aslb_fd_bc* b) {
+  if (!b) return ASLB_OK;
+  if (b->fd) {
+    cudaStreamSynchronize(b->fd->stream);
+    auto& v = b->fd->bcs;
+    v.erase(std::remove(v.begin(), v.end(), b), v.end());
+  }
+  cudaFree(b->cells);
+  cudaFree(b->wt);
+  cudaFree(b->nd);
+  delete b;
+  return ASLB_OK;
+}
+
 int aslb_fd_destroy(aslb_fd* f) {
   if (!f) return ASLB_OK;
   if (f->stream) cudaStreamSynchronize(f->stream);
   if (f->bound) lbgk_detach_fd(f->bound, f);
+  for (aslb_fd_bc* b : f->bcs) b->fd = nullptr;
   for (void* p : f->c)
     if (p) cudaFree(p);
   if (f->own) cudaStreamDestroy(f->own);

@@ -85,10 +85,53 @@ def generateFDAdvectionDiffusion(c, D: float, v=None, vt=7, compressibilityCorre
     return FDAdvectionDiffusion(c, D, vt, v, compressibilityCorrection)
 
 
-def generateBCConstantValue(fd: FDAdvectionDiffusion, value: float, walls: Iterable):
+class FDMapBC:
+    """A condition on the FD field at a map surface; ``execute()`` after each
+    FD step, as ASL's executeAll(bc)."""
+
+    def __init__(self, fd: FDAdvectionDiffusion, kind: int, m: np.ndarray, value: float):
+        m = np.ascontiguousarray(m, dtype=np.float32)
+        if m.shape != fd.shape:
+            raise L.ASLError("ASL ERROR: map must cover the FD field's ghosted block")
+        self.fd = fd
+        h = C.c_void_p()
+        L.check(fd.lib.aslb_fd_bc_create(fd.h, kind, m.ctypes.data_as(C.c_void_p), float(value), C.byref(h)),
+                "generateBC")
+        self.h = h
+
+    def init(self):
+        pass
+
+    def execute(self):
+        L.check(self.fd.lib.aslb_fd_bc_execute(self.h), "BC::execute")
+
+    @property
+    def cells(self) -> int:
+        return int(self.fd.lib.aslb_fd_bc_cells(self.h))
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.fd.lib.aslb_fd_bc_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def generateBCConstantValue(fd: FDAdvectionDiffusion, value: float, where):
     """BCConstantValue on faces (src/num/aslBasicBC.cxx:51-57): the ghost
-    layers of the given faces hold ``value``."""
+    layers of the given faces hold ``value`` (applied at once, never
+    overwritten by a step); on a map (BCConstantValueMap, :71-108) a
+    condition object whose ``execute()`` sets the guard cells to ``value``."""
+    if isinstance(where, np.ndarray):
+        return FDMapBC(fd, 0, where, value)
     mask = 0
-    for w in walls:
+    for w in where:
         mask |= 1 << int(w)
     L.check(fd.lib.aslb_fd_set_face_value(fd.h, mask, float(value)), "generateBCConstantValue")
+
+
+def generateBCConstantGradient(fd: FDAdvectionDiffusion, value: float, m: np.ndarray) -> FDMapBC:
+    """BCConstantGradientMap (src/num/aslBasicBC.cxx:271-350) on the FD's
+    template: the guard cells take the normal gradient ``value``."""
+    return FDMapBC(fd, 1, m, value)

@@ -93,6 +93,7 @@ typedef struct aslb_bc aslb_bc;
 typedef struct aslb_force aslb_force;
 typedef struct aslb_force aslb_flux;
 typedef struct aslb_fd aslb_fd;
+typedef struct aslb_fd_bc aslb_fd_bc;
 typedef struct aslb_batch aslb_batch;
 
 /* Last error message of the calling thread ("" if none). */
@@ -423,6 +424,21 @@ int aslb_fd_read(aslb_fd* fd, int dtype, void* host_out);
  * faces as ASLB_WALL bits): the face ghost layers (interior tangential
  * indices) hold value from now on. */
 int aslb_fd_set_face_value(aslb_fd* fd, unsigned wallmask, double value);
+/* Conditions on c at a map surface, executed like ASL's (after each FD step,
+ * asynchronous on the FD's stream), on guard cells -0.9999 < map <= 0 (map:
+ * host floats in the FD's ghosted layout): ASLB_FD_BC_VALUE_MAP sets
+ * c = value (generateBCConstantValue(c, v, map): BCConstantValueMap,
+ * src/num/aslBasicBC.cxx:71-108); ASLB_FD_BC_GRADIENT_MAP sets a normal
+ * gradient `value` (generateBCConstantGradient(c, v, map, template):
+ * BCConstantGradientMap, :271-350): c = sum_k W_k (c(x + e_k) - (n.e_k/|e_k|)
+ * value) / sum_k W_k over fluid neighbours (map > 0, interior) of the FD's
+ * template, W_k = (n.e_k/|e_k| + 1)^2, n the unit map gradient. */
+#define ASLB_FD_BC_VALUE_MAP 0
+#define ASLB_FD_BC_GRADIENT_MAP 1
+int aslb_fd_bc_create(aslb_fd* fd, int kind, const float* map, double value, aslb_fd_bc** out);
+int aslb_fd_bc_execute(aslb_fd_bc* bc);
+long long aslb_fd_bc_cells(aslb_fd_bc* bc);
+int aslb_fd_bc_destroy(aslb_fd_bc* bc);
 /* execute() n times (asynchronous on the FD's stream). */
 int aslb_fd_step(aslb_fd* fd, int n);
 int aslb_fd_sync(aslb_fd* fd);

@@ -74,3 +74,40 @@ def fd_step(c: np.ndarray, D: float, q: int, u: np.ndarray | None = None, cc: bo
     out = c.copy()
     out[1:-1, 1:-1, 1:-1] = cnew
     return out
+
+
+def fd_map_bc(c: np.ndarray, m: np.ndarray, q: int, gradient: bool, value: float) -> np.ndarray:
+    """BCConstantValueMap / BCConstantGradientMap (src/num/aslBasicBC.cxx:71-108,
+    271-350) on the guard cells -0.9999 < m <= 0: value, or the normal
+    gradient ``value`` from fluid neighbours (m > 0, interior) of the
+    template, weighted by (n.e/|e| + 1)^2 with n the unit map gradient
+    (template gradient coefficients; m is -0.9 off the grid)."""
+    T = c.dtype.type
+    e, _, gc = template(q)
+    g = c.shape
+    out = c.copy()
+
+    def mat(p):
+        return float(m[p]) if all(0 <= p[a] < g[a] for a in range(3)) else -0.9
+    for x in np.ndindex(*g):
+        if not (m[x] <= 0 and m[x] > np.float32(-0.9999)):
+            continue
+        if not gradient:
+            out[x] = T(value)
+            continue
+        nbs = [(k, tuple(x[a] + int(e[k][a]) for a in range(3))) for k in range(1, q)]
+        n = sum(gc[k] * e[k].astype(float) * float(np.float32(mat(p))) for k, p in nbs)
+        ln = np.linalg.norm(n)
+        fluid = [(k, p) for k, p in nbs if all(1 <= p[a] <= g[a] - 2 for a in range(3)) and mat(p) > 0]
+        if ln == 0 or not fluid:
+            continue
+        s = T(0)
+        cnt = T(0)
+        for k, p in fluid:
+            dn = (n @ e[k]) / ln / np.linalg.norm(e[k])
+            w = T((dn + 1) ** 2)
+            s = s + (c[p] - T(dn) * T(value)) * w
+            cnt = cnt + w
+        if cnt > T(0.1):
+            out[x] = s / cnt
+    return out

@@ -39,3 +39,24 @@ def test_diffusion_conserves_mass_away_from_faces(oracle_mod):
     for _ in range(5):
         c = fd_step(c, 0.1, 19)
     assert abs(c.sum() - m0) < 1e-10 * m0  # summation rounding only
+
+
+def test_map_conditions_known_answers(oracle_mod):
+    """A flat wall (solid for x <= 3.5): the zero-gradient condition copies
+    the fluid neighbours' value when they agree; a gradient condition shifts
+    it by the normal component; the value condition sets the guard cells."""
+    from oracle.fd_oracle import fd_map_bc
+    g = (10, 8, 8)
+    x = np.arange(g[0], dtype=float)[:, None, None] * np.ones(g)
+    m = np.clip((x - 3.5) / 1.8, -1, 1).astype(np.float32)   # normal +x
+    c = np.full(g, 0.4)
+    guard = (m <= 0) & (m > -0.9999)
+    out = fd_map_bc(c, m, 7, True, 0.0)
+    has_fluid = guard & (x == 3)
+    assert np.allclose(out[has_fluid & (np.arange(g[1])[None, :, None] > 0) & (np.arange(g[1])[None, :, None] < g[1] - 1)
+                           & (np.arange(g[2])[None, None, :] > 0) & (np.arange(g[2])[None, None, :] < g[2] - 1)], 0.4)
+    # d3q7: the only fluid neighbour of x = 3 is x = 4 (n . e = 1, W = 4): c = c(4) - value
+    out = fd_map_bc(c, m, 7, True, 0.1)
+    assert np.allclose(out[3, 1:-1, 1:-1], 0.3)
+    out = fd_map_bc(c, m, 19, False, 0.9)
+    assert np.all(out[guard] == 0.9) and np.all(out[~guard] == 0.4)

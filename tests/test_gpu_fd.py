@@ -74,3 +74,31 @@ def test_unbind_on_domain_destroy_and_errors(gpu):
     got = fd.getC()
     assert np.isfinite(got).all() and got.shape == c.shape
     assert np.abs(got - ref).max() > 0  # the first two steps saw the flow
+
+
+@pytest.mark.parametrize("q", [7, 19])
+@pytest.mark.parametrize("kind", ["value", "gradient"])
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-13), (np.float32, 5e-6)])
+def test_map_conditions_match_oracle(gpu, q, kind, dtype, tol):
+    """FD steps coupled to the cylinder flow, each followed by a value or
+    normal-gradient condition on the cylinder map (the multicomponent-flow
+    pattern: lbgk step, FD step, executeAll(bc))."""
+    from oracle.fd_oracle import fd_map_bc
+    w = W.channel_cylinder(size=(20, 12, 10), radius=2.5, center=(7.0, 6.0), u_in=0.04)
+    storage = "f64" if dtype == np.float64 else "f32"
+    lb, bcs = W.build_lbgk(w, storage)
+    c = blob(tuple(s + 2 for s in w.size), dtype)
+    fd = FD.generateFDAdvectionDiffusion(c, 0.05, lb, q)
+    if kind == "value":
+        fb = FD.generateBCConstantValue(fd, 0.3, w.map)
+    else:
+        fb = FD.generateBCConstantGradient(fd, 0.02, w.map)
+    assert fb.cells > 0
+    ref = fd.getC()
+    for _ in range(4):
+        lb.run(1, bcs)
+        fd.execute()
+        fb.execute()
+        u = lb.getVelocity(dtype)
+        ref = fd_map_bc(fd_step(ref, 0.05, q, u), w.map, q, kind == "gradient", 0.02 if kind == "gradient" else 0.3)
+    assert np.abs(fd.getC() - ref).max() <= tol
