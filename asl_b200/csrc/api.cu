@@ -6,6 +6,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <nvtx3/nvToolsExt.h>
 #include "aslb.h"
 #include "kernels.h"
 #include "mlp.cuh"
@@ -32,6 +33,14 @@ void aslb::set_last_error(const std::string& msg) { g_err = msg; }
 
 #define ASLB_CHECK_HANDLE(h) \
   if (!(h)) return fail(ASLB_ERR_ARG, std::string(__func__) + ": null handle")
+
+// A named range on the profiler timeline (NVTX) for the duration of a call:
+// nsys / ncu show the library's steps, conditions and batches by name. Without
+// a tool attached the push and pop return at once.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 struct aslb_lbgk {
   DomainDev d{};
@@ -674,6 +683,7 @@ int aslb_lbgk_init_f_fields(aslb_lbgk* h, const double* rho, const double* u) {
 }
 
 int aslb_lbgk_step(aslb_lbgk* h, int nsteps) {
+  NvtxRange range("aslb_lbgk_step");
   ASLB_CHECK_HANDLE(h);
   if (nsteps < 0) return fail(ASLB_ERR_ARG, "aslb_lbgk_step: negative step count");
   for (int i = 0; i < nsteps; ++i) {
@@ -684,6 +694,7 @@ int aslb_lbgk_step(aslb_lbgk* h, int nsteps) {
 }
 
 int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int use_graph) {
+  NvtxRange range("aslb_lbgk_run");
   ASLB_CHECK_HANDLE(h);
   if (nsteps < 0 || nbc < 0 || (nbc > 0 && !bcs)) return fail(ASLB_ERR_ARG, "aslb_lbgk_run: bad arguments");
   for (int b = 0; b < nbc; ++b)
@@ -1323,6 +1334,7 @@ int aslb_bc_fuse(aslb_bc* bc) {
 int aslb_bc_is_fused(aslb_bc* bc) { return bc && bc->fused ? 1 : 0; }
 
 int aslb_bc_execute(aslb_bc* bc) {
+  NvtxRange range("aslb_bc_execute");
   if (!bc) return fail(ASLB_ERR_ARG, "aslb_bc_execute: null handle");
   if (!bc->h) return fail(ASLB_ERR_STATE, "aslb_bc_execute: its domain was destroyed");
   return do_bc(bc);
@@ -1442,6 +1454,7 @@ int aslb_flux_compute(aslb_flux* fc, float* field_host, double* total) {
 int aslb_flux_destroy(aslb_flux* fc) { return aslb_force_destroy(fc); }
 
 int aslb_force_compute(aslb_force* fc, const double r0[3], float* field_host, double out6[6]) {
+  NvtxRange range("aslb_force_compute");
   if (!fc || !out6) return fail(ASLB_ERR_ARG, "aslb_force_compute: null argument");
   if (fc->flux) return fail(ASLB_ERR_ARG, "aslb_force_compute: a flux object, not a force object");
   if (!fc->h) return fail(ASLB_ERR_STATE, "aslb_force_compute: its domain was destroyed");
@@ -1722,6 +1735,7 @@ int aslb_batch_create(aslb_lbgk* const* domains, int n, aslb_batch** out) {
 }
 
 int aslb_batch_run(aslb_batch* b, int nsteps, aslb_bc* const* bcs, const int* nbc, int use_graph) {
+  NvtxRange range("aslb_batch_run");
   ASLB_CHECK_HANDLE(b);
   if (b->detached) return fail(ASLB_ERR_STATE, "aslb_batch_run: a domain of the batch was destroyed");
   const int n = (int)b->doms.size();

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <nvtx3/nvToolsExt.h>
 #include "aslb.h"
 #include "kernels.h"
 #include "lattice.cuh"
@@ -379,6 +380,8 @@ int aslb_fd_set_face_value(aslb_fd* f, unsigned wallmask, double value) {
 }
 
 int aslb_fd_step(aslb_fd* f, int n) {
+  nvtxRangePushA("aslb_fd_step");
+  struct Pop { ~Pop() { nvtxRangePop(); } } pop;
   if (!f || n < 0) return fd_arg("aslb_fd_step: null argument or negative count");
   for (int s = 0; s < n; ++s) {
     cudaError_t e = f->dtype == ASLB_F64 ? fd_step_t<double>(f) : fd_step_t<float>(f);
