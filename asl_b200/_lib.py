@@ -67,6 +67,7 @@ PROTOTYPES = {
     "aslb_lbgk_read": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "aslb_lbgk_write": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "aslb_bc_map_create_cd": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_double, _pd, _pd, _pd, _vp]),
+    "aslb_lbgk_watchdog": (C.c_int, [_vp, _pd]),
     "aslb_lattice": (C.c_int, [C.c_int, _vp, _vp, _vp]),
     "aslb_bc_field_create": (C.c_int, [_vp, C.c_int, _vp, _pd, _pd, _pd, _vp]),
     "aslb_bc_deposition_create": (C.c_int, [_vp, C.c_int, _vp, C.c_double, C.c_double, C.c_double, _vp]),

@@ -1024,6 +1024,31 @@ int aslb_lbgk_moments(aslb_lbgk* h, double out[4]) {
   return ASLB_OK;
 }
 
+int aslb_lbgk_watchdog(aslb_lbgk* h, double out[3]) {
+  ASLB_CHECK_HANDLE(h);
+  if (!out) return fail(ASLB_ERR_ARG, "aslb_lbgk_watchdog: null output");
+  const int nb = moments_blocks(h->d.g);
+  if (!h->red_partials) ASLB_CUDA(cudaMalloc((void**)&h->red_partials, (size_t)nb * 4 * sizeof(double)));
+  prepare_params(h);
+  std::vector<double> rows((size_t)nb * 3);
+  cudaError_t e = launch_watchdog(h->d, h->p, h->parity, h->red_partials, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(rows.data(), h->red_partials, rows.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                        h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_watchdog: ") + cudaGetErrorString(e));
+  double umax = 0.0, rmin = 1e300, bad = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    umax = std::max(umax, rows[(size_t)b * 3]);
+    rmin = std::min(rmin, rows[(size_t)b * 3 + 1]);
+    bad += rows[(size_t)b * 3 + 2];
+  }
+  out[0] = std::sqrt(umax);
+  out[1] = rmin;
+  out[2] = bad;
+  return ASLB_OK;
+}
+
 // ---- boundary conditions ---------------------------------------------------
 
 int aslb_bc_slice_create(aslb_lbgk* h, int kind, unsigned wallmask, double p, const double u[3], aslb_bc** out) {

@@ -682,4 +682,77 @@ cudaError_t launch_moments(const DomainDev& d, const StepParams& p, int parity, 
   ASLB_DISPATCH(d, moments_impl, d, p, parity, partials, out4, st)
 }
 
+// Blow-up watchdog: per block, the largest |u|^2 and smallest rho over its
+// interior cells (u = m / rho, or m for the incompressible equilibrium) and
+// the number of cells with a non-finite rho or u; rows [max u^2, min rho,
+// count], reduced on the host.
+template <int Q, class S>
+__global__ void __launch_bounds__(kMomentThreads)
+    k_watchdog(const S* __restrict__ F, const GridDesc g, const StepParams p, int parity,
+               double* __restrict__ partials) {
+  using Lt = Lattice<Q>;
+  double umax = 0.0, rmin = 1e300, bad = 0.0;
+  const long long total = (long long)g.nx * g.ny * g.nz;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int z = int(c % g.nz) + 1;
+    const long long r = c / g.nz;
+    const int y = int(r % g.ny) + 1;
+    const int x = int(r / g.ny) + 1;
+    double rho = 0, m[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      // stored populations are f_i / w_i (ASL's layout): rho = sum w f, m = sum w c f
+      const double wf =
+          Lt::w(i) * double(Store<S>::val(F + fstar_index<Q>(g, p.mask, parity, x, y, z, i), p.inv_scale));
+      rho += wf;
+      m[0] += Lt::c(i, 0) * wf;
+      m[1] += Lt::c(i, 1) * wf;
+      m[2] += Lt::c(i, 2) * wf;
+    }
+    const double inv = p.compressible ? 1.0 / rho : 1.0;
+    const double u2 = (m[0] * m[0] + m[1] * m[1] + m[2] * m[2]) * inv * inv;
+    if (!isfinite(u2) || !isfinite(rho)) {
+      bad += 1.0;
+    } else {
+      umax = fmax(umax, u2);
+      rmin = fmin(rmin, rho);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    umax = fmax(umax, __shfl_down_sync(0xffffffffu, umax, o));
+    rmin = fmin(rmin, __shfl_down_sync(0xffffffffu, rmin, o));
+    bad += __shfl_down_sync(0xffffffffu, bad, o);
+  }
+  __shared__ double sh[32][3];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sh[warp][0] = umax;
+    sh[warp][1] = rmin;
+    sh[warp][2] = bad;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      umax = fmax(umax, sh[w][0]);
+      rmin = fmin(rmin, sh[w][1]);
+      bad += sh[w][2];
+    }
+    partials[(size_t)blockIdx.x * 3 + 0] = umax;
+    partials[(size_t)blockIdx.x * 3 + 1] = rmin;
+    partials[(size_t)blockIdx.x * 3 + 2] = bad;
+  }
+}
+
+template <int Q, class S>
+static cudaError_t watchdog_impl(const DomainDev& d, const StepParams& p, int parity, double* partials,
+                                 cudaStream_t st) {
+  k_watchdog<Q, S><<<moments_blocks(d.g), kMomentThreads, 0, st>>>((const S*)d.F, d.g, p, parity, partials);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_watchdog(const DomainDev& d, const StepParams& p, int parity, double* partials, cudaStream_t st) {
+  ASLB_DISPATCH(d, watchdog_impl, d, p, parity, partials, st)
+}
+
 }  // namespace aslb

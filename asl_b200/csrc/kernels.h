@@ -61,6 +61,9 @@ cudaError_t launch_bc_links(const DomainDev& d, const int* links, int n, const L
 // Surface force: per-cell field (ASL layout, optional) and per-block FP64
 // partial sums of (F, (r - r0) x F), then a fixed-order final sum into out6.
 int force_blocks(int n);
+// Blow-up watchdog rows (moments_blocks(g) rows of [max |u|^2, min rho, non-finite cells]).
+int moments_blocks(const GridDesc& g);
+cudaError_t launch_watchdog(const DomainDev& d, const StepParams& p, int parity, double* partials, cudaStream_t st);
 // Surface flux (ComputeSurfaceFluxMap): same cell lists as the force, one
 // value per cell (field, optional) and its FP64 total (out1).
 cudaError_t launch_flux(const DomainDev& d, const int4* cells, const uint32_t* mask_in, int n, float* field,

@@ -271,6 +271,12 @@ class LBGK:
         L.check(self.lib.aslb_lbgk_load_state(self.h, data.ctypes.data_as(C.c_void_p), data.nbytes, m),
                 "LBGK::loadState")
 
+    def watchdog(self) -> dict:
+        """Largest |u|, smallest rho and number of non-finite cells (FP64)."""
+        out = (C.c_double * 3)()
+        L.check(self.lib.aslb_lbgk_watchdog(self.h, out), "LBGK::watchdog")
+        return {"max_u": out[0], "min_rho": out[1], "nonfinite": int(out[2])}
+
     def moments(self) -> np.ndarray:
         out = (C.c_double * 4)()
         L.check(self.lib.aslb_lbgk_moments(self.h, out), "LBGK::moments")

@@ -227,6 +227,12 @@ int aslb_lbgk_parity(aslb_lbgk* h);
 /* Global FP64 moments of the post-collision populations over interior cells:
  * out[0] mass, out[1..3] momentum (a blow-up watchdog). Synchronises. */
 int aslb_lbgk_moments(aslb_lbgk* h, double out[4]);
+/* Extension (no ASL analogue): blow-up watchdog over the interior cells
+ * (solid ones included), from the post-collision populations in FP64:
+ * out[0] the largest |u| (u = m / rho; m for the incompressible
+ * equilibrium), out[1] the smallest rho, out[2] the number of cells whose
+ * rho or u is not finite. Synchronises. */
+int aslb_lbgk_watchdog(aslb_lbgk* h, double out[3]);
 
 /* ---- boundary conditions ----------------------------------------------- */
 

@@ -614,3 +614,28 @@ def test_output_field_conditions_reject_d3q27(gpu):
     m = np.ones((10, 10, 10), dtype=np.float32)
     with pytest.raises(A.L.ASLError, match="d3q27"):
         A.generateBCNoSlipVel(lb, m)
+
+
+@pytest.mark.parametrize("storage,tol", [("f64", 1e-12), ("f32", 1e-5)])
+def test_watchdog(gpu, storage, tol):
+    """aslb_lbgk_watchdog: largest |u| and smallest rho from the populations
+    agree with the velocity / density outputs (periodic box, no force: the
+    collision keeps both moments); a non-finite cell is counted, not folded
+    into the extremes."""
+    size = (12, 10, 8)
+    g = tuple(s + 2 for s in size)
+    rho, u = smooth_field(g, 77, amp=0.05)
+    lb = A.LBGK(A.Block(size), 0.03, A.d3q19(), storage=storage, periodic=(True, True, True))
+    A.LBGKUtilities(lb).initF(rho, u)
+    lb.run(5)
+    wd = lb.watchdog()
+    uo = lb.getVelocity()[I4]
+    ro = lb.getRho()[1:-1, 1:-1, 1:-1]
+    assert wd["nonfinite"] == 0
+    assert abs(wd["max_u"] - np.sqrt((uo ** 2).sum(0)).max()) <= tol
+    assert abs(wd["min_rho"] - ro.min()) <= tol
+    f = lb.getF()
+    f[3, 5, 5, 5] = np.nan
+    lb.setF(f)
+    wd2 = lb.watchdog()
+    assert wd2["nonfinite"] == 1 and np.isfinite(wd2["max_u"]) and np.isfinite(wd2["min_rho"])
