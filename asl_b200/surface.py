@@ -141,8 +141,184 @@ def surfaceToData(tri, b: Union[Block, float], *offsets, solid_interior: bool = 
     return _wrap(m, tuple(lo), dx)
 
 
+# ---- VTK XML PolyData (.vtp) ------------------------------------------------
+#
+# The .vtp branch of readSurface (aslVTKFormatReaders.cxx:219-257 reads it with
+# vtkXMLPolyDataReader). Points and polygons are read from the file's
+# DataArrays in any of VTK's encodings: ascii, binary (base64 with a UInt32 or
+# UInt64 size header), appended (raw or base64), optionally compressed in
+# zlib blocks (vtkZLibDataCompressor); polygons are split into fans of
+# triangles.
+
+_VTK_TYPES = {"Float32": "<f4", "Float64": "<f8", "Int8": "<i1", "UInt8": "<u1", "Int16": "<i2", "UInt16": "<u2",
+              "Int32": "<i4", "UInt32": "<u4", "Int64": "<i8", "UInt64": "<u8"}
+
+
+def _vtp_block(raw: bytes, pos: int, hdt: str, compressed: bool, b64: bool):
+    """Decode one binary data block starting at raw[pos:]; returns (bytes, next pos)."""
+    import base64
+    import zlib
+    hsz = np.dtype(hdt).itemsize
+    if not b64:
+        if not compressed:
+            n = int(np.frombuffer(raw[pos:pos + hsz], hdt)[0])
+            return raw[pos + hsz:pos + hsz + n], pos + hsz + n
+        nb = int(np.frombuffer(raw[pos:pos + hsz], hdt)[0])
+        head = np.frombuffer(raw[pos:pos + hsz * (3 + nb)], hdt)
+        sizes = head[3:3 + nb].astype(np.int64)
+        q = pos + hsz * (3 + nb)
+        out = b"".join(zlib.decompress(raw[q + int(o):q + int(o) + int(sz)])
+                       for o, sz in zip(np.concatenate([[0], np.cumsum(sizes)[:-1]]), sizes))
+        return out, q + int(sizes.sum())
+    # base64: the text runs to the next tag; arrays of an appended section
+    # follow each other, so only the characters this block needs are decoded
+    text = b"".join(raw[pos:].split(b"<", 1)[0].split())
+
+    def dec(chars: int) -> bytes:
+        return base64.b64decode(text[:chars])
+    if not compressed:
+        n = int(np.frombuffer(dec(((hsz + 2) // 3) * 4)[:hsz], hdt)[0])
+        return dec(((hsz + n + 2) // 3) * 4)[hsz:hsz + n], len(raw)
+    # compressed: the header is encoded on its own, then the blocks
+    nb = int(np.frombuffer(dec(((hsz + 2) // 3) * 4)[:hsz], hdt)[0])
+    hlen = ((hsz * (3 + nb) + 2) // 3) * 4
+    head = np.frombuffer(dec(hlen)[:hsz * (3 + nb)], hdt)
+    sizes = head[3:3 + nb].astype(np.int64)
+    total = int(sizes.sum())
+    body = base64.b64decode(text[hlen:hlen + ((total + 2) // 3) * 4])
+    out, q = [], 0
+    for sz in sizes:
+        out.append(zlib.decompress(body[q:q + int(sz)]))
+        q += int(sz)
+    return b"".join(out), len(raw)
+
+
+def readVTP(path: str) -> np.ndarray:
+    """Triangles of a VTK XML PolyData file, (n, 3, 3) float32 in file coordinates."""
+    import re
+    with open(path, "rb") as f:
+        raw = f.read()
+    head_end = raw.find(b"<AppendedData")
+    head = raw[: head_end if head_end >= 0 else len(raw)].decode("latin-1")
+    root = re.search(r"<VTKFile([^>]*)>", head)
+    if not root or 'type="PolyData"' not in root.group(1):
+        raise L.ASLError("ASL ERROR: readVTP: not a VTK XML PolyData file")
+    attrs = root.group(1)
+    hdt = "<u8" if 'header_type="UInt64"' in attrs else "<u4"
+    if 'byte_order="BigEndian"' in attrs:
+        raise L.ASLError("ASL ERROR: readVTP: big-endian files are not supported")
+    compressed = "vtkZLibDataCompressor" in attrs
+    app_start, app_b64 = None, False
+    if head_end >= 0:
+        m = re.match(rb"<AppendedData[^>]*encoding=\"(\w+)\"[^>]*>", raw[head_end:])
+        app_b64 = bool(m) and m.group(1) == b"base64"
+        app_start = raw.index(b"_", head_end) + 1
+
+    def array(section: str, name: str | None):
+        sec = re.search(r"<%s>(.*?)</%s>" % (section, section), head, re.S)
+        if not sec:
+            raise L.ASLError("ASL ERROR: readVTP: no %s section" % section)
+        for m in re.finditer(r"<DataArray([^>]*[^/])>(.*?)</DataArray>|<DataArray([^>]*)/>", sec.group(1), re.S):
+            at = m.group(1) or m.group(3)
+            if name is not None and ('Name="%s"' % name) not in at:
+                continue
+            vt = re.search(r'type="(\w+)"', at).group(1)
+            fmt = re.search(r'format="(\w+)"', at).group(1)
+            dt = _VTK_TYPES[vt]
+            if fmt == "ascii":
+                return np.array((m.group(2) or "").split(), dtype=dt)
+            if fmt == "binary":
+                body = (m.group(2) or "").encode()
+                data, _ = _vtp_block(body, 0, hdt, compressed, True)
+                return np.frombuffer(data, dt)
+            if app_start is None:
+                raise L.ASLError("ASL ERROR: readVTP: appended array without an AppendedData section")
+            off = int(re.search(r'offset="(\d+)"', at).group(1))
+            data, _ = _vtp_block(raw, app_start + off, hdt, compressed, app_b64)
+            return np.frombuffer(data, dt)
+        raise L.ASLError("ASL ERROR: readVTP: array %s of %s not found" % (name, section))
+
+    pts = array("Points", None).astype(np.float32).reshape(-1, 3)
+    conn = array("Polys", "connectivity").astype(np.int64)
+    offs = array("Polys", "offsets").astype(np.int64)
+    tris = []
+    start = 0
+    for end in offs:
+        poly = conn[start:end]
+        for k in range(1, len(poly) - 1):
+            tris.append((poly[0], poly[k], poly[k + 1]))
+        start = end
+    if not tris:
+        return np.zeros((0, 3, 3), dtype=np.float32)
+    return np.ascontiguousarray(pts[np.asarray(tris)], dtype=np.float32)
+
+
+def writeVTP(path: str, tri: np.ndarray, encoding: str = "appended", compress: bool = False):
+    """Write triangles (n, 3, 3) as VTK XML PolyData: encoding "ascii",
+    "binary" (base64) or "appended" (raw); zlib-compressed blocks with
+    ``compress`` (binary encodings). Points are not merged."""
+    import base64
+    import struct
+    import zlib
+    tri = np.asarray(tri, dtype=np.float32).reshape(-1, 3, 3)
+    pts = tri.reshape(-1, 3)
+    conn = np.arange(len(pts), dtype=np.int64)
+    offs = np.arange(3, len(pts) + 1, 3, dtype=np.int64)
+    arrays = [("Points", None, "Float32", pts.reshape(-1), 3), ("Polys", "connectivity", "Int64", conn, 1),
+              ("Polys", "offsets", "Int64", offs, 1)]
+
+    def block(a: np.ndarray) -> bytes:
+        raw = a.tobytes()
+        if not compress:
+            return struct.pack("<Q", len(raw)) + raw
+        z = zlib.compress(raw)
+        return struct.pack("<QQQQ", 1, len(raw), len(raw), len(z)) + z
+
+    comp = ' compressor="vtkZLibDataCompressor"' if compress and encoding != "ascii" else ""
+    out = ['<?xml version="1.0"?>\n<VTKFile type="PolyData" version="1.0" byte_order="LittleEndian" '
+           'header_type="UInt64"%s>\n  <PolyData>\n    <Piece NumberOfPoints="%d" NumberOfPolys="%d">\n'
+           % (comp, len(pts), len(tri))]
+    appended, off = [], 0
+    for section in ("Points", "Polys"):
+        out.append("      <%s>\n" % section)
+        for sec, name, vt, a, nc in arrays:
+            if sec != section:
+                continue
+            nm = ' Name="%s"' % name if name else ""
+            ncs = ' NumberOfComponents="3"' if nc == 3 else ""
+            if encoding == "ascii":
+                out.append('        <DataArray type="%s"%s%s format="ascii">%s</DataArray>\n'
+                           % (vt, nm, ncs, " ".join(repr(float(v)) if vt == "Float32" else str(int(v)) for v in a)))
+            elif encoding == "binary":
+                b = block(a)
+                if compress:  # header and blocks encoded separately, as VTK does
+                    hl = 8 * 4
+                    txt = base64.b64encode(b[:hl]) + base64.b64encode(b[hl:])
+                else:
+                    txt = base64.b64encode(b)
+                out.append('        <DataArray type="%s"%s%s format="binary">%s</DataArray>\n'
+                           % (vt, nm, ncs, txt.decode()))
+            else:
+                b = block(a)
+                out.append('        <DataArray type="%s"%s%s format="appended" offset="%d"/>\n' % (vt, nm, ncs, off))
+                appended.append(b)
+                off += len(b)
+        out.append("      </%s>\n" % section)
+    out.append("    </Piece>\n  </PolyData>\n")
+    with open(path, "wb") as f:
+        f.write("".join(out).encode())
+        if appended:
+            f.write(b'  <AppendedData encoding="raw">\n   _' + b"".join(appended) + b"\n  </AppendedData>\n")
+        f.write(b"</VTKFile>\n")
+
+
 def readSurface(fileName: str, b: Union[Block, float], *offsets, solid_interior: bool = False) -> SurfaceData:
+    """readSurface (aslVTKFormatReaders.cxx:307-345): .stl or .vtp."""
     ext = os.path.splitext(fileName)[1].lower()
-    if ext != ".stl":
+    if ext == ".stl":
+        tri = readSTL(fileName)
+    elif ext == ".vtp":
+        tri = readVTP(fileName)
+    else:
         raise L.ASLError("ASL ERROR: Reader: file format not supported")
-    return surfaceToData(readSTL(fileName), b, *offsets, solid_interior=solid_interior)
+    return surfaceToData(tri, b, *offsets, solid_interior=solid_interior)

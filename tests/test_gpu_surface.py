@@ -84,3 +84,16 @@ def test_read_surface_spacing_overloads(gpu, tmp_path):
     ext = sph.reshape(-1, 3)[:, ::-1].max(0) - sph.reshape(-1, 3)[:, ::-1].min(0)
     expect = [int(np.floor((ext[a] * (1 + f)) / 0.5)) + 1 for a, f in enumerate((1.5, 1.0, 6.0))]
     assert list(m2.shape) == expect
+
+
+def test_read_surface_vtp_equals_stl(gpu, tmp_path):
+    """readSurface gives the same map from the same surface in .stl and .vtp
+    (compressed appended binary)."""
+    sph = SO.icosphere(3.0, (8.0, 7.0, 6.0), subdiv=2)
+    S.writeSTL(str(tmp_path / "s.stl"), sph)
+    S.writeVTP(str(tmp_path / "s.vtp"), sph, encoding="appended", compress=True)
+    b = A.Block((16, 14, 12), 1.0, (0.0, 0.0, 0.0))
+    a = S.readSurface(str(tmp_path / "s.stl"), b)
+    v = S.readSurface(str(tmp_path / "s.vtp"), b)
+    assert np.array_equal(np.asarray(a), np.asarray(v))
+    assert v.getInternalBlock().size == (14, 12, 10)

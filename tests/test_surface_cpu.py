@@ -47,4 +47,34 @@ def test_stl_errors(tmp_path):
     with pytest.raises(S.L.ASLError):
         S.readSTL(str(tmp_path / "missing.stl"))
     with pytest.raises(S.L.ASLError, match="not supported"):
-        S.readSurface(str(tmp_path / "x.vtp"), 1.0)
+        S.readSurface(str(tmp_path / "x.obj"), 1.0)
+
+
+@pytest.mark.parametrize("encoding,compress", [("ascii", False), ("binary", False), ("binary", True),
+                                               ("appended", False), ("appended", True)])
+def test_vtp_roundtrip(tmp_path, encoding, compress):
+    sph = SO.icosphere(1.5, (0.5, -1.0, 2.0), subdiv=1)
+    path = str(tmp_path / ("s_%s_%d.vtp" % (encoding, compress)))
+    S.writeVTP(path, sph, encoding=encoding, compress=compress)
+    got = S.readVTP(path)
+    assert got.shape == sph.shape and np.array_equal(got, sph)
+
+
+def test_vtp_polygons_become_triangle_fans(tmp_path):
+    """A hand-written ascii file with one quad and one triangle sharing points."""
+    path = tmp_path / "quad.vtp"
+    path.write_text('<?xml version="1.0"?>\n<VTKFile type="PolyData" version="0.1" byte_order="LittleEndian">\n'
+                    ' <PolyData><Piece NumberOfPoints="5" NumberOfPolys="2">\n'
+                    '  <Points><DataArray type="Float32" NumberOfComponents="3" format="ascii">\n'
+                    '   0 0 0  1 0 0  1 1 0  0 1 0  0 0 1</DataArray></Points>\n'
+                    '  <Polys><DataArray type="Int32" Name="connectivity" format="ascii">0 1 2 3 0 1 4</DataArray>\n'
+                    '   <DataArray type="Int32" Name="offsets" format="ascii">4 7</DataArray></Polys>\n'
+                    ' </Piece></PolyData>\n</VTKFile>\n')
+    got = S.readVTP(str(path))
+    want = np.array([[[0, 0, 0], [1, 0, 0], [1, 1, 0]], [[0, 0, 0], [1, 1, 0], [0, 1, 0]],
+                     [[0, 0, 0], [1, 0, 0], [0, 0, 1]]], dtype=np.float32)
+    assert np.array_equal(got, want)
+    bad = tmp_path / "img.vtp"
+    bad.write_text('<?xml version="1.0"?><VTKFile type="ImageData"></VTKFile>')
+    with pytest.raises(S.L.ASLError):
+        S.readVTP(str(bad))
