@@ -77,6 +77,7 @@ PROTOTYPES = {
     "aslb_fd_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _vp]),
     "aslb_fd_set_velocity": (C.c_int, [_vp, _vp, C.c_int]),
     "aslb_fd_set_diffusion": (C.c_int, [_vp, C.c_double]),
+    "aslb_fd_set_electric_field": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
     "aslb_fd_write": (C.c_int, [_vp, C.c_int, _vp]),
     "aslb_fd_read": (C.c_int, [_vp, C.c_int, _vp]),
     "aslb_fd_set_face_value": (C.c_int, [_vp, C.c_uint, C.c_double]),

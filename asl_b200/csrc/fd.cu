@@ -3,12 +3,14 @@
 // 209-226) for one component with a constant diffusion coefficient D,
 //   c' = D lap(c) + c - divProduct(u, c)
 //   (compressibility correction: c' /= 1 - div(u); c' += lap(c) |u(x)|^2 / 2)
-// with the stencil operators of src/math/aslTemplateVE.cxx:164-267 on the
+// and, with setElectricFieldParameters (:66-74, 166-172), c' -= divAgradB(c q / k, phi),
+// with the stencil operators of src/math/aslTemplateVE.cxx:164-280 on the
 // templates d3q7 / d3q15 / d3q19 (laplacian and gradient coefficients of
 // src/math/aslTemplates.cxx:134-186):
 //   lap(c)            = sum_i LC_i c(x + e_i)
 //   div(u)            = sum_d sum_i GC_i e_i,d u_d(x + e_i)
 //   divProduct(u, c)  = sum_d sum_i GC_i e_i,d (u_d(x + e_i) + u_d(x)) (c(x + e_i) + c(x)) / 2
+//   divAgradB(a, b)   = sum_i GC_i (a(x + e_i) + a(x)) (b(x + e_i) - b(x))
 // The update writes the interior of a second buffer and the buffers swap
 // (postProcessing), so ghost values persist in both: they are the
 // boundary values (BCConstantValue on faces, src/num/aslBasicBC.cxx:51-57).
@@ -50,8 +52,8 @@ struct FdGrid {
 
 // The update of one cell from its stencil values: cv(i) = c(x + e_i),
 // uv(d, i) = u_d(x + e_i).
-template <int Q, class T, bool U, class CV, class UV>
-__device__ __forceinline__ T fd_cell(CV cvf, UV uvf, T D, int cc) {
+template <int Q, class T, bool U, bool E, class CV, class UV, class EV>
+__device__ __forceinline__ T fd_cell(CV cvf, UV uvf, EV evf, T D, int cc) {
   using Tp = FdTemplate<Q>;
   T cv[Q];
 #pragma unroll
@@ -84,6 +86,15 @@ __device__ __forceinline__ T fd_cell(CV cvf, UV uvf, T D, int cc) {
       cnew += lap * (u0[0] * u0[0] + u0[1] * u0[1] + u0[2] * u0[2]) * T(0.5);
     }
   }
+  if (E) {
+    // electric term: - divAgradB(c q / k, phi) = - sum_i GC_i (a_i + a_0) (phi_i - phi_0),
+    // a = c q / k (evf(0, i) = phi, evf(1, i) = k, evf(2, i) = q at x + e_i)
+    const T a0 = cv[0] * evf(2, 0) / evf(1, 0), p0 = evf(0, 0);
+    T s = T(0);
+#pragma unroll
+    for (int i = 1; i < Q; ++i) s += T(Tp::gc(i)) * (cv[i] * evf(2, i) / evf(1, i) + a0) * (evf(0, i) - p0);
+    cnew -= s;
+  }
   return cnew;
 }
 
@@ -94,12 +105,18 @@ __device__ __forceinline__ T fd_cell(CV cvf, UV uvf, T D, int cc) {
 // neighbour read of the stencil is a shared-memory load.
 constexpr int kFdTZ = 64, kFdTY = 4, kFdPlanes = 32;
 
-template <int Q, class T, bool U>
+template <int Q, class T, bool U, bool E>
 __global__ void __launch_bounds__(kFdTZ * kFdTY) k_fd_step(const T* __restrict__ c, T* __restrict__ cn,
-                                                          const T* __restrict__ u, FdGrid g, T D, int cc) {
+                                                          const T* __restrict__ u, const T* __restrict__ ef,
+                                                          FdGrid g, T D, int cc) {
   using Tp = FdTemplate<Q>;
-  constexpr int W = kFdTZ + 2, H = kFdTY + 2, P = W * H, NF = U ? 4 : 1;
-  __shared__ T sm[3][NF][P];
+  // fields per plane: c, then u (3) with a velocity, then phi, k, q with the electric term
+  constexpr int UB = 1, EB = U ? 4 : 1;
+  constexpr int W = kFdTZ + 2, H = kFdTY + 2, P = W * H, NF = 1 + (U ? 3 : 0) + (E ? 3 : 0);
+  // three planes of the tile (dynamic: FP64 with velocity and electric fields
+  // needs 66.5 KB)
+  extern __shared__ __align__(16) unsigned char fd_smem[];
+  auto sm = reinterpret_cast<T(*)[NF][P]>(fd_smem);
   const int tz = threadIdx.x, ty = threadIdx.y, t = ty * kFdTZ + tz;
   const int z0 = blockIdx.x * kFdTZ, y0 = blockIdx.y * kFdTY;  // ghosted origin of the tile
   const int x0 = blockIdx.z * kFdPlanes + 1, x1 = min(g.nx, x0 + kFdPlanes - 1);
@@ -120,9 +137,14 @@ __global__ void __launch_bounds__(kFdTZ * kFdTY) k_fd_step(const T* __restrict__
         const long long a = ((long long)xp * g.gy + yy) * g.gz + zz;
         r[k][0] = c[a];
         if (U) {
-          r[k][1 % NF] = u[a];
-          r[k][2 % NF] = u[g.L + a];
-          r[k][3 % NF] = u[2 * g.L + a];
+          r[k][UB % NF] = u[a];
+          r[k][(UB + 1) % NF] = u[g.L + a];
+          r[k][(UB + 2) % NF] = u[2 * g.L + a];
+        }
+        if (E) {
+          r[k][EB % NF] = ef[a];
+          r[k][(EB + 1) % NF] = ef[g.L + a];
+          r[k][(EB + 2) % NF] = ef[2 * g.L + a];
         }
       }
     }
@@ -150,8 +172,9 @@ __global__ void __launch_bounds__(kFdTZ * kFdTY) k_fd_step(const T* __restrict__
       const int sl[3] = {(x + 2) % 3, x % 3, (x + 1) % 3};
       const int base = (ty + 1) * W + tz + 1;
       auto cvf = [&](int i) { return sm[sl[1 + Tp::e(i, 0)]][0][base + Tp::e(i, 1) * W + Tp::e(i, 2)]; };
-      auto uvf = [&](int d, int i) { return sm[sl[1 + Tp::e(i, 0)]][U ? 1 + d : 0][base + Tp::e(i, 1) * W + Tp::e(i, 2)]; };
-      cn[((long long)x * g.gy + y) * g.gz + z] = fd_cell<Q, T, U>(cvf, uvf, D, cc);
+      auto uvf = [&](int d, int i) { return sm[sl[1 + Tp::e(i, 0)]][U ? UB + d : 0][base + Tp::e(i, 1) * W + Tp::e(i, 2)]; };
+      auto evf = [&](int f, int i) { return sm[sl[1 + Tp::e(i, 0)]][E ? EB + f : 0][base + Tp::e(i, 1) * W + Tp::e(i, 2)]; };
+      cn[((long long)x * g.gy + y) * g.gz + z] = fd_cell<Q, T, U, E>(cvf, uvf, evf, D, cc);
     }
     __syncthreads();
   }
@@ -219,6 +242,7 @@ struct aslb_fd {
   int cc = 0;
   cudaStream_t stream = nullptr, own = nullptr;
   aslb_lbgk* bound = nullptr;  // domain whose velocity and stream are used
+  void* ef = nullptr;           // electric term: phi, k, q (3 L values), or none
   long long steps = 0;
   std::vector<aslb_fd_bc*> bcs;  // map conditions on c (detached on destroy)
 };
@@ -254,17 +278,34 @@ int fd_arg(const char* what) {
 }
 size_t fd_elem(const aslb_fd* f) { return f->dtype == ASLB_F64 ? 8 : 4; }
 
+// Launch one instantiation with its dynamic shared memory (three tile planes
+// of every field it stages), raising the limit once where above 48 KB.
+template <int Q, class T, bool U, bool E>
+cudaError_t fd_launch_one(aslb_fd* f, dim3 grid, dim3 block, const T* c, T* cn, const T* u, const T* ef) {
+  constexpr int NF = 1 + (U ? 3 : 0) + (E ? 3 : 0);
+  constexpr size_t bytes = 3u * NF * (kFdTZ + 2) * (kFdTY + 2) * sizeof(T);
+  static bool raised = false;
+  if (bytes > 48 * 1024 && !raised) {
+    cudaError_t e = cudaFuncSetAttribute(k_fd_step<Q, T, U, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    raised = true;
+  }
+  k_fd_step<Q, T, U, E><<<grid, block, bytes, f->stream>>>(c, cn, u, ef, f->g, T(f->D), U ? f->cc : 0);
+  return cudaGetLastError();
+}
+
 template <int Q, class T>
 cudaError_t fd_launch(aslb_fd* f) {
   dim3 block(kFdTZ, kFdTY),
       grid((f->g.nz + kFdTZ - 1) / kFdTZ, (f->g.ny + kFdTY - 1) / kFdTY, (f->g.nx + kFdPlanes - 1) / kFdPlanes);
   const T* c = (const T*)f->c[f->cur];
   T* cn = (T*)f->c[1 - f->cur];
-  if (f->u)
-    k_fd_step<Q, T, true><<<grid, block, 0, f->stream>>>(c, cn, (const T*)f->u, f->g, T(f->D), f->cc);
-  else
-    k_fd_step<Q, T, false><<<grid, block, 0, f->stream>>>(c, cn, nullptr, f->g, T(f->D), 0);
-  return cudaGetLastError();
+  const T* ef = (const T*)f->ef;
+  const T* u = (const T*)f->u;
+  if (u && ef) return fd_launch_one<Q, T, true, true>(f, grid, block, c, cn, u, ef);
+  if (u) return fd_launch_one<Q, T, true, false>(f, grid, block, c, cn, u, nullptr);
+  if (ef) return fd_launch_one<Q, T, false, true>(f, grid, block, c, cn, nullptr, ef);
+  return fd_launch_one<Q, T, false, false>(f, grid, block, c, cn, nullptr, nullptr);
 }
 
 template <class T>
@@ -329,6 +370,29 @@ int aslb_fd_set_velocity(aslb_fd* f, aslb_lbgk* h, int compressibility_correctio
   f->cc = compressibility_correction ? 1 : 0;
   f->bound = h;
   lbgk_attach_fd(h, f);
+  return ASLB_OK;
+}
+
+int aslb_fd_set_electric_field(aslb_fd* f, int dtype, const void* phi, const void* k, const void* q) {
+  if (!f) return fd_arg("aslb_fd_set_electric_field: null argument");
+  if (!phi && !k && !q) {
+    if (f->ef) {
+      cudaStreamSynchronize(f->stream);
+      cudaFree(f->ef);
+      f->ef = nullptr;
+    }
+    return ASLB_OK;
+  }
+  if (!phi || !k || !q || dtype != f->dtype)
+    return fd_arg("aslb_fd_set_electric_field: phi, k and q are all needed, in the FD's dtype");
+  const size_t bytes = (size_t)f->g.L * fd_elem(f);
+  cudaError_t e = cudaSuccess;
+  if (!f->ef) e = cudaMalloc(&f->ef, 3 * bytes);
+  const void* src[3] = {phi, k, q};
+  for (int i = 0; i < 3 && e == cudaSuccess; ++i)
+    e = cudaMemcpyAsync((char*)f->ef + i * bytes, src[i], bytes, cudaMemcpyHostToDevice, f->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
+  if (e != cudaSuccess) return fd_err("aslb_fd_set_electric_field", e);
   return ASLB_OK;
 }
 
@@ -522,6 +586,7 @@ int aslb_fd_destroy(aslb_fd* f) {
   if (f->stream) cudaStreamSynchronize(f->stream);
   if (f->bound) lbgk_detach_fd(f->bound, f);
   for (aslb_fd_bc* b : f->bcs) b->fd = nullptr;
+  if (f->ef) cudaFree(f->ef);
   for (void* p : f->c)
     if (p) cudaFree(p);
   if (f->own) cudaStreamDestroy(f->own);

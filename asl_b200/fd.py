@@ -60,6 +60,15 @@ class FDAdvectionDiffusion:
         L.check(self.lib.aslb_fd_read(self.h, self.code, out.ctypes.data_as(C.c_void_p)), "FDAdvectionDiffusion")
         return out
 
+    def setElectricFieldParameters(self, phi: np.ndarray, k: np.ndarray, f2=None, q: np.ndarray = None):
+        """c' -= divAgradB(c q / k, phi) each step (ASL's f2 is unused there)."""
+        arrs = [np.ascontiguousarray(a, dtype=self.dtype) for a in (phi, k, q)]
+        if any(a.shape != self.shape for a in arrs):
+            raise L.ASLError("ASL ERROR: setElectricFieldParameters: fields of another shape")
+        self._ef = arrs
+        L.check(self.lib.aslb_fd_set_electric_field(self.h, self.code, *[a.ctypes.data_as(C.c_void_p) for a in arrs]),
+                "FDAdvectionDiffusion::setElectricFieldParameters")
+
     def setDiffusionCoefficient(self, D: float):
         L.check(self.lib.aslb_fd_set_diffusion(self.h, float(D)), "FDAdvectionDiffusion")
 

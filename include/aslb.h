@@ -423,6 +423,12 @@ int aslb_fd_create(int nx, int ny, int nz, int q, int dtype, double D, aslb_fd**
  * otherwise. NULL unbinds. Destroying the domain unbinds it. */
 int aslb_fd_set_velocity(aslb_fd* fd, aslb_lbgk* h, int compressibility_correction);
 int aslb_fd_set_diffusion(aslb_fd* fd, double D);
+/* setElectricFieldParameters(phi, k, f2, q) (src/num/aslFDAdvectionDiffusion.cxx:
+ * 66-74, 166-172; f2 is unused there): each step also subtracts
+ * divAgradB(c q / k, phi) = sum_i GC_i (a_i + a_0) (phi_i - phi_0), a = c q / k.
+ * phi, k, q: host arrays of L values in the FD's dtype, copied to the device;
+ * all three NULL removes the term. */
+int aslb_fd_set_electric_field(aslb_fd* fd, int dtype, const void* phi, const void* k, const void* q);
 /* Host copies of c (ghosted, L values of dtype); writing resets both buffers. */
 int aslb_fd_write(aslb_fd* fd, int dtype, const void* host_in);
 int aslb_fd_read(aslb_fd* fd, int dtype, void* host_out);

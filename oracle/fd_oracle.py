@@ -38,7 +38,8 @@ def template(q: int):
     return e, lc, gc
 
 
-def fd_step(c: np.ndarray, D: float, q: int, u: np.ndarray | None = None, cc: bool = False) -> np.ndarray:
+def fd_step(c: np.ndarray, D: float, q: int, u: np.ndarray | None = None, cc: bool = False,
+            electric=None) -> np.ndarray:
     """One step; returns the new field (ghosts copied unchanged)."""
     T = c.dtype.type
     e, lc, gc = template(q)
@@ -71,6 +72,14 @@ def fd_step(c: np.ndarray, D: float, q: int, u: np.ndarray | None = None, cc: bo
         if cc:
             cnew = cnew / (T(1) - (dv[0] + dv[1] + dv[2]))
             cnew = cnew + lap * (u0[0] * u0[0] + u0[1] * u0[1] + u0[2] * u0[2]) * T(0.5)
+    if electric is not None:  # (phi, k, charge): - divAgradB(c q / k, phi)
+        phi, kk, qq = electric
+        a0 = cv[0] * sh(qq, e[0]) / sh(kk, e[0])
+        p0 = sh(phi, e[0])
+        s = np.zeros_like(cv[0])
+        for i in range(1, q):
+            s = s + T(gc[i]) * (cv[i] * sh(qq, e[i]) / sh(kk, e[i]) + a0) * (sh(phi, e[i]) - p0)
+        cnew = cnew - s
     out = c.copy()
     out[1:-1, 1:-1, 1:-1] = cnew
     return out

@@ -102,3 +102,37 @@ def test_map_conditions_match_oracle(gpu, q, kind, dtype, tol):
         u = lb.getVelocity(dtype)
         ref = fd_map_bc(fd_step(ref, 0.05, q, u), w.map, q, kind == "gradient", 0.02 if kind == "gradient" else 0.3)
     assert np.abs(fd.getC() - ref).max() <= tol
+
+
+@pytest.mark.parametrize("q", [7, 19])
+@pytest.mark.parametrize("with_flow", [False, True])
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-13), (np.float32, 5e-6)])
+def test_electric_field_term_matches_oracle(gpu, q, with_flow, dtype, tol):
+    """setElectricFieldParameters(phi, k, f2, q): each step subtracts
+    divAgradB(c q / k, phi), alone or after the advection terms."""
+    w = W.channel_cylinder(size=(18, 12, 10), radius=2.5, center=(6.0, 6.0), u_in=0.04)
+    g = tuple(s + 2 for s in w.size)
+    x, y, z = np.meshgrid(*[np.arange(n, dtype=float) for n in g], indexing="ij")
+    phi = (0.02 * np.sin(x / 3.0) + 0.01 * np.cos(y / 2.0) * z / g[2]).astype(dtype)
+    kk = (1.0 + 0.2 * np.cos(z / 2.5)).astype(dtype)
+    qq = (0.5 + 0.1 * np.sin(x * y / 20.0)).astype(dtype)
+    c = blob(g, dtype)
+    if with_flow:
+        lb, bcs = W.build_lbgk(w, "f64" if dtype == np.float64 else "f32")
+        fd = FD.generateFDAdvectionDiffusion(c, 0.05, lb, q)
+    else:
+        lb, bcs = None, []
+        fd = FD.generateFDAdvectionDiffusion(c, 0.05, None, q)
+    fd.setElectricFieldParameters(phi, kk, None, qq)
+    ref = fd.getC()
+    for _ in range(4):
+        u = None
+        if lb is not None:
+            lb.run(1, bcs)
+            u = lb.getVelocity(dtype)
+        fd.execute()
+        ref = fd_step(ref, 0.05, q, u, False, electric=(phi, kk, qq))
+    got = fd.getC()
+    assert np.abs(got - ref).max() <= tol
+    plain = fd_step(fd_step(c, 0.05, q), 0.05, q)
+    assert np.abs(ref - plain).max() > 1e-5  # the term acts
