@@ -269,7 +269,7 @@ def pack(params, norm, out_scale=OUT_SCALE) -> bytes:
 
 
 def study(n=256, seed=20261207, times=(250, 500, 1000), train_times=(200, 400, 600), settle=8, iters=1500,
-          period=16, log=print):
+          period=32, log=print):
     """The whole closure study at coarse size n (fine 2n). Returns a dict."""
     torch = _torch()
     import time
@@ -351,7 +351,7 @@ def study(n=256, seed=20261207, times=(250, 500, 1000), train_times=(200, 400, 6
     return res
 
 
-def closure_speed(n: int, blob: bytes, steps: int = 192, period: int = 16, seed: int = 20261207):
+def closure_speed(n: int, blob: bytes, steps: int = 192, period: int = 32, seed: int = 20261207):
     """MLUPS of the plain, Smagorinsky and learned steps on an n^3 periodic
     turbulence field (CUDA graph, CUDA events on the domain's stream)."""
     torch = _torch()
@@ -388,7 +388,7 @@ def _main(argv=None):
     ap.add_argument("what", choices=["study", "speed"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--steps", type=int, default=192)
-    ap.add_argument("--period", type=int, default=16)
+    ap.add_argument("--period", type=int, default=32)
     a = ap.parse_args(argv)
     if a.what == "study":
         res = study(n=a.n, period=a.period)

@@ -58,7 +58,7 @@ struct aslb_lbgk {
   void* mlp_dev = nullptr;
   // learned closure: Cs^2 per storage cell, refreshed every mlp_period steps
   float* cs2_field = nullptr;
-  int mlp_period = 16;
+  int mlp_period = 32;
   long long mlp_last = -1;  // step at which the field was last computed
   double* red_partials = nullptr;  // moments scratch
   double* red_out = nullptr;

@@ -218,7 +218,7 @@ class LBGK:
         L.check(self.lib.aslb_lbgk_set_mlp(self.h, C.cast(buf, C.c_void_p), len(blob)), "LBGK::setMLP")
 
     def setMLPPeriod(self, steps: int):
-        """Steps between two evaluations of the closure network (default 16)."""
+        """Steps between two evaluations of the closure network (default 32)."""
         L.check(self.lib.aslb_lbgk_set_mlp_period(self.h, int(steps)), "LBGK::setMLPPeriod")
 
     def closureFeatures(self, out_dev_ptr: int):

@@ -22,7 +22,7 @@ from . import lbgk as A
 from . import workloads as W
 
 
-def series(w, storage: str, closure: str, steps: int, every: int, blob: bytes | None = None, period: int = 16):
+def series(w, storage: str, closure: str, steps: int, every: int, blob: bytes | None = None, period: int = 32):
     """Run `steps` steps, recording (step, drag = sum F_x, lift = sum F_z)
     every `every` steps. Returns the series and the step rate (MLUPS, CUDA
     events around the time loop, force evaluations excluded)."""

@@ -141,7 +141,7 @@ int aslb_lbgk_set_closure(aslb_lbgk* h, int closure, double cs);
  * limiter): `bytes` of the packed device layout produced by the training code
  * (see aslb_mlp_layout_bytes). Copied to the device. With closure
  * ASLB_CLOSURE_MLP, every `period` steps (aslb_lbgk_set_mlp_period, default
- * 16) a tensor-core kernel evaluates the network on the invariants of every
+ * 32) a tensor-core kernel evaluates the network on the invariants of every
  * cell's non-equilibrium stress and stores a Cs^2 field; each step then
  * applies the Smagorinsky closed form with that cell's Cs^2. D3Q19 / D3Q27,
  * FP32 or FP16 storage. */
