@@ -1,9 +1,11 @@
 // C ABI of libaslb.so (declared in include/aslb.h): domain handles, host-side
 // construction of the compact boundary-link lists, and the time loop.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 #include <nvtx3/nvToolsExt.h>
@@ -60,6 +62,7 @@ struct aslb_lbgk {
   float* cs2_field = nullptr;
   int mlp_period = 32;
   long long mlp_last = -1;  // step at which the field was last computed
+  void* stage = nullptr;            // one-direction transfer buffer (stage_buffer)
   double* red_partials = nullptr;  // moments scratch
   double* red_out = nullptr;
   double* host_out = nullptr;      // pinned
@@ -500,6 +503,7 @@ int aslb_lbgk_destroy(aslb_lbgk* h) {
   cudaFree(h->mask_dev);
   cudaFree(h->mask32_dev);
   cudaFree(h->red_partials);
+  cudaFree(h->stage);
   cudaFree(h->red_out);
   cudaFree(h->d.err);
   if (h->host_out) cudaFreeHost(h->host_out);
@@ -663,14 +667,13 @@ int aslb_lbgk_init_f_fields(aslb_lbgk* h, const double* rho, const double* u) {
   if (!u) return fail(ASLB_ERR_ARG, "aslb_lbgk_init_f_fields: velocity field required");
   const size_t L = (size_t)h->d.g.L;
   double *drho = nullptr, *du = nullptr;
-  ASLB_CUDA(cudaMalloc(&du, 3 * L * sizeof(double)));
-  ASLB_CUDA(cudaMemcpyAsync(du, u, 3 * L * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  if (rho) {
-    ASLB_CUDA(cudaMalloc(&drho, L * sizeof(double)));
-    ASLB_CUDA(cudaMemcpyAsync(drho, rho, L * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  }
+  // every path below frees both buffers: errors are collected, not returned early
+  cudaError_t e = cudaMalloc(&du, 3 * L * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(du, u, 3 * L * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess && rho) e = cudaMalloc(&drho, L * sizeof(double));
+  if (e == cudaSuccess && rho) e = cudaMemcpyAsync(drho, rho, L * sizeof(double), cudaMemcpyHostToDevice, h->stream);
   const double z[3] = {0, 0, 0};
-  cudaError_t e = launch_init_f(h->d, h->p, 1.0, z, drho, du, h->stream);
+  if (e == cudaSuccess) e = launch_init_f(h->d, h->p, 1.0, z, drho, du, h->stream);
   cudaError_t e2 = cudaStreamSynchronize(h->stream);
   cudaFree(du);
   cudaFree(drho);
@@ -796,69 +799,81 @@ int aslb_lbgk_get_kernel(aslb_lbgk* h) { return h ? h->d.variant : -1; }
 
 long long aslb_lbgk_steps(aslb_lbgk* h) { return h ? h->steps : -1; }
 
+namespace {
+// Staging buffer of one direction (L values of the macro type) for the
+// population and Cs^2 transfers: allocated at the first such transfer, kept
+// with the domain, so later reads and writes allocate nothing.
+int stage_buffer(aslb_lbgk* h, void** out) {
+  const size_t need = (size_t)h->d.g.L * macro_bytes(h->d.storage);
+  if (!h->stage) ASLB_CUDA(cudaMalloc(&h->stage, need));
+  *out = h->stage;
+  return ASLB_OK;
+}
+
+// Device -> host copy of `count` values of `mb` bytes into host_out (dtype
+// F32 / F64) at element offset `at`: straight into the caller's buffer when
+// the types agree (a pinned buffer then transfers at full speed), else through
+// a host copy and a conversion. Enqueued on the domain's stream; converting
+// copies synchronise it.
+cudaError_t copy_out(aslb_lbgk* h, const void* dev, size_t count, size_t mb, int dtype, void* host_out, size_t at,
+                     std::vector<char>& tmp) {
+  const bool direct = (mb == 4) == (dtype == ASLB_F32);
+  if (direct) return cudaMemcpyAsync((char*)host_out + at * mb, dev, count * mb, cudaMemcpyDeviceToHost, h->stream);
+  tmp.resize(count * mb);
+  cudaError_t e = cudaMemcpyAsync(tmp.data(), dev, count * mb, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return e;
+  if (mb == 4) {
+    const float* src = (const float*)tmp.data();
+    for (size_t i = 0; i < count; ++i) ((double*)host_out)[at + i] = src[i];
+  } else {
+    const double* src = (const double*)tmp.data();
+    for (size_t i = 0; i < count; ++i) ((float*)host_out)[at + i] = (float)src[i];
+  }
+  return cudaSuccess;
+}
+}  // namespace
+
 int aslb_lbgk_read(aslb_lbgk* h, int field, int dtype, void* host_out) {
   ASLB_CHECK_HANDLE(h);
   if (!host_out) return fail(ASLB_ERR_ARG, "aslb_lbgk_read: null output");
   if (dtype != ASLB_F32 && dtype != ASLB_F64) return fail(ASLB_ERR_ARG, "aslb_lbgk_read: dtype must be F32 or F64");
+  if (field != ASLB_FIELD_CS2 && field != ASLB_FIELD_RHO && field != ASLB_FIELD_VELOCITY && field != ASLB_FIELD_F)
+    return fail(ASLB_ERR_ARG, "aslb_lbgk_read: unknown field");
   const size_t L = (size_t)h->d.g.L;
   const size_t mb = field == ASLB_FIELD_CS2 ? sizeof(float) : macro_bytes(h->d.storage);
-  size_t count;
-  void* dev = nullptr;
-  bool own = false;
+  std::vector<char> tmp;
+  cudaError_t e = cudaSuccess;
   if (field == ASLB_FIELD_CS2) {
     if (h->closure != CL_MLP || !h->cs2_field)
       return fail(ASLB_ERR_STATE, "aslb_lbgk_read: the Cs^2 field exists with the learned closure only");
+    void* stage = nullptr;
+    if (int rc = stage_buffer(h, &stage)) return rc;
     if (mlp_due(h)) {  // the field the next step will use
       prepare_params(h);
-      cudaError_t e = launch_closure_field(h->d, h->p, h->mlp_dev, h->cs2_field, h->parity, h->stream);
+      e = launch_closure_field(h->d, h->p, h->mlp_dev, h->cs2_field, h->parity, h->stream);
       if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_read: ") + cudaGetErrorString(e));
       h->mlp_last = h->steps;
     }
-    count = L;
-    ASLB_CUDA(cudaMalloc(&dev, count * mb));
-    own = true;
-    cudaError_t e = launch_gather_cells(h->d.g, h->cs2_field, (float*)dev, h->stream);
-    if (e != cudaSuccess) {
-      cudaFree(dev);
-      return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_read: ") + cudaGetErrorString(e));
-    }
+    e = launch_gather_cells(h->d.g, h->cs2_field, (float*)stage, h->stream);
+    if (e == cudaSuccess) e = copy_out(h, stage, L, mb, dtype, host_out, 0, tmp);
   } else if (field == ASLB_FIELD_RHO) {
-    count = L;
-    dev = h->d.rho;
+    e = copy_out(h, h->d.rho, L, mb, dtype, host_out, 0, tmp);
   } else if (field == ASLB_FIELD_VELOCITY) {
-    count = 3 * L;
-    dev = h->d.u;
-  } else if (field == ASLB_FIELD_F) {
-    count = (size_t)h->d.q * L;
-    ASLB_CUDA(cudaMalloc(&dev, count * mb));
-    own = true;
-    prepare_params(h);
-    cudaError_t e = launch_export_f(h->d, h->p, h->parity, dev, h->stream);
-    if (e != cudaSuccess) {
-      cudaFree(dev);
-      return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_read: ") + cudaGetErrorString(e));
-    }
+    e = copy_out(h, h->d.u, 3 * L, mb, dtype, host_out, 0, tmp);
   } else {
-    return fail(ASLB_ERR_ARG, "aslb_lbgk_read: unknown field");
-  }
-  // Copy straight into the caller's buffer when the types agree (pinned
-  // buffers then transfer at full speed), through a host staging copy otherwise.
-  const bool direct = (mb == 4) == (dtype == ASLB_F32);
-  std::vector<char> tmp(direct ? 0 : count * mb);
-  void* dst = direct ? host_out : (void*)tmp.data();
-  cudaError_t e = cudaMemcpyAsync(dst, dev, count * mb, cudaMemcpyDeviceToHost, h->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-  if (own) cudaFree(dev);
-  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_read: ") + cudaGetErrorString(e));
-  if (!direct) {
-    if (mb == 4) {
-      const float* src = (const float*)tmp.data();
-      for (size_t i = 0; i < count; ++i) ((double*)host_out)[i] = src[i];
-    } else {
-      const double* src = (const double*)tmp.data();
-      for (size_t i = 0; i < count; ++i) ((float*)host_out)[i] = (float)src[i];
+    // one direction at a time through the staging buffer (stream order keeps
+    // each export behind the previous copy out of the same buffer)
+    void* stage = nullptr;
+    if (int rc = stage_buffer(h, &stage)) return rc;
+    prepare_params(h);
+    for (int i = 0; i < h->d.q && e == cudaSuccess; ++i) {
+      e = launch_export_f(h->d, h->p, h->parity, i, i + 1, stage, h->stream);
+      if (e == cudaSuccess) e = copy_out(h, stage, L, mb, dtype, host_out, (size_t)i * L, tmp);
     }
   }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_read: ") + cudaGetErrorString(e));
   return ASLB_OK;
 }
 
@@ -866,23 +881,31 @@ int aslb_lbgk_write(aslb_lbgk* h, int field, int dtype, const void* host_in) {
   ASLB_CHECK_HANDLE(h);
   if (field != ASLB_FIELD_F || !host_in) return fail(ASLB_ERR_ARG, "aslb_lbgk_write: only the F field is writable");
   if (dtype != ASLB_F32 && dtype != ASLB_F64) return fail(ASLB_ERR_ARG, "aslb_lbgk_write: dtype must be F32 or F64");
-  const size_t count = (size_t)h->d.q * h->d.g.L;
+  const size_t L = (size_t)h->d.g.L;
   const size_t mb = macro_bytes(h->d.storage);
   const bool direct = (mb == 4) == (dtype == ASLB_F32);
-  std::vector<char> tmp(direct ? 0 : count * mb);
-  if (!direct) {
-    if (mb == 4)
-      for (size_t i = 0; i < count; ++i) ((float*)tmp.data())[i] = (float)((const double*)host_in)[i];
-    else
-      for (size_t i = 0; i < count; ++i) ((double*)tmp.data())[i] = ((const float*)host_in)[i];
+  void* stage = nullptr;
+  if (int rc = stage_buffer(h, &stage)) return rc;
+  std::vector<char> tmp(direct ? 0 : L * mb);
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < h->d.q && e == cudaSuccess; ++i) {
+    const void* src;
+    if (direct) {
+      src = (const char*)host_in + (size_t)i * L * mb;
+    } else {
+      // the previous direction's copy reads tmp: wait for it before refilling
+      e = cudaStreamSynchronize(h->stream);
+      if (e != cudaSuccess) break;
+      if (mb == 4)
+        for (size_t k = 0; k < L; ++k) ((float*)tmp.data())[k] = (float)((const double*)host_in)[(size_t)i * L + k];
+      else
+        for (size_t k = 0; k < L; ++k) ((double*)tmp.data())[k] = ((const float*)host_in)[(size_t)i * L + k];
+      src = tmp.data();
+    }
+    e = cudaMemcpyAsync(stage, src, L * mb, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = launch_import_f(h->d, h->p, i, i + 1, stage, h->stream);
   }
-  void* dev = nullptr;
-  ASLB_CUDA(cudaMalloc(&dev, count * mb));
-  cudaError_t e = cudaMemcpyAsync(dev, direct ? host_in : (const void*)tmp.data(), count * mb,
-                                  cudaMemcpyHostToDevice, h->stream);
-  if (e == cudaSuccess) e = launch_import_f(h->d, h->p, dev, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-  cudaFree(dev);
   if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_write: ") + cudaGetErrorString(e));
   h->parity = 0;
   h->fresh = true;
@@ -1519,12 +1542,12 @@ int aslb_force_destroy(aslb_force* fc) {
 // ---- surface force without any allocation ---------------------------------
 //
 // For callers that cannot allocate device memory at the moment they need a
-// force: code running inside a stream capture or under an allocator that
-// forbids new device allocations, or an embedding runtime that hands out all
-// memory up front. aslb_force_compute allocates nothing per call either, but
-// its scratch rows come from cudaMalloc at aslb_force_create; this variant
-// takes the per-block partial sums and the final sums from one fixed array in
-// the library's own device memory instead.
+// force: a host program whose allocator forbids new device allocations after
+// set-up, or an embedding runtime that hands out all memory up front.
+// aslb_force_compute allocates nothing per call either, but its scratch rows
+// come from cudaMalloc at aslb_force_create; this variant takes the
+// per-block partial sums and the final sums from one fixed array in the
+// library's own device memory instead.
 
 }  // extern "C"
 
@@ -1537,8 +1560,10 @@ constexpr int kNoAllocForceCells = kNoAllocForceBlocks * 256;
 constexpr int kNoAllocScratch = kNoAllocForceBlocks * 6 + 8;
 static __device__ __align__(256) double g_force_scratch[kNoAllocScratch];
 // Device address of g_force_scratch per device (the name is only a host-side
-// stand-in in host code), looked up on the first call on each device.
-double* g_force_scratch_dev[64] = {nullptr};
+// stand-in in host code), looked up on the first call on each device; the
+// lock makes concurrent first calls from several host threads safe.
+std::atomic<double*> g_force_scratch_dev[64];
+std::mutex g_force_scratch_lock;
 }  // namespace
 
 extern "C" int aslb_force_compute_noalloc(aslb_force* fc, const double r0[3], double out6[6]) {
@@ -1555,12 +1580,15 @@ extern "C" int aslb_force_compute_noalloc(aslb_force* fc, const double r0[3], do
   if (dev != h->device)
     return fail(ASLB_ERR_STATE, "aslb_force_compute_noalloc: make the domain's device current first");
   if (dev < 0 || dev >= 64) return fail(ASLB_ERR_ARG, "aslb_force_compute_noalloc: device index out of range");
-  if (!g_force_scratch_dev[dev]) {
-    double* p = nullptr;
-    ASLB_CUDA(cudaGetSymbolAddress((void**)&p, g_force_scratch));
-    g_force_scratch_dev[dev] = p;
+  double* partials = g_force_scratch_dev[dev].load(std::memory_order_acquire);
+  if (!partials) {
+    std::lock_guard<std::mutex> lock(g_force_scratch_lock);
+    partials = g_force_scratch_dev[dev].load(std::memory_order_relaxed);
+    if (!partials) {
+      ASLB_CUDA(cudaGetSymbolAddress((void**)&partials, g_force_scratch));
+      g_force_scratch_dev[dev].store(partials, std::memory_order_release);
+    }
   }
-  double* partials = g_force_scratch_dev[dev];
   double* sums = partials + (size_t)kNoAllocForceBlocks * 6;
   // Every block writes its whole row of partial sums and the final kernel
   // overwrites the six sums, so nothing left by an earlier call is read.

@@ -39,8 +39,14 @@ extern "C" int aslb_geom_pack_spheres(int nx, int ny, int nz, double rmin, doubl
     vol += 4.0 / 3.0 * M_PI * r * r * r;
   }
   std::sort(rs.begin(), rs.end(), [](double a, double b) { return a > b; });
+  // Buckets at least 2 rmax wide, so every sphere that can overlap a
+  // candidate sits in the candidate's bucket or an adjacent one. Along a
+  // periodic x the buckets tile the period exactly (nbx whole buckets of
+  // width nx / nbx), so the adjacency also holds across the seam.
   const double bucket = 2.0 * rmax;
-  const int nbx = (int)std::ceil(nx / bucket), nby = (int)std::ceil(ny / bucket), nbz = (int)std::ceil(nz / bucket);
+  const int nbx = periodic_x ? std::max(1, (int)std::floor(nx / bucket)) : (int)std::ceil(nx / bucket);
+  const double bwx = periodic_x ? double(nx) / nbx : bucket;
+  const int nby = (int)std::ceil(ny / bucket), nbz = (int)std::ceil(nz / bucket);
   std::unordered_map<long long, std::vector<int>> grid;
   auto key = [&](int bx, int by, int bz) { return ((long long)bx * (nby + 2) + (by + 1)) * (nbz + 2) + (bz + 1); };
   int n = 0;
@@ -50,10 +56,12 @@ extern "C" int aslb_geom_pack_spheres(int nx, int ny, int nz, double rmin, doubl
     for (int a = 0; a < attempts; ++a) {
       const double cx = periodic_x ? rng.uniform(0, nx) : rng.uniform(r, nx - 1 - r);
       const double cy = rng.uniform(r, ny - 1 - r), cz = rng.uniform(r, nz - 1 - r);
-      const int bx = (int)std::floor(cx / bucket), by = (int)std::floor(cy / bucket), bz = (int)std::floor(cz / bucket);
+      const int bx = std::min((int)std::floor(cx / bwx), nbx - 1);
+      const int by = (int)std::floor(cy / bucket), bz = (int)std::floor(cz / bucket);
       bool ok = true;
       for (int ix = bx - 1; ix <= bx + 1 && ok; ++ix) {
         int jx = ix;
+        // (with fewer than three buckets a wrapped bucket is checked twice)
         if (periodic_x) jx = ((ix % nbx) + nbx) % nbx;
         for (int iy = by - 1; iy <= by + 1 && ok; ++iy)
           for (int iz = bz - 1; iz <= bz + 1 && ok; ++iz) {
@@ -72,8 +80,7 @@ extern "C" int aslb_geom_pack_spheres(int nx, int ny, int nz, double rmin, doubl
           }
       }
       if (ok) {
-        int kx = periodic_x ? ((bx % nbx) + nbx) % nbx : bx;
-        grid[key(kx, by, bz)].push_back(n);
+        grid[key(bx, by, bz)].push_back(n);
         centers[3 * n] = cx;
         centers[3 * n + 1] = cy;
         centers[3 * n + 2] = cz;

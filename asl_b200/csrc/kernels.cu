@@ -132,8 +132,8 @@ cudaError_t launch_init_f(const DomainDev& d, const StepParams& p, double rho0, 
 // Export f*_i(x) in ASL's layout. In representation B the value sits at the
 // cell it was pushed to; ghost cells whose target leaves the block read NaN.
 template <int Q, class S>
-__global__ void k_export_f(const S* __restrict__ F, const GridDesc g, const StepParams p, int parity,
-                           typename MacroT<S>::T* __restrict__ out) {
+__global__ void k_export_f(const S* __restrict__ F, const GridDesc g, const StepParams p, int parity, int i0,
+                           int i1, typename MacroT<S>::T* __restrict__ out) {
   using M = typename MacroT<S>::T;
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
@@ -142,25 +142,28 @@ __global__ void k_export_f(const S* __restrict__ F, const GridDesc g, const Step
   const long long a = aidx(g, x, y, z);
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
+    if (i < i0 || i >= i1) continue;
     const long long k = fstar_index<Q>(g, p.mask, parity, x, y, z, i);
-    out[(long long)i * g.L + a] = k < 0 ? M(NAN) : M(Store<S>::val(F + k, p.inv_scale));
+    out[(long long)(i - i0) * g.L + a] = k < 0 ? M(NAN) : M(Store<S>::val(F + k, p.inv_scale));
   }
 }
 
 template <int Q, class S>
-static cudaError_t export_impl(const DomainDev& d, const StepParams& p, int parity, void* out, cudaStream_t st) {
+static cudaError_t export_impl(const DomainDev& d, const StepParams& p, int parity, int i0, int i1, void* out,
+                               cudaStream_t st) {
   using M = typename MacroT<S>::T;
   dim3 block(128), grid((d.g.gz + 127) / 128, d.g.gy, d.g.gx);
-  k_export_f<Q, S><<<grid, block, 0, st>>>((const S*)d.F, d.g, p, parity, (M*)out);
+  k_export_f<Q, S><<<grid, block, 0, st>>>((const S*)d.F, d.g, p, parity, i0, i1, (M*)out);
   return cudaGetLastError();
 }
 
-cudaError_t launch_export_f(const DomainDev& d, const StepParams& p, int parity, void* out, cudaStream_t st) {
-  ASLB_DISPATCH(d, export_impl, d, p, parity, out, st)
+cudaError_t launch_export_f(const DomainDev& d, const StepParams& p, int parity, int i0, int i1, void* out,
+                            cudaStream_t st) {
+  ASLB_DISPATCH(d, export_impl, d, p, parity, i0, i1, out, st)
 }
 
 template <int Q, class S>
-__global__ void k_import_f(S* __restrict__ F, const GridDesc g, const StepParams p,
+__global__ void k_import_f(S* __restrict__ F, const GridDesc g, const StepParams p, int i0, int i1,
                            const typename MacroT<S>::T* __restrict__ in) {
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
@@ -169,20 +172,25 @@ __global__ void k_import_f(S* __restrict__ F, const GridDesc g, const StepParams
   const long long a = aidx(g, x, y, z);
   const long long s = sidx(g, x, y, z);
 #pragma unroll
-  for (int i = 0; i < Q; ++i)
-    Store<S>::set_val(F + (size_t)i * g.dstride + s, typename Store<S>::C(in[(long long)i * g.L + a]), p.scale);
+  for (int i = 0; i < Q; ++i) {
+    if (i < i0 || i >= i1) continue;
+    Store<S>::set_val(F + (size_t)i * g.dstride + s, typename Store<S>::C(in[(long long)(i - i0) * g.L + a]),
+                      p.scale);
+  }
 }
 
 template <int Q, class S>
-static cudaError_t import_impl(const DomainDev& d, const StepParams& p, const void* in, cudaStream_t st) {
+static cudaError_t import_impl(const DomainDev& d, const StepParams& p, int i0, int i1, const void* in,
+                               cudaStream_t st) {
   using M = typename MacroT<S>::T;
   dim3 block(128), grid((d.g.gz + 127) / 128, d.g.gy, d.g.gx);
-  k_import_f<Q, S><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (const M*)in);
+  k_import_f<Q, S><<<grid, block, 0, st>>>((S*)d.F, d.g, p, i0, i1, (const M*)in);
   return cudaGetLastError();
 }
 
-cudaError_t launch_import_f(const DomainDev& d, const StepParams& p, const void* in, cudaStream_t st) {
-  ASLB_DISPATCH(d, import_impl, d, p, in, st)
+cudaError_t launch_import_f(const DomainDev& d, const StepParams& p, int i0, int i1, const void* in,
+                            cudaStream_t st) {
+  ASLB_DISPATCH(d, import_impl, d, p, i0, i1, in, st)
 }
 
 // ---------------------------------------------------------------------------

@@ -43,10 +43,12 @@ cudaError_t launch_step(const DomainDev& d, const StepParams& p, int closure, in
 // rho_field / u_field: device arrays in ASL layout (double) or null for constants.
 cudaError_t launch_init_f(const DomainDev& d, const StepParams& p, double rho0, const double* u0,
                           const double* rho_field, const double* u_field, cudaStream_t st);
-// Copy populations to / from ASL's layout (f_i at i*L + ghosted index), values
-// in the macro type (float or double).
-cudaError_t launch_export_f(const DomainDev& d, const StepParams& p, int parity, void* out, cudaStream_t st);
-cudaError_t launch_import_f(const DomainDev& d, const StepParams& p, const void* in, cudaStream_t st);
+// Copy directions [i0, i1) of the populations to / from ASL's layout (f_i at
+// (i - i0)*L + ghosted index), values in the macro type (float or double).
+cudaError_t launch_export_f(const DomainDev& d, const StepParams& p, int parity, int i0, int i1, void* out,
+                            cudaStream_t st);
+cudaError_t launch_import_f(const DomainDev& d, const StepParams& p, int i0, int i1, const void* in,
+                            cudaStream_t st);
 // Boundary links: anchors (x, y, z, direction mask) in ghosted coordinates.
 // Conditions on the rho / u output fields (visualisation): guard cells with
 // their fluid-neighbour masks, per-cell weights for the rho condition.

@@ -75,10 +75,17 @@ def channel_cylinder(size=(128, 64, 64), radius=8.0, center=(32.0, 32.0), u_in=0
 
 
 def porous_channel(size=(512, 256, 256), rmin=4.0, rmax=12.0, solid_fraction=0.4, g=1e-6, tau=0.6, steps=5000,
-                   seed=BASE_SEED + 2) -> Workload:
+                   seed=BASE_SEED + 2, packer=None) -> Workload:
+    """``packer``: a function with the signature of geometry.pack_spheres'
+    first six arguments returning (centers, radii), used instead of the
+    library's packer (a CPU-only caller that must not load the CUDA library
+    passes an equivalent one; the spheres are the same)."""
     from .lbgk import Block
     block = Block(size, 1.0)
-    pack = G.pack_spheres(size, rmin, rmax, solid_fraction, seed, periodic_x=True)
+    if packer is None:
+        pack = G.pack_spheres(size, rmin, rmax, solid_fraction, seed, periodic_x=True)
+    else:
+        pack = G.SpherePack(*packer(size, rmin, rmax, solid_fraction, seed, True))
     m = G.rasterize_spheres(block, pack, periodic_x=True)
     nu = (tau - 0.5) / 3.0
     solid = float((m[1:-1, 1:-1, 1:-1] <= 0).mean())

@@ -176,25 +176,61 @@ def cpu_baseline(w, steps: int, warm: int = 2):
                       f"workload, FP32, {threads} OpenMP threads"}
 
 
+def repo_libraries():
+    """Shared libraries of this repository mapped into the process."""
+    out = set()
+    try:
+        for line in Path("/proc/self/maps").read_text().splitlines():
+            path = line.split()[-1] if len(line.split()) >= 6 else ""
+            if path.endswith(".so") and path.startswith(str(ROOT)):
+                out.add(str(Path(path).relative_to(ROOT)))
+    except OSError:
+        pass
+    return sorted(out)
+
+
 def run_reference(args):
+    """The CPU restatement of the reference's LBGK on the host cores. The
+    workload is built with the oracle's sphere packer: nothing of the CUDA
+    library is loaded (the line lists the repository libraries the process
+    mapped)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
+    from oracle import oracle as O
     from asl_b200 import workloads as W
-    w = W.porous_channel(size=parse_size(args.size))
+    w = W.porous_channel(size=parse_size(args.size), packer=O.pack_spheres)
     steps = max(1, min(args.steps, args.cpu_steps))
-    cb = cpu_baseline(w, steps, warm=max(0, min(args.warmup, 2)))
+    warm = max(0, min(args.warmup, 10))
+    cb = cpu_baseline(w, steps, warm=warm)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "MLUPS", "n_gpus": args.gpus,
-            "steps": steps, "warmup": min(args.warmup, 2), "ms_per_step": w.cells / (cb["value"] * 1e6) * 1e3,
+            "steps": steps, "warmup": warm, "ms_per_step": w.cells / (cb["value"] * 1e6) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded random spheres)",
             "config": {"workload": w.name, "lattice": "D3Q19", "cells": w.cells, "storage": "f32",
                        "implementation": "CPU restatement of the reference LBGK (oracle/lbgk_oracle.cpp); "
                                          "the reference's OpenCL build is unavailable on this box"},
             "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "repo_libraries_loaded": repo_libraries()}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def cpu_baseline_subprocess(args):
+    """The reference arm's CPU measurement, run in a fresh process before this
+    process touches the GPU (no CUDA context, no clock sampler, the host's
+    threads free), so that the in-arm baseline and the reference arm measure
+    the same thing the same way."""
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR",
+                                                            "MASTER_PORT")}
+    cmd = [sys.executable, str(Path(__file__).resolve()), "--impl", "reference", "--size", args.size,
+           "--steps", str(args.cpu_steps), "--warmup", "2", "--cpu-steps", str(args.cpu_steps)]
+    r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=900)
+    for line in reversed(r.stdout.splitlines()):
+        if line.startswith("{"):
+            return json.loads(line)["cpu_baseline"]
+    raise RuntimeError("CPU baseline run failed: " + (r.stderr or r.stdout)[-2000:])
 
 
 # ---------------------------------------------------------------------------
@@ -384,9 +420,12 @@ def batch_run(W, n: int, steps: int, peak: float):
 
 
 def run_ours(args):
+    rank, world, local = dist_env()
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline_subprocess(args)
     import numpy as np
     import torch
-    rank, world, local = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
@@ -529,10 +568,6 @@ def run_ours(args):
             "bytes_per_cell": bpc, "cells_per_launch": w.cells, "kernel_ms": tk * 1e3,
             "note": "algorithmic bytes: read + write of 19 populations per cell; the 8-byte fused-link "
                     "mask per cell is overhead and not counted"}
-
-    cb = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline(w, args.cpu_steps)
 
     if rank == 0:
         line = {"metric": METRIC, "value": head["value"], "unit": "MLUPS", "n_gpus": world, "steps": K,

@@ -314,14 +314,17 @@ int aslb_force_compute(aslb_force* fc, const double r0[3], float* field_host, do
 int aslb_force_destroy(aslb_force* fc);
 /* No counterpart in the reference. The same totals as aslb_force_compute
  * (without the per-cell field) for callers that cannot allocate device memory
- * when they need them, e.g. inside a stream capture or under an allocator
- * that forbids new allocations: it calls no cudaMalloc or cudaFree and keeps
- * its partial sums in a fixed array of the library's device memory (196,672
- * bytes per device, held until exit). Lists of more than 1,048,576 force
- * cells are rejected with ASLB_ERR_ARG. The domain's device must be current;
- * the first call on each device looks up the array's address, so make that
- * first call before any stream capture. All calls share the array: calls
- * whose work overlaps on the GPU (different streams) race. Synchronises. */
+ * when they need them: a host program whose device memory is managed by an
+ * allocator that forbids new allocations after set-up, or an embedding
+ * runtime that hands out all device memory up front. It calls no cudaMalloc
+ * or cudaFree and keeps its partial sums in a fixed array of the library's
+ * device memory (196,672 bytes per device, held until exit). Lists of more
+ * than 1,048,576 force cells are rejected with ASLB_ERR_ARG. The domain's
+ * device must be current; the first call on each device looks up the
+ * array's device address (a lookup, not an allocation; safe from several
+ * host threads). All calls share the array and each call overwrites what the
+ * previous one left there: calls whose work overlaps on the GPU (different
+ * streams) race. Synchronises the domain's stream. */
 int aslb_force_compute_noalloc(aslb_force* fc, const double r0[3], double out6[6]);
 
 /* ---- surface flux -------------------------------------------------------- */

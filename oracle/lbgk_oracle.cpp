@@ -895,4 +895,92 @@ double orc_sum(const double* a, long n) {
   return s;
 }
 
+// Workload geometry for the CPU side of the benchmark: the porous channel's
+// seeded random sequential addition of non-overlapping spheres, so that the
+// CPU runs build their workload without the CUDA library. Same draws as the
+// library's aslb_geom_pack_spheres (splitmix64 stream, uniform doubles from
+// the top 53 bits, radii drawn until 1.25x the target volume and placed
+// largest first, up to `attempts` centres per radius), with its own neighbour
+// search: a dense grid of cells at least 2 rmax wide in every axis (the grid
+// tiles a periodic x exactly), so the accept / reject decisions -- and the
+// spheres -- are the same. A CPU test checks the two bit for bit.
+int orc_pack_spheres(int nx, int ny, int nz, double rmin, double rmax, double solid_fraction,
+                     unsigned long long seed, int periodic_x, int attempts, int max_spheres, double* centers,
+                     double* radii, int* count) {
+  if (!centers || !radii || !count || nx < 1 || ny < 1 || nz < 1 || !(rmin > 0) || rmax < rmin || max_spheres < 1)
+    return -1;
+  uint64_t state = seed;
+  auto draw = [&](double a, double b) {
+    state += 0x9e3779b97f4a7c15ull;
+    uint64_t z = state;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    return a + (b - a) * (double)(z >> 11) * (1.0 / 9007199254740992.0);
+  };
+  const double target = solid_fraction * (double(nx) * ny * nz);
+  std::vector<double> rs;
+  double vol = 0.0;
+  while (vol < target * 1.25 && (int)rs.size() < 4 * max_spheres) {
+    const double r = draw(rmin, rmax);
+    rs.push_back(r);
+    vol += 4.0 / 3.0 * M_PI * r * r * r;
+  }
+  std::sort(rs.begin(), rs.end(), [](double a, double b) { return a > b; });
+  const int N[3] = {nx, ny, nz};
+  int nc[3];
+  double cw[3];
+  for (int a = 0; a < 3; ++a) {
+    nc[a] = std::max(1, (int)std::floor(N[a] / (2.0 * rmax)));
+    cw[a] = double(N[a]) / nc[a];
+  }
+  std::vector<std::vector<int>> cells((size_t)nc[0] * nc[1] * nc[2]);
+  auto cell_of = [&](double v, int a) { return std::min(std::max((int)std::floor(v / cw[a]), 0), nc[a] - 1); };
+  int n = 0;
+  double placed = 0.0;
+  for (double r : rs) {
+    if (placed >= target || n >= max_spheres) break;
+    for (int t = 0; t < attempts; ++t) {
+      const double cx = periodic_x ? draw(0, nx) : draw(r, nx - 1 - r);
+      const double cy = draw(r, ny - 1 - r), cz = draw(r, nz - 1 - r);
+      const int c0[3] = {cell_of(cx, 0), cell_of(cy, 1), cell_of(cz, 2)};
+      bool free = true;
+      for (int i = -1; i <= 1 && free; ++i) {
+        int ix = c0[0] + i;
+        if (periodic_x) ix = (ix + nc[0]) % nc[0];
+        else if (ix < 0 || ix >= nc[0]) continue;
+        for (int j = -1; j <= 1 && free; ++j) {
+          const int iy = c0[1] + j;
+          if (iy < 0 || iy >= nc[1]) continue;
+          for (int k = -1; k <= 1 && free; ++k) {
+            const int iz = c0[2] + k;
+            if (iz < 0 || iz >= nc[2]) continue;
+            for (int o : cells[((size_t)ix * nc[1] + iy) * nc[2] + iz]) {
+              double dx = centers[3 * o] - cx;
+              const double dy = centers[3 * o + 1] - cy, dz = centers[3 * o + 2] - cz;
+              if (periodic_x) dx -= nx * std::nearbyint(dx / nx);
+              const double rr = radii[o] + r;
+              if (dx * dx + dy * dy + dz * dz < rr * rr) {
+                free = false;
+                break;
+              }
+            }
+          }
+        }
+      }
+      if (!free) continue;
+      cells[((size_t)c0[0] * nc[1] + c0[1]) * nc[2] + c0[2]].push_back(n);
+      centers[3 * n] = cx;
+      centers[3 * n + 1] = cy;
+      centers[3 * n + 2] = cz;
+      radii[n] = r;
+      ++n;
+      placed += 4.0 / 3.0 * M_PI * r * r * r;
+      break;
+    }
+  }
+  *count = n;
+  return 0;
+}
+
 }  // extern "C"

@@ -72,6 +72,8 @@ def load():
             "orc_get_u": (None, [vp, pd]),
             "orc_lattice": (None, [C.c_int, C.POINTER(C.c_int), pd, C.POINTER(C.c_int)]),
             "orc_sum": (d, [pd, C.c_long]),
+            "orc_pack_spheres": (C.c_int, [C.c_int, C.c_int, C.c_int, d, d, d, C.c_ulonglong, C.c_int, C.c_int,
+                                           C.c_int, pd, pd, C.POINTER(C.c_int)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -207,3 +209,22 @@ class Oracle:
 def reduction_sum(a) -> float:
     a = np.ascontiguousarray(a, dtype=np.float64)
     return float(load().orc_sum(_dp(a), a.size))
+
+
+def pack_spheres(size, rmin: float, rmax: float, solid_fraction: float, seed: int, periodic_x: bool = True,
+                 attempts: int = 400):
+    """The porous channel's seeded sphere packing computed by the oracle
+    library (the same spheres as the CUDA library's aslb_geom_pack_spheres),
+    for CPU runs that must not load the product library. Returns
+    (centers (n, 3), radii (n,))."""
+    import math
+    nx, ny, nz = (int(v) for v in size)
+    cap = int(solid_fraction * nx * ny * nz / (4.0 / 3.0 * math.pi * rmin ** 3)) + 16
+    centers = np.zeros((cap, 3))
+    radii = np.zeros(cap)
+    n = C.c_int(0)
+    rc = load().orc_pack_spheres(nx, ny, nz, float(rmin), float(rmax), float(solid_fraction), int(seed),
+                                 int(bool(periodic_x)), int(attempts), cap, _dp(centers), _dp(radii), C.byref(n))
+    if rc != 0:
+        raise ValueError("orc_pack_spheres: bad arguments")
+    return centers[:n.value].copy(), radii[:n.value].copy()

@@ -55,6 +55,34 @@ def test_sphere_pack_is_seeded_and_non_overlapping():
     assert vol >= 0.3
 
 
+def _assert_no_overlap(c, r, nx):
+    d = c[:, None, :] - c[None, :, :]
+    d[..., 0] -= nx * np.round(d[..., 0] / nx)
+    dist = np.sqrt((d ** 2).sum(-1))
+    np.fill_diagonal(dist, np.inf)
+    assert (dist >= (r[:, None] + r[None, :]) - 1e-9).all()
+
+
+def test_sphere_pack_no_overlap_across_the_periodic_seam():
+    # 100 is not a multiple of the 2 rmax = 16 bucket width: spheres near
+    # x = 0 and x = 100 are neighbours across the seam
+    for seed in range(6):
+        p = G.pack_spheres((100, 40, 40), 4, 8, 0.35, seed=seed)
+        _assert_no_overlap(p.centers, p.radii, 100)
+
+
+def test_sphere_pack_matches_the_oracle_packer():
+    """The CPU benchmark runs build the porous channel with the oracle's
+    packer (no CUDA library): it must give the library's spheres bit for bit."""
+    from oracle import oracle as O
+    for size, per, seed in [((100, 40, 40), True, 1), ((96, 48, 48), True, 5), ((90, 40, 50), False, 2),
+                            ((256, 128, 128), True, 20261205)]:
+        p = G.pack_spheres(size, 4, 12, 0.4, seed=seed, periodic_x=per)
+        c, r = O.pack_spheres(size, 4, 12, 0.4, seed, per)
+        assert len(r) > 0
+        assert np.array_equal(p.centers, c) and np.array_equal(p.radii, r)
+
+
 def test_rasterized_spheres_match_direct_union():
     b = Block((40, 20, 20))
     p = G.pack_spheres((40, 20, 20), 2, 4, 0.2, seed=3)

@@ -1,8 +1,10 @@
 """GPU tests of aslb_force_compute_noalloc, the surface-force entry point that
 allocates nothing, for callers that cannot allocate device memory when they
-ask for a force (inside a stream capture, under an allocator that forbids new
-allocations). It must give the same totals as aslb_force_compute, call after
-call, and refuse force-cell lists larger than its fixed scratch array.
+ask for a force (a program whose allocator forbids new device allocations
+after set-up, or a runtime that hands out all device memory up front). It
+must give the same totals as aslb_force_compute, call after call, refuse
+force-cell lists larger than its fixed scratch array, and refuse objects it
+cannot serve without touching that array.
 
 This file is collected last so that a run stopping at the first failure has
 already run every other test."""
@@ -46,3 +48,23 @@ def test_noalloc_force_rejects_lists_beyond_its_scratch(gpu):
     with pytest.raises(L.ASLError, match="scratch limit"):
         _noalloc(gpu, force, (0.0, 0.0, 0.0))
     assert np.isfinite(force.execute()).all()  # the allocating path still serves it
+
+
+def test_noalloc_force_refuses_flux_objects_and_detached_forces(gpu):
+    w = W.channel_cylinder(size=(32, 16, 16), radius=3.0, center=(10.0, 8.0), steps=0)
+    lb, bcs = W.build_lbgk(w)
+    lb.run(3, bcs)
+    flux = C.c_void_p()
+    L.check(gpu.aslb_flux_create(lb.h, w.map.ctypes.data_as(L._pf), C.byref(flux)), "aslb_flux_create")
+    out = (C.c_double * 6)()
+    assert gpu.aslb_force_compute_noalloc(flux, L.dvec((0.0, 0.0, 0.0)), out) == -1  # ASLB_ERR_ARG
+    assert b"flux object" in gpu.aslb_last_error()
+    gpu.aslb_flux_destroy(flux)
+    assert gpu.aslb_force_compute_noalloc(None, L.dvec((0.0, 0.0, 0.0)), out) == -1
+    # a force object whose domain was destroyed is detached: ASLB_ERR_STATE, no launch
+    force = C.c_void_p()
+    L.check(gpu.aslb_force_create(lb.h, w.map.ctypes.data_as(L._pf), C.byref(force)), "aslb_force_create")
+    lb.close()
+    assert gpu.aslb_force_compute_noalloc(force, L.dvec((0.0, 0.0, 0.0)), out) == -4  # ASLB_ERR_STATE
+    assert b"destroyed" in gpu.aslb_last_error()
+    gpu.aslb_force_destroy(force)
