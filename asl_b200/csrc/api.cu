@@ -166,6 +166,16 @@ void prepare_params(aslb_lbgk* h) {
   h->p.cs2 = h->cs2_field;
   h->p.mask = h->fresh ? nullptr : h->mask_dev;
   h->p.mask32 = h->fresh ? nullptr : h->mask32_dev;
+  const GridDesc& g = h->d.g;
+  for (int i = 0; i < h->d.q; ++i) {
+    const int j = lattice_inv(h->d.q, i);
+    const long long ct = lattice_c(h->d.q, i, 0) * g.plane + lattice_c(h->d.q, i, 1) * (long long)g.pitch +
+                         lattice_c(h->d.q, i, 2);
+    h->p.slot[0][i] = (unsigned)(i * g.dstride - ct);
+    h->p.slot[1][i] = (unsigned)(i * g.dstride);
+    h->p.slot[2][i] = (unsigned)(j * g.dstride + ct);
+    h->p.slot[3][i] = (unsigned)(j * g.dstride);
+  }
 }
 
 bool mlp_due(const aslb_lbgk* h) {

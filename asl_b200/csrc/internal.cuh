@@ -76,12 +76,21 @@ struct StepParams {
   // so it is read by bounce-back from the cell's own outgoing population.
   // y (elide): bit k = the cell's outgoing population k lands in the incoming
   // slot of a fused link, which the condition would overwrite: the slot keeps
-  // its bits (FP32/FP64 skip the store; FP16 stores back what it holds, so
-  // that warps write whole sectors).
+  // its bits (the store is skipped).
   const uint2* mask;
   // The same links in one word per cell, when no cell has both kinds: bit 31
   // set = the low bits are elide bits, clear = bounce bits (or null).
   const uint32_t* mask32;
+  // Element offsets of the population slots of direction i relative to a
+  // cell's storage index s, for cells whose neighbours do not wrap across a
+  // periodic face (with ds = dstride and t = (plane, pitch, 1)):
+  //   slot[0][i] = i ds - c_i.t       F[i][x - c_i]      (pull)
+  //   slot[1][i] = i ds                F[i][x]            (own)
+  //   slot[2][i] = inv(i) ds + c_i.t   F[inv i][x + c_i]  (push)
+  //   slot[3][i] = inv(i) ds           F[inv i][x]        (own, opposite)
+  // Modulo 2^32: s + slot is the slot's index (Q * dstride < 2^32). Set on
+  // the host from the domain's grid, so a population address is one add.
+  unsigned slot[4][27];
 };
 
 // ---- storage formats -------------------------------------------------------

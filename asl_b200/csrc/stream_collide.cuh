@@ -2,6 +2,7 @@
 // launch helpers. Instantiated per lattice and storage in step_q<Q>_<type>.cu
 // so the instantiations compile in parallel.
 #pragma once
+#include <algorithm>
 #include <type_traits>
 #include "kernels.h"
 #include "collide.cuh"
@@ -52,25 +53,20 @@ struct StepOccupancy {
                                     : (CL == CL_NONE ? (FUSED ? 4 : (Q == 27 ? 2 : 3)) : 3);
 };
 
-// Store one outgoing population. An elided slot keeps its bits: FP32/FP64
-// skip the store; 2-byte storage writes back what the slot holds (bits no
-// other cell writes this step), so a warp's store covers whole sectors
-// instead of leaving partial ones that HBM must read to merge.
+// Store one outgoing population unless its slot is elided (the slot keeps its
+// bits). In the AA pattern a cell writes exactly the slots it read moments
+// before, so the lines are still in L2 and a warp's partial store merges there
+// without an HBM read.
 template <class S>
 __device__ __forceinline__ void store_slot(S* __restrict__ slot, typename Store<S>::C v, bool elided,
                                            const StepParams& p) {
-  if (sizeof(S) > 2) {
-    if (!elided) *slot = Store<S>::encode(v, p);
-  } else {
-    S out = Store<S>::encode(v, p);
-    if (elided) out = *slot;
-    *slot = out;
-  }
+  if (!elided) *slot = Store<S>::encode(v, p);
 }
 
 // Gather the Q incoming populations of cell s. MASKED: bounce bits select
 // the bounce-back slot (this cell's own outgoing population: the upstream and
-// own slots swap roles between representations).
+// own slots swap roles between representations). Offsets from the periodic
+// wrap (nb_offsets): the slow path of cells on a periodic face.
 template <int Q, class S, bool ODD, bool MASKED>
 __device__ __forceinline__ void cell_load(const S* __restrict__ F, unsigned ds, unsigned s, const int (&ox)[3],
                                           const int (&oy)[3], const int (&oz)[3], uint32_t bounce,
@@ -92,18 +88,28 @@ __device__ __forceinline__ void cell_load(const S* __restrict__ F, unsigned ds, 
   }
 }
 
-// Collide cell (x, y, z) at storage index s, write rho / u when asked, and
-// store the outgoing populations (elide bits keep the slot, store_slot).
-template <int Q, class S, int CL, bool ODD, bool MASKED>
-__device__ __forceinline__ void cell_finish(S* __restrict__ F, const GridDesc& g, const StepParams& p,
-                                            typename MacroT<S>::T* __restrict__ rho_out,
-                                            typename MacroT<S>::T* __restrict__ u_out, int x, int y, int z,
-                                            unsigned s, const int (&ox)[3], const int (&oy)[3], const int (&oz)[3],
-                                            uint32_t elide, typename Store<S>::C (&f)[Q],
-                                            typename Store<S>::C om0) {
-  using Lt = Lattice<Q>;
+// The same gather for a cell whose neighbours do not wrap: every slot is the
+// cell's index plus a precomputed offset (p.slot).
+template <int Q, class S, bool ODD, bool MASKED>
+__device__ __forceinline__ void cell_load_flat(const S* __restrict__ F, unsigned s, const StepParams& p,
+                                               uint32_t bounce, typename Store<S>::C (&f)[Q]) {
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const bool b = MASKED && ((bounce >> i) & 1u);
+    // ODD: pull, or the opposite own slot when bounced; EVEN: the reverse
+    const unsigned off = (ODD != b) ? p.slot[0][i] : p.slot[3][i];
+    f[i] = Store<S>::load_c(F + (s + off));
+  }
+}
+
+// Collide cell (x, y, z) at storage index s and write rho / u when asked;
+// f becomes the outgoing populations.
+template <int Q, class S, int CL>
+__device__ __forceinline__ void cell_collide(const GridDesc& g, const StepParams& p,
+                                             typename MacroT<S>::T* __restrict__ rho_out,
+                                             typename MacroT<S>::T* __restrict__ u_out, int x, int y, int z,
+                                             unsigned s, typename Store<S>::C (&f)[Q], typename Store<S>::C om0) {
   using C = typename Store<S>::C;
-  const unsigned ds = (unsigned)g.dstride;
   C rho, u[3];
   const C cs2 = CL == CL_MLP ? C(p.cs2[s]) : C(0);
   collide_cell<Q, C, CL, Store<S>::kDev>(f, p, om0, cs2, rho, u);
@@ -116,6 +122,14 @@ __device__ __forceinline__ void cell_finish(S* __restrict__ F, const GridDesc& g
       u_out[2 * g.L + a] = u[2];
     }
   }
+}
+
+// Store the outgoing populations (elide bits keep the slot), wrap-aware.
+template <int Q, class S, bool ODD, bool MASKED>
+__device__ __forceinline__ void cell_store(S* __restrict__ F, const StepParams& p, unsigned ds, unsigned s,
+                                           const int (&ox)[3], const int (&oy)[3], const int (&oz)[3],
+                                           uint32_t elide, const typename Store<S>::C (&f)[Q]) {
+  using Lt = Lattice<Q>;
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
     unsigned idx;
@@ -125,6 +139,129 @@ __device__ __forceinline__ void cell_finish(S* __restrict__ F, const GridDesc& g
       idx = (unsigned)i * ds + s;
     store_slot<S>(F + idx, f[i], MASKED && ((elide >> i) & 1u), p);
   }
+}
+
+// s, seen by the compiler as computed after v: addresses derived from the
+// result cannot be hoisted above the collision that produced v (hoisted, the
+// Q store addresses of a cell would stay live across it and spill).
+__device__ __forceinline__ unsigned after(unsigned s, float v) {
+  asm volatile("" : "+r"(s) : "f"(v));
+  return s;
+}
+__device__ __forceinline__ unsigned after(unsigned s, double v) {
+  asm volatile("" : "+r"(s) : "d"(v));
+  return s;
+}
+
+// The same stores for a cell whose neighbours do not wrap (p.slot).
+template <int Q, class S, bool ODD, bool MASKED>
+__device__ __forceinline__ void cell_store_flat(S* __restrict__ F, const StepParams& p, unsigned s, uint32_t elide,
+                                                const typename Store<S>::C (&f)[Q]) {
+  const unsigned sl = after(s, f[0]);
+#pragma unroll
+  for (int i = 0; i < Q; ++i)
+    store_slot<S>(F + (sl + (ODD ? p.slot[2][i] : p.slot[1][i])), f[i], MASKED && ((elide >> i) & 1u), p);
+}
+
+// Collision and wrap-aware stores of one cell (the batched step's form).
+template <int Q, class S, int CL, bool ODD, bool MASKED>
+__device__ __forceinline__ void cell_finish(S* __restrict__ F, const GridDesc& g, const StepParams& p,
+                                            typename MacroT<S>::T* __restrict__ rho_out,
+                                            typename MacroT<S>::T* __restrict__ u_out, int x, int y, int z,
+                                            unsigned s, const int (&ox)[3], const int (&oy)[3], const int (&oz)[3],
+                                            uint32_t elide, typename Store<S>::C (&f)[Q],
+                                            typename Store<S>::C om0) {
+  cell_collide<Q, S, CL>(g, p, rho_out, u_out, x, y, z, s, f, om0);
+  cell_store<Q, S, ODD, MASKED>(F, p, (unsigned)g.dstride, s, ox, oy, oz, elide, f);
+}
+
+// Whether any neighbour of a cell with coordinate v on a periodic axis of n
+// interior cells wraps to the opposite face.
+__device__ __forceinline__ bool wraps(int periodic_bit, int v, int n) { return periodic_bit && (v == 1 || v == n); }
+
+// ---------------------------------------------------------------------------
+// Cells on periodic faces, whose neighbours wrap to the opposite face, are
+// skipped by the main blocks of a stream-collide launch (by their loop range,
+// so the main loop has no branch) and advanced by extra blocks of the same
+// launch, one cell per thread with the wrap-aware offsets (disjoint cells:
+// the AA update of a cell touches only its own slots). The face cells lie on
+// up to eight planes: the two faces of every periodic axis and, with the
+// two-cells-per-thread kernel (which skips both cells of a pair when either
+// wraps), the planes of the z partners of the skipped pairs. A cell on
+// several planes belongs to the first that holds it. The face blocks come
+// first in the grid (blockIdx.z < fz), so they run alongside the main blocks
+// instead of after them.
+struct FaceWork {
+  int n;          // planes
+  int axis[8];
+  int coord[8];
+  int start[9];   // prefix sums of the planes' cell counts
+  int fz;         // grid z-slices of face blocks
+};
+
+template <int Q, class S, int CL, bool ODD, bool FUSED>
+__device__ __forceinline__ void face_cell(S* __restrict__ F, const GridDesc& g, const StepParams& p,
+                                          const FaceWork& fw, typename MacroT<S>::T* __restrict__ rho_out,
+                                          typename MacroT<S>::T* __restrict__ u_out) {
+  using C = typename Store<S>::C;
+  const int threads = blockDim.x * blockDim.y;
+  const long long blk = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  const long long c = blk * threads + threadIdx.y * blockDim.x + threadIdx.x;
+  if (c >= fw.start[fw.n]) return;
+  int k = 0;
+  while (c >= fw.start[k + 1]) ++k;
+  const int r = (int)(c - fw.start[k]);
+  const int axis = fw.axis[k];
+  // in-plane coordinates: the two other axes in order
+  const int nu = axis == 0 ? g.ny : g.nx;
+  const int nv = axis == 2 ? g.ny : g.nz;
+  (void)nu;
+  const int u = r / nv + 1, v = r % nv + 1;
+  const int x = axis == 0 ? fw.coord[k] : u;
+  const int y = axis == 1 ? fw.coord[k] : (axis == 0 ? u : v);
+  const int z = axis == 2 ? fw.coord[k] : v;
+  for (int j = 0; j < k; ++j)
+    if ((fw.axis[j] == 0 ? x : (fw.axis[j] == 1 ? y : z)) == fw.coord[j]) return;
+  const unsigned s = (unsigned)sidx(g, x, y, z);
+  uint2 m = make_uint2(0u, 0u);
+  if (FUSED) m = p.mask[s];
+  int ox[3], oy[3], oz[3];
+  nb_offsets(g, x, y, z, ox, oy, oz);
+  C f[Q];
+  cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, s, ox, oy, oz, m.x, f);
+  cell_collide<Q, S, CL>(g, p, rho_out, u_out, x, y, z, s, f, step_omega<C>(p));
+  cell_store<Q, S, ODD, FUSED>(F, p, (unsigned)g.dstride, s, ox, oy, oz, m.y, f);
+}
+
+// The face planes of a domain and the grid z-slices their cells need with
+// blocks of `threads` threads on a gx x gy grid face. paired: the main
+// kernel is the two-cells-per-thread kernel, whose pairs are (z, z + 32) for
+// z - 1 mod 64 < 32: with a periodic z it also skips cell 33 (partner of
+// z = 1) and, when nz is the second cell of its pair, cell nz - 32.
+inline FaceWork face_work(const GridDesc& g, bool paired, int threads, int gx, int gy) {
+  FaceWork fw{};
+  const int n[3] = {g.nx, g.ny, g.nz};
+  auto add = [&](int a, int c) {
+    for (int j = 0; j < fw.n; ++j)
+      if (fw.axis[j] == a && fw.coord[j] == c) return;
+    fw.axis[fw.n] = a;
+    fw.coord[fw.n] = c;
+    const int cells = (a == 0 ? g.ny * g.nz : (a == 1 ? g.nx * g.nz : g.nx * g.ny));
+    fw.start[fw.n + 1] = fw.start[fw.n] + cells;
+    ++fw.n;
+  };
+  for (int a = 0; a < 3; ++a)
+    if ((g.periodic >> a) & 1) {
+      add(a, 1);
+      add(a, n[a]);
+    }
+  if (paired && (g.periodic & 4)) {
+    if (g.nz >= 33) add(2, 33);
+    if ((g.nz - 1) % 64 >= 32) add(2, g.nz - 32);
+  }
+  const long long per_slice = (long long)threads * gx * gy;
+  fw.fz = (int)((fw.start[fw.n] + per_slice - 1) / per_slice);
+  return fw;
 }
 
 // ---------------------------------------------------------------------------
@@ -139,14 +276,27 @@ __device__ __forceinline__ void cell_finish(S* __restrict__ F, const GridDesc& g
 constexpr int kOnePlanes = 4;
 template <int Q, class S, int CL, bool ODD, bool FUSED>
 __global__ void __launch_bounds__(256, StepOccupancy<Q, S, CL, FUSED>::blocks)
-    k_stream_collide(S* __restrict__ F, const GridDesc g, const StepParams p,
-                     typename MacroT<S>::T* __restrict__ rho_out, typename MacroT<S>::T* __restrict__ u_out) {
+    k_stream_collide(S* __restrict__ F, const __grid_constant__ GridDesc g, const __grid_constant__ StepParams p,
+                     const __grid_constant__ FaceWork fw, typename MacroT<S>::T* __restrict__ rho_out,
+                     typename MacroT<S>::T* __restrict__ u_out) {
   using C = typename Store<S>::C;
+  if ((int)blockIdx.z < fw.fz) {
+    face_cell<Q, S, CL, ODD, FUSED>(F, g, p, fw, rho_out, u_out);
+    return;
+  }
   const int z = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int x0 = blockIdx.z * kOnePlanes + 1;
-  const int x1 = min(g.nx, x0 + kOnePlanes - 1);
+  int x0 = (blockIdx.z - fw.fz) * kOnePlanes + 1;
+  int x1 = min(g.nx, x0 + kOnePlanes - 1);
   if (z > g.nz || y > g.ny) return;
+  // cells whose neighbours wrap across a periodic face belong to the face
+  // kernel; skipped by the loop's range, the loop body has no branch
+  if (wraps(g.periodic & 2, y, g.ny) || wraps(g.periodic & 4, z, g.nz)) return;
+  if (g.periodic & 1) {
+    x0 = max(x0, 2);
+    x1 = min(x1, g.nx - 1);
+    if (x0 > x1) return;
+  }
   const unsigned pl = (unsigned)g.plane;
   const unsigned s0 = (unsigned)sidx(g, x0, y, z);
   // fused no-slip links: a fluid cell reads bounce-back populations, a solid
@@ -157,11 +307,10 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, CL, FUSED>::blocks)
     const unsigned s = s0 + (unsigned)(x - x0) * pl;
     uint2 mn = make_uint2(0u, 0u);
     if (FUSED && x < x1) mn = p.mask[s + pl];
-    int ox[3], oy[3], oz[3];
-    nb_offsets(g, x, y, z, ox, oy, oz);
     C f[Q];
-    cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, s, ox, oy, oz, m.x, f);
-    cell_finish<Q, S, CL, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, z, s, ox, oy, oz, m.y, f, step_omega<C>(p));
+    cell_load_flat<Q, S, ODD, FUSED>(F, s, p, m.x, f);
+    cell_collide<Q, S, CL>(g, p, rho_out, u_out, x, y, z, s, f, step_omega<C>(p));
+    cell_store_flat<Q, S, ODD, FUSED>(F, p, s, m.y, f);
     m = mn;
   }
 }
@@ -169,11 +318,10 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, CL, FUSED>::blocks)
 // Two cells per thread, z and z + 32 of the same row: a warp covers 64
 // consecutive cells, and each thread has the loads of both cells in flight
 // before it collides the first, which doubles the bytes in flight per
-// register-limited warp. Used for the plain (no closure) FP32 step of
-// D3Q15/D3Q19 domains with fused links, at 768 threads (80 registers) per
-// SM; without fused links the schedule hoists every address of both cells
-// (over 128 registers), and with FP16 storage (fewer bytes, more
-// instructions) the one-cell kernel is faster.
+// register-limited warp. Used for the plain (no closure) FP32 and FP16 steps
+// of D3Q15/D3Q19 domains with fused links, at 768 threads (80 registers) per
+// SM (FP16 porous channel: 0.704 ms against 0.786 ms with one cell per
+// thread).
 // M32: the links come from the one-word mask (p.mask32). A block walks
 // kPairPlanes consecutive x planes; each thread loads the fused-link words of
 // the next plane one iteration ahead, so that the population loads, whose
@@ -184,18 +332,32 @@ constexpr int kPairPlanes = 2;
 constexpr int kPairThreads = 128;
 template <int Q, class S, bool ODD, bool FUSED, bool M32>
 __global__ void __launch_bounds__(kPairThreads, 768 / kPairThreads)
-    k_stream_collide_pair(S* __restrict__ F, const GridDesc g, const StepParams p,
+    k_stream_collide_pair(S* __restrict__ F, const __grid_constant__ GridDesc g,
+                          const __grid_constant__ StepParams p, const __grid_constant__ FaceWork fw,
                           typename MacroT<S>::T* __restrict__ rho_out, typename MacroT<S>::T* __restrict__ u_out) {
   using C = typename Store<S>::C;
+  if ((int)blockIdx.z < fw.fz) {
+    face_cell<Q, S, CL_NONE, ODD, FUSED>(F, g, p, fw, rho_out, u_out);
+    return;
+  }
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int za = blockIdx.x * (2 * blockDim.x) + 64 * w + lane + 1;
   const int zb = za + 32;
   const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int x0 = blockIdx.z * kPairPlanes + 1;
-  const int x1 = min(g.nx, x0 + kPairPlanes - 1);
+  int x0 = (blockIdx.z - fw.fz) * kPairPlanes + 1;
+  int x1 = min(g.nx, x0 + kPairPlanes - 1);
   if (za > g.nz || y > g.ny) return;
   const bool has_b = zb <= g.nz;
-  const unsigned ds = (unsigned)g.dstride;
+  // A pair with a cell whose neighbours wrap across a periodic face is left to
+  // the face kernel (both cells; face_planes lists the partners). Skipping
+  // by the loop's range keeps the loop body free of branches.
+  if (wraps(g.periodic & 2, y, g.ny) || wraps(g.periodic & 4, za, g.nz) || (has_b && (g.periodic & 4) && zb == g.nz))
+    return;
+  if (g.periodic & 1) {
+    x0 = max(x0, 2);
+    x1 = min(x1, g.nx - 1);
+    if (x0 > x1) return;
+  }
   const unsigned pl = (unsigned)g.plane;
   const unsigned s0 = (unsigned)sidx(g, x0, y, za);
   const C om0 = step_omega<C>(p);
@@ -227,16 +389,15 @@ __global__ void __launch_bounds__(kPairThreads, 768 / kPairThreads)
       ma = (wa.x >> 31) ? make_uint2(0u, wa.x & 0x7fffffffu) : make_uint2(wa.x, 0u);
       mb = (wb.x >> 31) ? make_uint2(0u, wb.x & 0x7fffffffu) : make_uint2(wb.x, 0u);
     }
-    int ox[3], oy[3], oza[3], ozb[3];
-    nb_offsets(g, x, y, za, ox, oy, oza);
-    ozb[0] = -1;  // zb >= 33: the lower neighbour never wraps
-    ozb[1] = 0;
-    ozb[2] = ((g.periodic & 4) && zb == g.nz) ? -(g.nz - 1) : 1;
     C fa[Q], fb[Q];
-    cell_load<Q, S, ODD, FUSED>(F, ds, sa, ox, oy, oza, ma.x, fa);
-    if (has_b) cell_load<Q, S, ODD, FUSED>(F, ds, sb, ox, oy, ozb, mb.x, fb);
-    cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, za, sa, ox, oy, oza, ma.y, fa, om0);
-    if (has_b) cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, rho_out, u_out, x, y, zb, sb, ox, oy, ozb, mb.y, fb, om0);
+    cell_load_flat<Q, S, ODD, FUSED>(F, sa, p, ma.x, fa);
+    if (has_b) cell_load_flat<Q, S, ODD, FUSED>(F, sb, p, mb.x, fb);
+    cell_collide<Q, S, CL_NONE>(g, p, rho_out, u_out, x, y, za, sa, fa, om0);
+    cell_store_flat<Q, S, ODD, FUSED>(F, p, sa, ma.y, fa);
+    if (has_b) {
+      cell_collide<Q, S, CL_NONE>(g, p, rho_out, u_out, x, y, zb, sb, fb, om0);
+      cell_store_flat<Q, S, ODD, FUSED>(F, p, sb, mb.y, fb);
+    }
     wa = na;
     wb = nb;
   }
@@ -275,31 +436,34 @@ cudaError_t step_q_s_cl(const DomainDev& d, const StepParams& p, int parity_in, 
   dim3 grid, block;
   using M = typename MacroT<S>::T;
   const bool fused = p.mask != nullptr;
-  if constexpr (CL == CL_NONE && Q != 27 && std::is_same<S, float>::value) {
+  S* F = (S*)d.F;
+  M* rho = (M*)d.rho;
+  M* u = (M*)d.u;
+  if constexpr (CL == CL_NONE && Q != 27 && !std::is_same<S, double>::value) {
     if (d.variant == 0 && fused) {
       pair_launch_shape(d.g, grid, block);
+      const FaceWork fw = face_work(d.g, true, block.x * block.y, grid.x, grid.y);
+      grid.z += fw.fz;
       const bool m32 = p.mask32 != nullptr;
       if (parity_in == 0) {
-        if (m32) k_stream_collide_pair<Q, S, true, true, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
-        else k_stream_collide_pair<Q, S, true, true, false><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+        if (m32) k_stream_collide_pair<Q, S, true, true, true><<<grid, block, 0, st>>>(F, d.g, p, fw, rho, u);
+        else k_stream_collide_pair<Q, S, true, true, false><<<grid, block, 0, st>>>(F, d.g, p, fw, rho, u);
       } else {
-        if (m32) k_stream_collide_pair<Q, S, false, true, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
-        else k_stream_collide_pair<Q, S, false, true, false><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+        if (m32) k_stream_collide_pair<Q, S, false, true, true><<<grid, block, 0, st>>>(F, d.g, p, fw, rho, u);
+        else k_stream_collide_pair<Q, S, false, true, false><<<grid, block, 0, st>>>(F, d.g, p, fw, rho, u);
       }
       return cudaGetLastError();
     }
   }
   plane_launch_shape(d.g, grid, block);
+  const FaceWork fw = face_work(d.g, false, block.x * block.y, grid.x, grid.y);
+  grid.z += fw.fz;
   if (parity_in == 0) {
-    if (fused)
-      k_stream_collide<Q, S, CL, true, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
-    else
-      k_stream_collide<Q, S, CL, true, false><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+    if (fused) k_stream_collide<Q, S, CL, true, true><<<grid, block, 0, st>>>(F, d.g, p, fw, rho, u);
+    else k_stream_collide<Q, S, CL, true, false><<<grid, block, 0, st>>>(F, d.g, p, fw, rho, u);
   } else {
-    if (fused)
-      k_stream_collide<Q, S, CL, false, true><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
-    else
-      k_stream_collide<Q, S, CL, false, false><<<grid, block, 0, st>>>((S*)d.F, d.g, p, (M*)d.rho, (M*)d.u);
+    if (fused) k_stream_collide<Q, S, CL, false, true><<<grid, block, 0, st>>>(F, d.g, p, fw, rho, u);
+    else k_stream_collide<Q, S, CL, false, false><<<grid, block, 0, st>>>(F, d.g, p, fw, rho, u);
   }
   return cudaGetLastError();
 }

@@ -365,6 +365,36 @@ def test_kernel_variants_bitwise_equal(gpu, q, storage, shape, periodic):
         assert np.array_equal(lbs[0][0].getVelocity(), lb.getVelocity())
 
 
+@pytest.mark.parametrize("nz", [33, 40, 65, 70, 100])
+@pytest.mark.parametrize("periodic", [(True, True, True), (False, True, True), (True, False, False)])
+def test_periodic_faces_bitwise_across_kernels(gpu, nz, periodic):
+    """Cells on periodic faces go to the face kernel; the two-cells-per-thread
+    kernel also leaves it the z partners of the pairs it skips (z = 33, and
+    nz - 32 when nz is the second cell of its pair). Every cell must still be
+    advanced exactly once: the pair kernel (variant 0, fused FP32), the
+    one-cell kernel (variant 2) and the TMA kernel (variant 1) agree bit for
+    bit, with fused walls on the non-periodic axes and a fused sphere map."""
+    shape = (12, 10, nz)
+    g = tuple(s + 2 for s in shape)
+    rho, u = smooth_field(g, nz)
+    m = sphere_map(g, (6.0, 4.5, nz / 2.0), 3.5)
+    out = []
+    for variant in (0, 1, 2):
+        lb = A.LBGK(A.Block(shape), 0.04, A.d3q19(), periodic=periodic, body_force=(2e-4, 1e-4, -1e-4))
+        lb.setKernel(variant)
+        A.LBGKUtilities(lb).initF(rho, u)
+        walls = [w for a, w in ((0, (A.X0, A.XE)), (1, (A.Y0, A.YE)), (2, (A.Z0, A.ZE))) if not periodic[a] for w in w]
+        bcs = ([A.generateBCNoSlip(lb, walls)] if walls else []) + [A.generateBCNoSlip(lb, m)]
+        for b in bcs:
+            b.fuse()
+        lb.run(9, bcs)
+        lb.sync()
+        out.append((lb.getF(), lb.getVelocity()))
+    for f, v in out[1:]:
+        assert np.array_equal(out[0][0], f, equal_nan=True)
+        assert np.array_equal(out[0][1], v)
+
+
 def test_kernel_variants_fused_porous_bitwise(gpu):
     w = W.porous_channel(size=(80, 40, 36), rmin=2.0, rmax=5.0, solid_fraction=0.35, steps=0)
     out = []
