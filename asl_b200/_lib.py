@@ -58,6 +58,8 @@ PROTOTYPES = {
     "aslb_lbgk_shape": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "aslb_lbgk_init_f": (C.c_int, [_vp, C.c_double, _pd]),
     "aslb_lbgk_init_f_fields": (C.c_int, [_vp, _pd, _pd]),
+    "aslb_lbgk_compute_macro": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "aslb_lbgk_bind_velocity": (C.c_int, [_vp, _vp]),
     "aslb_lbgk_step": (C.c_int, [_vp, C.c_int]),
     "aslb_lbgk_run": (C.c_int, [_vp, C.c_int, C.POINTER(_vp), C.c_int, C.c_int]),
     "aslb_lbgk_sync": (C.c_int, [_vp]),

@@ -63,6 +63,7 @@ struct aslb_lbgk {
   int mlp_period = 32;
   long long mlp_last = -1;  // step at which the field was last computed
   void* stage = nullptr;            // one-direction transfer buffer (stage_buffer)
+  void* u_own = nullptr;            // the domain's own velocity field (d.u may be a caller's)
   double* red_partials = nullptr;  // moments scratch
   double* red_out = nullptr;
   double* host_out = nullptr;      // pinned
@@ -446,6 +447,7 @@ int aslb_lbgk_create(int nx, int ny, int nz, int q, int storage, double nu, unsi
   cudaError_t e = cudaMalloc(&h->d.F, fbytes);
   if (e == cudaSuccess) e = cudaMalloc(&h->d.rho, (size_t)g.L * mb);
   if (e == cudaSuccess) e = cudaMalloc(&h->d.u, 3 * (size_t)g.L * mb);
+  h->u_own = h->d.u;
   if (e == cudaSuccess) e = cudaMalloc((void**)&h->red_out, 8 * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc((void**)&h->d.err, sizeof(int));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&h->host_err, sizeof(int));
@@ -507,7 +509,7 @@ int aslb_lbgk_destroy(aslb_lbgk* h) {
   }
   cudaFree(h->d.F);
   cudaFree(h->d.rho);
-  cudaFree(h->d.u);
+  cudaFree(h->u_own);
   cudaFree(h->mlp_dev);
   cudaFree(h->cs2_field);
   cudaFree(h->mask_dev);
@@ -692,6 +694,23 @@ int aslb_lbgk_init_f_fields(aslb_lbgk* h, const double* rho, const double* u) {
   h->parity = 0;
   h->fresh = true;
   h->version++;
+  return ASLB_OK;
+}
+
+int aslb_lbgk_bind_velocity(aslb_lbgk* h, void* u_dev) {
+  ASLB_CHECK_HANDLE(h);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_bind_velocity: ") + cudaGetErrorString(e));
+  h->d.u = u_dev ? u_dev : h->u_own;
+  h->version++;  // recorded graphs hold the old pointer
+  return ASLB_OK;
+}
+
+int aslb_lbgk_compute_macro(aslb_lbgk* h, int comp_rho, int comp_vel) {
+  ASLB_CHECK_HANDLE(h);
+  prepare_params(h);
+  cudaError_t e = launch_compute_macro(h->d, h->p, h->parity, comp_rho ? 1 : 0, comp_vel ? 1 : 0, h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_compute_macro: ") + cudaGetErrorString(e));
   return ASLB_OK;
 }
 

@@ -763,4 +763,53 @@ cudaError_t launch_watchdog(const DomainDev& d, const StepParams& p, int parity,
   ASLB_DISPATCH(d, watchdog_impl, d, p, parity, partials, st)
 }
 
+// Density and velocity of every interior cell from the populations as they
+// stand (the post-collision values of the last step), into the domain's rho /
+// u fields in ASL's ghosted layout: rho = sum w f, u = m / rho (m for the
+// incompressible equilibrium), m = sum w c f, accumulated in the macro type.
+template <int Q, class S>
+__global__ void __launch_bounds__(256) k_compute_macro(const S* __restrict__ F, const GridDesc g, const StepParams p,
+                                                       int parity, int comp_rho, int comp_vel,
+                                                       typename MacroT<S>::T* __restrict__ rho_out,
+                                                       typename MacroT<S>::T* __restrict__ u_out) {
+  using Lt = Lattice<Q>;
+  using M = typename MacroT<S>::T;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int y = blockIdx.y + 1;
+  const int x = blockIdx.z + 1;
+  if (z > g.nz) return;
+  M rho = M(0), m0 = M(0), m1 = M(0), m2 = M(0);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const M wf = M(Lt::w(i)) * M(Store<S>::val(F + fstar_index<Q>(g, p.mask, parity, x, y, z, i), p.inv_scale));
+    rho += wf;
+    if (Lt::c(i, 0)) m0 += Lt::c(i, 0) > 0 ? wf : -wf;
+    if (Lt::c(i, 1)) m1 += Lt::c(i, 1) > 0 ? wf : -wf;
+    if (Lt::c(i, 2)) m2 += Lt::c(i, 2) > 0 ? wf : -wf;
+  }
+  const long long a = aidx(g, x, y, z);
+  if (comp_rho) rho_out[a] = rho;
+  if (comp_vel) {
+    const M inv = p.compressible ? M(1) / rho : M(1);
+    u_out[a] = m0 * inv;
+    u_out[g.L + a] = m1 * inv;
+    u_out[2 * g.L + a] = m2 * inv;
+  }
+}
+
+template <int Q, class S>
+static cudaError_t compute_macro_impl(const DomainDev& d, const StepParams& p, int parity, int comp_rho,
+                                      int comp_vel, cudaStream_t st) {
+  using M = typename MacroT<S>::T;
+  dim3 block(128), grid((d.g.nz + 127) / 128, d.g.ny, d.g.nx);
+  k_compute_macro<Q, S><<<grid, block, 0, st>>>((const S*)d.F, d.g, p, parity, comp_rho, comp_vel, (M*)d.rho,
+                                                (M*)d.u);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_compute_macro(const DomainDev& d, const StepParams& p, int parity, int comp_rho, int comp_vel,
+                                 cudaStream_t st) {
+  ASLB_DISPATCH(d, compute_macro_impl, d, p, parity, comp_rho, comp_vel, st)
+}
+
 }  // namespace aslb

@@ -49,6 +49,9 @@ cudaError_t launch_export_f(const DomainDev& d, const StepParams& p, int parity,
                             cudaStream_t st);
 cudaError_t launch_import_f(const DomainDev& d, const StepParams& p, int i0, int i1, const void* in,
                             cudaStream_t st);
+// rho and / or u of every interior cell from the current populations.
+cudaError_t launch_compute_macro(const DomainDev& d, const StepParams& p, int parity, int comp_rho, int comp_vel,
+                                 cudaStream_t st);
 // Boundary links: anchors (x, y, z, direction mask) in ghosted coordinates.
 // Conditions on the rho / u output fields (visualisation): guard cells with
 // their fluid-neighbour masks, per-cell weights for the rho condition.

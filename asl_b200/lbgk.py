@@ -332,6 +332,17 @@ class LBGKUtilities:
         L.check(lib.aslb_lbgk_init_f_fields(self.num.h, None if r is None else r.ctypes.data_as(L._pd),
                                             u.ctypes.data_as(L._pd)), "LBGKUtilities::initF")
 
+    # Declared but never defined by the reference (src/num/aslLBGK.h:153-155):
+    # the density / velocity fields from the populations as they stand.
+    def computeRho(self):
+        L.check(self.num.lib.aslb_lbgk_compute_macro(self.num.h, 1, 0), "LBGKUtilities::computeRho")
+
+    def computeVelocity(self):
+        L.check(self.num.lib.aslb_lbgk_compute_macro(self.num.h, 0, 1), "LBGKUtilities::computeVelocity")
+
+    def computeRhoVelocity(self):
+        L.check(self.num.lib.aslb_lbgk_compute_macro(self.num.h, 1, 1), "LBGKUtilities::computeRhoVelocity")
+
 
 # ---- boundary conditions -----------------------------------------------------
 

@@ -1,0 +1,6 @@
+/* acl/aclMath/aclVectorOfElements.h -- ASL header name of the LBGK path; the classes and functions are in
+ * aslb_asl.hpp (over the C ABI of libaslb.so, aslb.h). */
+#ifndef ASLB_FACADE_ACL_ACLMATH_ACLVECTOROFELEMENTS_H
+#define ASLB_FACADE_ACL_ACLMATH_ACLVECTOROFELEMENTS_H
+#include "../../aslb_asl_io.hpp"
+#endif

@@ -1,0 +1,6 @@
+/* writers/aslVTKFormatWriters.h -- ASL header name of the LBGK path; the classes and functions are in
+ * aslb_asl.hpp (over the C ABI of libaslb.so, aslb.h). */
+#ifndef ASLB_FACADE_WRITERS_ASLVTKFORMATWRITERS_H
+#define ASLB_FACADE_WRITERS_ASLVTKFORMATWRITERS_H
+#include "../aslb_asl_io.hpp"
+#endif

@@ -167,6 +167,23 @@ int aslb_lbgk_init_f(aslb_lbgk* h, double rho, const double u[3]);
 /* initF with fields: rho (L doubles, or NULL for 1) and u (3L doubles), host. */
 int aslb_lbgk_init_f_fields(aslb_lbgk* h, const double* rho, const double* u);
 
+/* asl::LBGK::LBGK(DataD v, Param nu, const VectorTemplate*) and
+ * LBGKTurbulence(DataD v, ...) (src/num/aslLBGK.h:112,165; src/num/aslLBGK.cxx:
+ * 95-112): the domain writes its velocity into the caller's container
+ * instead of its own. u_dev is DEVICE memory of 3 * L values (float; double
+ * for FP64 storage) in ASL's ghosted layout, owned by the caller and valid
+ * until it is unbound (NULL restores the domain's own field). Every later
+ * velocity write, read and FD binding uses it. Synchronises the domain's
+ * stream. */
+int aslb_lbgk_bind_velocity(aslb_lbgk* h, void* u_dev);
+/* LBGKUtilities::computeRho / computeVelocity / computeRhoVelocity (declared,
+ * never defined in the reference: src/num/aslLBGK.h:153-155): rho = sum w_i f_i
+ * and u = m / rho (m for the incompressible equilibrium), m = sum w_i c_i f_i,
+ * of every interior cell from the populations as they stand (the
+ * post-collision values of the last step), into the domain's density and / or
+ * velocity fields. Enqueued on the domain's stream. */
+int aslb_lbgk_compute_macro(aslb_lbgk* h, int comp_rho, int comp_vel);
+
 /* LBGK::execute(): one stream + collide step (src/num/aslLBGK.cxx:237-250,
  * src/num/aslSingleKernelNM.cxx:48-53), nsteps times. Boundary conditions are
  * separate objects, executed by the caller after each step as in ASL. */
