@@ -60,6 +60,8 @@ PROTOTYPES = {
     "aslb_lbgk_init_f_fields": (C.c_int, [_vp, _pd, _pd]),
     "aslb_lbgk_compute_macro": (C.c_int, [_vp, C.c_int, C.c_int]),
     "aslb_lbgk_bind_velocity": (C.c_int, [_vp, _vp]),
+    "aslb_lbgk_step_planes": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
+    "aslb_lbgk_step_commit": (C.c_int, [_vp]),
     "aslb_lbgk_step": (C.c_int, [_vp, C.c_int]),
     "aslb_lbgk_run": (C.c_int, [_vp, C.c_int, C.POINTER(_vp), C.c_int, C.c_int]),
     "aslb_lbgk_sync": (C.c_int, [_vp]),

@@ -725,6 +725,46 @@ int aslb_lbgk_step(aslb_lbgk* h, int nsteps) {
   return ASLB_OK;
 }
 
+int aslb_lbgk_step_planes(aslb_lbgk* h, int x_first, int x_last, void* stream) {
+  ASLB_CHECK_HANDLE(h);
+  const GridDesc& g = h->d.g;
+  if (x_first < 1 || x_last > g.nx || x_first > x_last)
+    return fail(ASLB_ERR_ARG, "aslb_lbgk_step_planes: planes outside 1 .. nx");
+  if (g.periodic & 1) return fail(ASLB_ERR_ARG, "aslb_lbgk_step_planes: the domain is periodic in x");
+  if (h->closure == CL_MLP) return fail(ASLB_ERR_ARG, "aslb_lbgk_step_planes: not with the learned closure");
+  prepare_params(h);
+  // a view of planes x_first .. x_last as a domain of their own: every
+  // per-cell array shifted by the planes before them (the slot offsets and
+  // strides are relative, the component stride L of u stays the whole one)
+  DomainDev v = h->d;
+  StepParams q = h->p;
+  const long long sh = (long long)(x_first - 1) * g.plane;
+  const long long ash = (long long)(x_first - 1) * g.gy * g.gz;
+  v.g.nx = x_last - x_first + 1;
+  v.g.gx = v.g.nx + 2;
+  v.F = (char*)h->d.F + sh * (long long)storage_bytes(h->d.storage);
+  v.rho = (char*)h->d.rho + ash * (long long)macro_bytes(h->d.storage);
+  v.u = (char*)h->d.u + ash * (long long)macro_bytes(h->d.storage);
+  if (v.variant == 1) v.variant = 0;
+  if (q.mask) q.mask += sh;
+  if (q.mask32) q.mask32 += sh;
+  if (q.cs2) q.cs2 += sh;
+  cudaError_t e = launch_step(v, q, h->closure, h->parity, stream ? (cudaStream_t)stream : h->stream);
+  if (e != cudaSuccess) return fail(ASLB_ERR_CUDA, std::string("aslb_lbgk_step_planes: ") + cudaGetErrorString(e));
+  return ASLB_OK;
+}
+
+int aslb_lbgk_step_commit(aslb_lbgk* h) {
+  ASLB_CHECK_HANDLE(h);
+  h->parity ^= 1;
+  h->steps += 1;
+  if (h->macro_once) {
+    h->macro_once = false;
+    h->version++;
+  }
+  return ASLB_OK;
+}
+
 int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int use_graph) {
   NvtxRange range("aslb_lbgk_run");
   ASLB_CHECK_HANDLE(h);

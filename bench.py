@@ -6,8 +6,10 @@ force 1e-6, tau 0.6; synthetic data generated from a seed).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One JSON line on rank 0. `value` is whole-job MLUPS (all ranks; one replica
-of the workload per GPU, weak scaling) with populations resident in HBM;
+One JSON line on rank 0. `value` is whole-job MLUPS with populations
+resident in HBM; with N > 1 GPUs the channel is N times longer and cut into
+x slabs, one per GPU, exchanging faces every step (weak scaling; --replicas
+runs independent copies instead);
 `e2e` is the same metric through the C ABI with the initial populations
 uploaded from pinned host memory and density/velocity downloaded to pinned
 host memory inside the timed region; `roofline` describes the dominant
@@ -45,12 +47,21 @@ def parse_args():
     ap.add_argument("--storage", default="f32", choices=["f32", "f16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp16", action="store_true")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with several GPUs: one independent replica per GPU instead of x slabs")
+    ap.add_argument("--slabs", action="store_true",
+                    help="the x-slab path even on one GPU (one slab closing its own x-periodic ring)")
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--accuracy-steps", type=int, default=5000,
                     help="steps of the FP16/FP32-against-FP64 accuracy study (0: skip)")
     ap.add_argument("--q27-steps", type=int, default=400,
                     help="timed steps of the D3Q27 vehicle workload (0: skip)")
     ap.add_argument("--q27-size", default="768,384,384")
+    ap.add_argument("--vehicle-study-steps", type=int, default=2000,
+                    help="steps of the D3Q27 closure / storage study on the downscaled tunnel (0: skip)")
+    ap.add_argument("--vehicle-small", default="192,96,96")
+    ap.add_argument("--details", default="bench_details.json",
+                    help="file for the full results of every leg (the JSON line carries a summary)")
     ap.add_argument("--batch-steps", type=int, default=2000,
                     help="timed steps of the 256-domain batch (0: skip)")
     ap.add_argument("--batch-domains", type=int, default=256)
@@ -313,7 +324,7 @@ def vehicle_run(W, size, steps: int, peak: float):
            "obstacles": w.info["obstacles"], "drag_lift_series": series,
            "series_columns": ["step", "drag (sum F_x)", "lift (sum F_z)"]}
     del force, lb, bcs
-    return res
+    return res, w
 
 
 def closure_run(n: int):
@@ -326,6 +337,69 @@ def closure_run(n: int):
     blob = res.pop("blob")
     res["speed"] = CL.closure_speed(n, blob)
     res["metric"] = "relative L2 of log E(k), 2 <= k <= n/4, against the 2x box-filtered fine run"
+    return res, blob
+
+
+def vehicle_series(W, w, storage: str, closure: str, steps: int, every: int, blob=None, period: int = 32):
+    """Drag (sum F_x) and lift (sum F_z) of the obstacles every `every` steps
+    of a D3Q27 vehicle tunnel, and the step rate (MLUPS, CUDA events around
+    the time loop; force evaluations excluded)."""
+    import numpy as np
+    import torch
+    from asl_b200 import _lib as L
+    from asl_b200 import lbgk as A
+    lb, bcs = W.build_lbgk(w, storage=storage, compVel=False, compRho=False, fuse=True)
+    if closure == "smagorinsky":
+        lb.setClosure(L.CLOSURE_SMAGORINSKY, 0.17)
+    elif closure == "learned":
+        lb.setMLP(blob)
+        lb.setMLPPeriod(period)
+        lb.setClosure(L.CLOSURE_MLP)
+    force = A.generateComputeSurfaceForce(lb, w.map)
+    st = torch.cuda.ExternalStream(lb.stream)
+    out, t = [], 0.0
+    for _ in range(max(1, steps // every)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        lb.run(every, bcs, use_graph=True)
+        e1.record(st)
+        e1.synchronize()
+        t += e0.elapsed_time(e1) / 1e3
+        f = force.execute()
+        out.append([int(lb.steps), float(f[0]), float(f[2])])
+    del force, lb, bcs
+    return np.array(out), w.cells * every * len(out) / t / 1e6
+
+
+def vehicle_study(W, blob, small, small_steps: int, full_w, full_steps: int):
+    """The D3Q27 vehicle configuration with closures and storage formats: on
+    a downscaled tunnel the drag / lift series of FP32 Smagorinsky, FP16
+    Smagorinsky and FP16 storage with the learned closure against FP64
+    Smagorinsky (the reference), and at full size the step rates of FP32
+    Smagorinsky and FP16 + learned closure."""
+    import numpy as np
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    every = max(1, small_steps // 8)
+    ws = W.vehicle_d3q27(size=small, steps=small_steps)
+    ref, _ = vehicle_series(W, ws, "f64", "smagorinsky", small_steps, every)
+    res = {"small": "%dx%dx%d" % tuple(small), "small_steps": small_steps, "reference": "f64 smagorinsky",
+           "vs_reference": {}}
+    for storage, closure in (("f32", "smagorinsky"), ("f16", "smagorinsky"), ("f16", "learned")):
+        sr, _ = vehicle_series(W, ws, storage, closure, small_steps, every, blob)
+        ok = bool(np.isfinite(sr).all())
+        res["vs_reference"]["%s_%s" % (storage, closure)] = {
+            "drag_rel_l2": rel(sr[:, 1], ref[:, 1]) if ok else None,
+            "lift_rel_l2": rel(sr[:, 2], ref[:, 2]) if ok else None}
+    res["full_cells"] = full_w.cells
+    speed = {}
+    for storage, closure in (("f32", "smagorinsky"), ("f16", "learned")):
+        _, mlups = vehicle_series(W, full_w, storage, closure, full_steps, full_steps, blob)
+        speed["%s_%s" % (storage, closure)] = mlups
+    res["full_mlups"] = speed
+    res["full_steps"] = full_steps
+    res["f16_learned_speedup_vs_f32_smagorinsky"] = speed["f16_learned"] / speed["f32_smagorinsky"]
     return res
 
 
@@ -419,8 +493,123 @@ def batch_run(W, n: int, steps: int, peak: float):
     return res
 
 
+def run_slabs(args):
+    """N > 1: one (N x 512) x 256 x 256 porous channel cut into x slabs, one
+    512 x 256 x 256 slab per GPU (weak scaling). Every step advances each
+    slab's boundary planes, exchanges the faces with NCCL point-to-point
+    operations while the interior planes run on a second stream, then unpacks
+    (asl_b200.slabs.overlapped_step). Timed with CUDA events on each rank's
+    domain stream, max over ranks."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if "MASTER_ADDR" not in os.environ:  # one GPU without a launcher (--slabs)
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT="29517", RANK="0", WORLD_SIZE="1")
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from asl_b200 import _lib
+    from asl_b200 import slabs as SL
+    from asl_b200 import workloads as W
+    _lib.check(_lib.load().aslb_set_device(local), "set_device")
+    sx, sy, sz = parse_size(args.size)
+    w = W.porous_channel(size=(sx * world, sy, sz))
+    slab = SL.Slab(w, rank, world, storage=args.storage, fuse=True, compVel=False, compRho=False)
+    lb = slab.lb
+    K, Wm = args.steps, args.warmup
+    peak, peak_kind = peak_hbm()
+
+    def max_over_ranks(v: float) -> float:
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(Wm):
+        SL.overlapped_step(slab, SL.nccl_transport)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(slab.stream)
+    for _ in range(K):
+        SL.overlapped_step(slab, SL.nccl_transport)
+    e1.record(slab.stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    dist.barrier()
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    # the stream-collide alone on each rank's slab (no exchange), for the roofline
+    nk = min(K, 200) // 2 * 2
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0.record(slab.stream)
+    lb.execute(nk)
+    k1.record(slab.stream)
+    k1.synchronize()
+    tk = max_over_ranks(k0.elapsed_time(k1) / 1e3 / nk)
+    cells_rank = slab.w.cells
+    bpc = BYTES_PER_CELL[(args.storage, 19)]
+    # end to end: every rank uploads its slab's populations from pinned host
+    # memory, runs K steps with the exchange, and reads density and velocity back
+    gx, gy, gz = (v + 2 for v in slab.w.size)
+    L = gx * gy * gz
+    f_host = torch.empty(19 * L, dtype=torch.float32, pin_memory=True)
+    rho_host = torch.empty(L, dtype=torch.float32, pin_memory=True)
+    u_host = torch.empty(3 * L, dtype=torch.float32, pin_memory=True)
+    lib = lb.lib
+    _lib.check(lib.aslb_lbgk_read(lb.h, _lib.FIELD_F, _lib.F32, f_host.data_ptr()), "read")
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(slab.stream)
+    _lib.check(lib.aslb_lbgk_write(lb.h, _lib.FIELD_F, _lib.F32, f_host.data_ptr()), "write")
+    for n in range(K):
+        if n == K - 1:
+            lb.requestMacro()
+        SL.overlapped_step(slab, SL.nccl_transport)
+    _lib.check(lib.aslb_lbgk_read(lb.h, _lib.FIELD_RHO, _lib.F32, rho_host.data_ptr()), "read")
+    _lib.check(lib.aslb_lbgk_read(lb.h, _lib.FIELD_VELOCITY, _lib.F32, u_host.data_ptr()), "read")
+    e1.record(slab.stream)
+    e1.synchronize()
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    mass = torch.tensor([lb.moments()[0]], dtype=torch.float64, device="cuda")
+    dist.all_reduce(mass)
+    if rank == 0:
+        achieved = bpc * cells_rank / tk / 1e9
+        line = {"metric": METRIC, "value": w.cells * K / t / 1e6, "unit": "MLUPS", "n_gpus": world, "steps": K,
+                "warmup": Wm, "ms_per_step": t / K * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": args.storage,
+                "data": "synthetic (seeded random spheres, base seed 20261203)",
+                "config": {"workload": w.name, "lattice": "D3Q19", "cells": w.cells, "storage": args.storage,
+                           "cells_per_gpu": cells_rank, "fused_noslip": True,
+                           "l2": "populations far exceed L2; no flush needed",
+                           "parallelism": "x slabs over %d GPUs, NCCL face exchange overlapped with the interior"
+                                          % world},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                             "kernel": "stream-collide of one slab, max over ranks", "bytes_per_cell": bpc,
+                             "cells_per_launch": cells_rank, "kernel_ms": tk * 1e3},
+                "cpu_baseline": None,
+                "e2e": {"value": w.cells * K / t_e2e / 1e6, "unit": "MLUPS",
+                        "h2d_bytes_per_step": world * 19 * L * 4 / K, "d2h_bytes_per_step": world * 4 * L * 4 / K,
+                        "timed": "every rank: population upload from pinned host memory, K overlapped steps, "
+                                 "density and velocity download; max over ranks"},
+                "clocks": clk, "gpu_launches": K * 3 * world,
+                "summary": {"exchange_overhead": t / K / tk - 1.0, "mass": float(mass.item())}}
+        print(json.dumps(line), flush=True)
+    del slab, lb
+    torch.cuda.synchronize()
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
+
+
 def run_ours(args):
     rank, world, local = dist_env()
+    if (world > 1 and not args.replicas) or args.slabs:
+        return run_slabs(args)
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline_subprocess(args)
@@ -549,12 +738,16 @@ def run_ours(args):
     batched = None
     if world == 1 and args.batch_steps > 0:
         batched = batch_run(W, args.batch_domains, args.batch_steps, peak)
-    learned = None
+    learned, blob = None, None
     if world == 1 and args.closure_size > 0:
-        learned = closure_run(args.closure_size)
+        learned, blob = closure_run(args.closure_size)
     vehicle = None
     if world == 1 and args.q27_steps > 0:
-        vehicle = vehicle_run(W, parse_size(args.q27_size), args.q27_steps, peak)
+        vehicle, wv = vehicle_run(W, parse_size(args.q27_size), args.q27_steps, peak)
+        if blob is not None and args.vehicle_study_steps > 0:
+            vehicle["study"] = vehicle_study(W, blob, parse_size(args.vehicle_small), args.vehicle_study_steps, wv,
+                                             args.q27_steps)
+        del wv
     fdad = None
     if world == 1 and args.fd_steps > 0:
         fdad = fd_run(W, w, args.fd_steps, peak)
@@ -570,6 +763,13 @@ def run_ours(args):
                     "mask per cell is overhead and not counted"}
 
     if rank == 0:
+        details = {"separate_conditions": sep, "tma_kernel": direct, "fp16": fp16, "accuracy": accuracy,
+                   "d3q27_vehicle": vehicle, "batched_domains": batched, "learned_closure": learned,
+                   "fd_advection_diffusion": fdad, "finite": finite, "mass": mom[0]}
+        try:
+            Path(args.details).write_text(json.dumps(details, indent=1))
+        except OSError:
+            pass
         line = {"metric": METRIC, "value": head["value"], "unit": "MLUPS", "n_gpus": world, "steps": K,
                 "warmup": Wm, "ms_per_step": t / K * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": args.storage,
@@ -582,14 +782,47 @@ def run_ours(args):
                            "time_loop": "CUDA graph of two steps, replayed"},
                 "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "clocks": clk,
                 "gpu_launches": K * head["launches_per_step"],
-                "separate_conditions": sep, "tma_kernel": direct, "fp16": fp16, "accuracy": accuracy,
-                "d3q27_vehicle": vehicle, "batched_domains": batched, "learned_closure": learned,
-                "fd_advection_diffusion": fdad,
-                "finite": finite, "mass": mom[0]}
+                "summary": summary(head, sep, fp16, accuracy, batched, learned, vehicle, fdad, finite)}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def _r(v, n=4):
+    return None if v is None else float("%.*g" % (n, v))
+
+
+def summary(head, sep, fp16, acc, batched, learned, vehicle, fdad, finite):
+    """The other legs in a few numbers (full results in the details file),
+    last in the JSON line so that a tail of it shows them."""
+    out = {"f32_kernel_ms": _r(head["kernel_ms"]), "f32_frac": _r(head["kernel_frac_of_peak"], 3),
+           "separate_conditions_mlups": _r(sep["value"])}
+    if fp16:
+        out["fp16"] = {"mlups": _r(fp16["value"]), "kernel_ms": _r(fp16["kernel_ms"]),
+                       "frac": _r(fp16["kernel_frac_of_peak"], 3), "speedup_vs_f32": _r(fp16["speedup_vs_f32"], 3)}
+    if acc:
+        out["accuracy_vs_f64"] = {"steps": acc["steps"],
+                                  "perm_err": {k: _r(v, 2) for k, v in acc["permeability_rel_err"].items()},
+                                  "u_l2": {k: _r(v, 2) for k, v in acc["velocity_rel_l2"].items()}}
+    if batched:
+        out["batch"] = {"mlups": _r(batched["value"]), "kernel_frac": _r(batched["kernel_frac_of_peak"], 3),
+                        "vs_separate": _r(batched["value"] / batched["separate_launches"]["value"], 3)}
+    if learned:
+        runs = learned["runs"]
+        out["closure"] = {k: [_r(v, 2) for v in runs[k]["spectrum_rel_l2_logE"].values()]
+                          for k in ("learned", "smagorinsky", "smagorinsky_fit")}
+        out["closure"]["overhead"] = _r(learned["speed"]["learned_overhead_vs_smagorinsky"], 3)
+    if vehicle:
+        out["d3q27"] = {"mlups": _r(vehicle["value"]), "frac": _r(vehicle["kernel_frac_of_peak"], 3)}
+        st = vehicle.get("study")
+        if st:
+            out["d3q27"]["drag_vs_f64"] = {k: _r(v["drag_rel_l2"], 2) for k, v in st["vs_reference"].items()}
+            out["d3q27"]["f16_learned_speedup"] = _r(st["f16_learned_speedup_vs_f32_smagorinsky"], 3)
+    if fdad:
+        out["fd_frac"] = {k: _r(fdad[k]["frac_of_peak"], 3) for k in ("d3q7", "d3q19")}
+    out["finite"] = finite
+    return out
 
 
 def main():

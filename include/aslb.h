@@ -192,6 +192,17 @@ int aslb_lbgk_step(aslb_lbgk* h, int nsteps);
  * (examples/flow/flow.cc:124-134) as one call. use_graph != 0 records two
  * steps into a CUDA graph once and replays it. */
 int aslb_lbgk_run(aslb_lbgk* h, int nsteps, aslb_bc* const* bcs, int nbc, int use_graph);
+/* Extension (no ASL analogue): one step split into parts, for overlapping
+ * the face exchange of an x-slab decomposition with the interior.
+ * aslb_lbgk_step_planes launches the stream-collide of interior x planes
+ * x_first .. x_last (1-based) at the current AA parity on `stream` (NULL: the
+ * domain's stream; the caller orders it against the domain's other work),
+ * without advancing the step; aslb_lbgk_step_commit then advances the step
+ * count and parity once every plane has been launched exactly once. Not for
+ * x-periodic domains or the learned closure. Parts of one step touch disjoint
+ * population slots, so they may run concurrently. */
+int aslb_lbgk_step_planes(aslb_lbgk* h, int x_first, int x_last, void* stream);
+int aslb_lbgk_step_commit(aslb_lbgk* h);
 /* Wait for all work of the domain; fails with ASLB_ERR_STATE if a kernel's
  * bounded wait gave up. */
 int aslb_lbgk_sync(aslb_lbgk* h);
