@@ -131,20 +131,29 @@ cudaError_t launch_init_f(const DomainDev& d, const StepParams& p, double rho0, 
 // ---------------------------------------------------------------------------
 // Export f*_i(x) in ASL's layout. In representation B the value sits at the
 // cell it was pushed to; ghost cells whose target leaves the block read NaN.
+// Population transfers between the storage and ASL's layout (a = the ghosted
+// index, z fastest), directions [i0, i1): a grid-stride loop over the cells,
+// so a one-direction transfer is one small launch.
+inline unsigned transfer_blocks(long long L) {
+  const long long b = (L + 255) / 256;
+  return (unsigned)(b < 148 * 16 ? b : 148 * 16);
+}
+
 template <int Q, class S>
-__global__ void k_export_f(const S* __restrict__ F, const GridDesc g, const StepParams p, int parity, int i0,
-                           int i1, typename MacroT<S>::T* __restrict__ out) {
+__global__ void __launch_bounds__(256) k_export_f(const S* __restrict__ F, const GridDesc g, const StepParams p,
+                                                  int parity, int i0, int i1,
+                                                  typename MacroT<S>::T* __restrict__ out) {
   using M = typename MacroT<S>::T;
-  const int z = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  const int x = blockIdx.z;
-  if (z >= g.gz) return;
-  const long long a = aidx(g, x, y, z);
+  for (long long a = (long long)blockIdx.x * blockDim.x + threadIdx.x; a < g.L; a += (long long)gridDim.x * blockDim.x) {
+    const int z = (int)(a % g.gz);
+    const long long r = a / g.gz;
+    const int y = (int)(r % g.gy), x = (int)(r / g.gy);
 #pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    if (i < i0 || i >= i1) continue;
-    const long long k = fstar_index<Q>(g, p.mask, parity, x, y, z, i);
-    out[(long long)(i - i0) * g.L + a] = k < 0 ? M(NAN) : M(Store<S>::val(F + k, p.inv_scale));
+    for (int i = 0; i < Q; ++i) {
+      if (i < i0 || i >= i1) continue;
+      const long long k = fstar_index<Q>(g, p.mask, parity, x, y, z, i);
+      out[(long long)(i - i0) * g.L + a] = k < 0 ? M(NAN) : M(Store<S>::val(F + k, p.inv_scale));
+    }
   }
 }
 
@@ -152,8 +161,7 @@ template <int Q, class S>
 static cudaError_t export_impl(const DomainDev& d, const StepParams& p, int parity, int i0, int i1, void* out,
                                cudaStream_t st) {
   using M = typename MacroT<S>::T;
-  dim3 block(128), grid((d.g.gz + 127) / 128, d.g.gy, d.g.gx);
-  k_export_f<Q, S><<<grid, block, 0, st>>>((const S*)d.F, d.g, p, parity, i0, i1, (M*)out);
+  k_export_f<Q, S><<<transfer_blocks(d.g.L), 256, 0, st>>>((const S*)d.F, d.g, p, parity, i0, i1, (M*)out);
   return cudaGetLastError();
 }
 
@@ -163,19 +171,17 @@ cudaError_t launch_export_f(const DomainDev& d, const StepParams& p, int parity,
 }
 
 template <int Q, class S>
-__global__ void k_import_f(S* __restrict__ F, const GridDesc g, const StepParams p, int i0, int i1,
-                           const typename MacroT<S>::T* __restrict__ in) {
-  const int z = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  const int x = blockIdx.z;
-  if (z >= g.gz) return;
-  const long long a = aidx(g, x, y, z);
-  const long long s = sidx(g, x, y, z);
+__global__ void __launch_bounds__(256) k_import_f(S* __restrict__ F, const GridDesc g, const StepParams p, int i0,
+                                                  int i1, const typename MacroT<S>::T* __restrict__ in) {
+  for (long long a = (long long)blockIdx.x * blockDim.x + threadIdx.x; a < g.L; a += (long long)gridDim.x * blockDim.x) {
+    // storage index: the rows (x, y) are in the same order in both layouts
+    const long long s = (a / g.gz) * g.pitch + g.zoff + a % g.gz;
 #pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    if (i < i0 || i >= i1) continue;
-    Store<S>::set_val(F + (size_t)i * g.dstride + s, typename Store<S>::C(in[(long long)(i - i0) * g.L + a]),
-                      p.scale);
+    for (int i = 0; i < Q; ++i) {
+      if (i < i0 || i >= i1) continue;
+      Store<S>::set_val(F + (size_t)i * g.dstride + s, typename Store<S>::C(in[(long long)(i - i0) * g.L + a]),
+                        p.scale);
+    }
   }
 }
 
@@ -183,8 +189,7 @@ template <int Q, class S>
 static cudaError_t import_impl(const DomainDev& d, const StepParams& p, int i0, int i1, const void* in,
                                cudaStream_t st) {
   using M = typename MacroT<S>::T;
-  dim3 block(128), grid((d.g.gz + 127) / 128, d.g.gy, d.g.gx);
-  k_import_f<Q, S><<<grid, block, 0, st>>>((S*)d.F, d.g, p, i0, i1, (const M*)in);
+  k_import_f<Q, S><<<transfer_blocks(d.g.L), 256, 0, st>>>((S*)d.F, d.g, p, i0, i1, (const M*)in);
   return cudaGetLastError();
 }
 
