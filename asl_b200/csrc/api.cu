@@ -1685,6 +1685,7 @@ struct aslb_batch {
   BatchDom* dev_doms = nullptr;
   long long ntiles = 0;
   bool any_mask = false;
+  int mask_mode = 0;  // 0 no fused links, 1 two-word masks, 2 one-word masks in every masked domain
   std::vector<BatchBc*> dev_pos;  // one table per condition position
   std::vector<int> pos_n;
   std::vector<long long> pos_links;
@@ -1741,6 +1742,7 @@ int batch_tables(aslb_batch* b, aslb_bc* const* bcs, const int* nbc) {
   b->host_doms.assign(n, BatchDom{});
   b->ntiles = 0;
   b->any_mask = false;
+  bool all_m32 = true;
   for (int i = 0; i < n; ++i) {
     aslb_lbgk* h = b->doms[i];
     BatchDom& D = b->host_doms[i];
@@ -1748,7 +1750,9 @@ int batch_tables(aslb_batch* b, aslb_bc* const* bcs, const int* nbc) {
     D.g = g;
     D.F = h->d.F;
     D.mask = h->fresh ? nullptr : h->mask_dev;
+    D.mask32 = h->fresh ? nullptr : h->mask32_dev;
     b->any_mask |= D.mask != nullptr;
+    if (D.mask && !D.mask32) all_m32 = false;
     D.rho = h->d.rho;
     D.u = h->d.u;
     D.om0f = 1.0f / (3.0f * (float)h->p.nu + 0.5f);
@@ -1757,6 +1761,8 @@ int batch_tables(aslb_batch* b, aslb_bc* const* bcs, const int* nbc) {
     D.tile0 = b->ntiles;
     b->ntiles += g.nx;
   }
+  // link-mask form of the launch: 0 none, 1 two words, 2 one word per cell
+  b->mask_mode = b->any_mask ? (all_m32 ? 2 : 1) : 0;
   ASLB_CUDA(cudaMalloc((void**)&b->dev_doms, n * sizeof(BatchDom)));
   ASLB_CUDA(cudaMemcpy(b->dev_doms, b->host_doms.data(), n * sizeof(BatchDom), cudaMemcpyHostToDevice));
   // condition positions: the j-th separate condition of every domain
@@ -1809,7 +1815,7 @@ int batch_step(aslb_batch* b) {
   aslb_lbgk* h0 = b->doms[0];
   prepare_params(h0);
   const int parity = h0->parity;
-  cudaError_t e = launch_batch_step(b->q, b->storage, b->dev_doms, (int)b->doms.size(), b->ntiles, b->any_mask,
+  cudaError_t e = launch_batch_step(b->q, b->storage, b->dev_doms, (int)b->doms.size(), b->ntiles, b->mask_mode,
                                     h0->p, parity, b->shape, b->stream);
   for (size_t j = 0; e == cudaSuccess && j < b->dev_pos.size(); ++j)
     if (b->pos_n[j] > 0)

@@ -4,19 +4,19 @@
 
 namespace aslb {
 
-cudaError_t batch_step_f32(int q, const BatchDom* doms, int ndom, long long ntiles, bool fused, const StepParams& p,
+cudaError_t batch_step_f32(int q, const BatchDom* doms, int ndom, long long ntiles, int fused, const StepParams& p,
                            int parity_in, int shape, cudaStream_t st);
-cudaError_t batch_step_f16(int q, const BatchDom* doms, int ndom, long long ntiles, bool fused, const StepParams& p,
+cudaError_t batch_step_f16(int q, const BatchDom* doms, int ndom, long long ntiles, int fused, const StepParams& p,
                            int parity_in, int shape, cudaStream_t st);
-cudaError_t batch_step_f64(int q, const BatchDom* doms, int ndom, long long ntiles, bool fused, const StepParams& p,
+cudaError_t batch_step_f64(int q, const BatchDom* doms, int ndom, long long ntiles, int fused, const StepParams& p,
                            int parity_in, int shape, cudaStream_t st);
 cudaError_t batch_links_f32(int q, const BatchBc* bcs, int nbc, long long nlinks, int parity, cudaStream_t st);
 cudaError_t batch_links_f16(int q, const BatchBc* bcs, int nbc, long long nlinks, int parity, cudaStream_t st);
 cudaError_t batch_links_f64(int q, const BatchBc* bcs, int nbc, long long nlinks, int parity, cudaStream_t st);
 
-int batch_shape_count() { return 3; }
+int batch_shape_count() { return 5; }
 
-cudaError_t launch_batch_step(int q, int storage, const BatchDom* doms, int ndom, long long ntiles, bool fused,
+cudaError_t launch_batch_step(int q, int storage, const BatchDom* doms, int ndom, long long ntiles, int fused,
                               const StepParams& p, int parity_in, int shape, cudaStream_t st) {
   switch (storage) {
     case ST_F32: return batch_step_f32(q, doms, ndom, ntiles, fused, p, parity_in, shape, st);

@@ -12,13 +12,29 @@
 
 namespace aslb {
 
-// Launch shapes of the persistent batched step: resident blocks of 256
-// threads per SM (4: 64 registers, 3: 80, 2: 128). aslb_batch_run times them
-// on the batch and keeps the fastest.
-constexpr int kBatchShapes = 3;
-__host__ __device__ constexpr int batch_shape_blocks(int shape) { return shape == 0 ? 4 : (shape == 1 ? 3 : 2); }
+// Launch shapes of the persistent batched step: one cell per thread at 4, 3
+// or 2 resident blocks of 256 threads per SM (64 / 80 / 128 registers), or
+// two cells per thread (cells l and l + 256 of a plane, both cells' loads in
+// flight before the first collision) at 3 or 2 blocks. aslb_batch_run times
+// them on the batch and keeps the fastest.
+constexpr int kBatchShapes = 5;
+__host__ __device__ constexpr int batch_shape_blocks(int shape) {
+  return shape == 0 ? 4 : (shape == 1 || shape == 3 ? 3 : 2);
+}
+__host__ __device__ constexpr bool batch_shape_pair(int shape) { return shape >= 3; }
 
-template <int Q, class S, bool ODD, bool FUSED, int BLOCKS>
+// The fused-link words of a cell: the two-word form, or the one-word form
+// (bit 31 set: the low bits are elide bits, else bounce bits).
+template <bool M32>
+__device__ __forceinline__ uint2 batch_links(const BatchDom& D, unsigned s) {
+  if (M32) {
+    const uint32_t w = D.mask32[s];
+    return (w >> 31) ? make_uint2(0u, w & 0x7fffffffu) : make_uint2(w, 0u);
+  }
+  return D.mask[s];
+}
+
+template <int Q, class S, bool ODD, bool FUSED, bool M32, int BLOCKS>
 __global__ void __launch_bounds__(256, BLOCKS)
     k_batch_step(const BatchDom* __restrict__ doms, int ndom, long long ntiles, const StepParams p) {
   using C = typename Store<S>::C;
@@ -57,7 +73,7 @@ __global__ void __launch_bounds__(256, BLOCKS)
     uint2 mnext = make_uint2(0u, 0u);
     if (FUSED && mask && threadIdx.x < plane_cells) {
       int y1, z1;
-      mnext = mask[cell_index(threadIdx.x, y1, z1)];
+      mnext = batch_links<M32>(D, cell_index(threadIdx.x, y1, z1));
     }
     for (unsigned l = threadIdx.x; l < plane_cells; l += 256u) {
       int y, z;
@@ -68,7 +84,7 @@ __global__ void __launch_bounds__(256, BLOCKS)
         elide = mnext.y;
         if (l + 256u < plane_cells) {
           int y1, z1;
-          mnext = mask[cell_index(l + 256u, y1, z1)];
+          mnext = batch_links<M32>(D, cell_index(l + 256u, y1, z1));
         }
       }
       int ox[3], oy[3], oz[3];
@@ -76,6 +92,71 @@ __global__ void __launch_bounds__(256, BLOCKS)
       C f[Q];
       cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, s, ox, oy, oz, bounce, f);
       cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, (M*)D.rho, (M*)D.u, x, y, z, s, ox, oy, oz, elide, f, om0);
+    }
+  }
+}
+
+// Two cells per thread: cells l and l + 256 of the plane.
+template <int Q, class S, bool ODD, bool FUSED, bool M32, int BLOCKS>
+__global__ void __launch_bounds__(256, BLOCKS)
+    k_batch_step_pair(const BatchDom* __restrict__ doms, int ndom, long long ntiles, const StepParams p) {
+  using C = typename Store<S>::C;
+  using M = typename MacroT<S>::T;
+  int d = -1;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    if (d < 0) {
+      int lo = 0, hi = ndom - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (doms[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
+      }
+      d = lo;
+    }
+    while (d + 1 < ndom && doms[d + 1].tile0 <= tile) ++d;
+    const BatchDom& D = doms[d];
+    const GridDesc g = D.g;
+    const int x = (int)(tile - D.tile0) + 1;
+    const unsigned plane_cells = (unsigned)(g.ny * g.nz);
+    const unsigned nz = (unsigned)g.nz, nz_inv = D.nz_inv;
+    S* F = (S*)D.F;
+    const bool masked = FUSED && D.mask;
+    const C om0 = std::is_same<C, double>::value ? C(D.om0d) : C(D.om0f);
+    auto cell_index = [&](unsigned l, int& y, int& z) {
+      unsigned yq = __umulhi(l, nz_inv);
+      if (yq * nz > l) --yq;
+      y = (int)yq + 1;
+      z = (int)(l - yq * nz) + 1;
+      return (unsigned)sidx(g, x, y, z);
+    };
+    uint2 na = make_uint2(0u, 0u), nb = make_uint2(0u, 0u);
+    if (masked) {
+      int y1, z1;
+      if (threadIdx.x < plane_cells) na = batch_links<M32>(D, cell_index(threadIdx.x, y1, z1));
+      if (threadIdx.x + 256u < plane_cells) nb = batch_links<M32>(D, cell_index(threadIdx.x + 256u, y1, z1));
+    }
+    for (unsigned l = threadIdx.x; l < plane_cells; l += 512u) {
+      const bool has_b = l + 256u < plane_cells;
+      int ya, za, yb = 0, zb = 0;
+      const unsigned sa = cell_index(l, ya, za);
+      const unsigned sb = has_b ? cell_index(l + 256u, yb, zb) : 0u;
+      const uint2 ma = na, mb = nb;
+      if (masked) {
+        int y1, z1;
+        if (l + 512u < plane_cells) na = batch_links<M32>(D, cell_index(l + 512u, y1, z1));
+        if (l + 768u < plane_cells) nb = batch_links<M32>(D, cell_index(l + 768u, y1, z1));
+      }
+      int ox[3], oya[3], oza[3], oyb[3], ozb[3];
+      nb_offsets(g, x, ya, za, ox, oya, oza);
+      C fa[Q], fb[Q];
+      cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, sa, ox, oya, oza, ma.x, fa);
+      if (has_b) {
+        nb_offsets(g, x, yb, zb, ox, oyb, ozb);
+        cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, sb, ox, oyb, ozb, mb.x, fb);
+      }
+      cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, (M*)D.rho, (M*)D.u, x, ya, za, sa, ox, oya, oza, ma.y, fa, om0);
+      if (has_b)
+        cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, (M*)D.rho, (M*)D.u, x, yb, zb, sb, ox, oyb, ozb, mb.y, fb,
+                                               om0);
     }
   }
 }
@@ -104,29 +185,63 @@ inline int batch_sm_count() {
   return g_sms;
 }
 
-template <int Q, class S, int BLOCKS>
+template <int Q, class S, int SHAPE, bool M32>
 cudaError_t batch_step_shape(const BatchDom* doms, int ndom, long long ntiles, bool fused, const StepParams& p,
                              int parity_in, cudaStream_t st) {
+  constexpr int BLOCKS = batch_shape_blocks(SHAPE);
   const long long cap = (long long)batch_sm_count() * BLOCKS;
   const int grid = (int)(ntiles < cap ? ntiles : cap);
-  if (parity_in == 0) {
-    if (fused) k_batch_step<Q, S, true, true, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
-    else k_batch_step<Q, S, true, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+  if constexpr (batch_shape_pair(SHAPE)) {
+    if (parity_in == 0) {
+      if (fused) k_batch_step_pair<Q, S, true, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+      else k_batch_step_pair<Q, S, true, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+    } else {
+      if (fused) k_batch_step_pair<Q, S, false, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+      else k_batch_step_pair<Q, S, false, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+    }
   } else {
-    if (fused) k_batch_step<Q, S, false, true, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
-    else k_batch_step<Q, S, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+    if (parity_in == 0) {
+      if (fused) k_batch_step<Q, S, true, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+      else k_batch_step<Q, S, true, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+    } else {
+      if (fused) k_batch_step<Q, S, false, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+      else k_batch_step<Q, S, false, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+    }
   }
   return cudaGetLastError();
 }
 
+// fused: 0 none, 1 two-word link masks, 2 one-word masks in every masked domain
+// Two cells per thread are built for D3Q15 / D3Q19 in 4- and 2-byte storage
+// with one-word link masks (or none); other cases take the one-cell shape
+// with the same residency.
+template <int Q, class S, int SHAPE>
+cudaError_t batch_step_m(const BatchDom* doms, int ndom, long long ntiles, int fused, const StepParams& p,
+                         int parity_in, cudaStream_t st) {
+  if constexpr (batch_shape_pair(SHAPE)) {
+    constexpr int ONE = SHAPE == 3 ? 1 : 2;
+    if constexpr (Q == 27 || sizeof(S) == 8) {
+      return batch_step_m<Q, S, ONE>(doms, ndom, ntiles, fused, p, parity_in, st);
+    } else {
+      if (fused == 1) return batch_step_m<Q, S, ONE>(doms, ndom, ntiles, fused, p, parity_in, st);
+      return batch_step_shape<Q, S, SHAPE, true>(doms, ndom, ntiles, fused != 0, p, parity_in, st);
+    }
+  } else {
+    if (fused == 2) return batch_step_shape<Q, S, SHAPE, true>(doms, ndom, ntiles, true, p, parity_in, st);
+    return batch_step_shape<Q, S, SHAPE, false>(doms, ndom, ntiles, fused != 0, p, parity_in, st);
+  }
+}
+
 template <int Q, class S>
-cudaError_t batch_step_impl(const BatchDom* doms, int ndom, long long ntiles, bool fused, const StepParams& p,
+cudaError_t batch_step_impl(const BatchDom* doms, int ndom, long long ntiles, int fused, const StepParams& p,
                             int parity_in, int shape, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
   switch (shape) {
-    case 0: return batch_step_shape<Q, S, batch_shape_blocks(0)>(doms, ndom, ntiles, fused, p, parity_in, st);
-    case 1: return batch_step_shape<Q, S, batch_shape_blocks(1)>(doms, ndom, ntiles, fused, p, parity_in, st);
-    case 2: return batch_step_shape<Q, S, batch_shape_blocks(2)>(doms, ndom, ntiles, fused, p, parity_in, st);
+    case 0: return batch_step_m<Q, S, 0>(doms, ndom, ntiles, fused, p, parity_in, st);
+    case 1: return batch_step_m<Q, S, 1>(doms, ndom, ntiles, fused, p, parity_in, st);
+    case 2: return batch_step_m<Q, S, 2>(doms, ndom, ntiles, fused, p, parity_in, st);
+    case 3: return batch_step_m<Q, S, 3>(doms, ndom, ntiles, fused, p, parity_in, st);
+    case 4: return batch_step_m<Q, S, 4>(doms, ndom, ntiles, fused, p, parity_in, st);
   }
   return cudaErrorInvalidValue;
 }

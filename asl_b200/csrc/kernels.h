@@ -102,6 +102,7 @@ struct BatchDom {
   GridDesc g;
   void* F;
   const uint2* mask;  // fused links, or null
+  const uint32_t* mask32;  // the same links in one word per cell (null when a cell has both kinds)
   void* rho;
   void* u;
   float om0f;
@@ -121,7 +122,7 @@ struct BatchBc {
 // One stream-collide step of every domain of a batch (same lattice, storage
 // and parity; CL_NONE), a persistent grid over all domains' tiles; `shape`
 // (0 .. batch_shape_count() - 1) picks the resident blocks per SM.
-cudaError_t launch_batch_step(int q, int storage, const BatchDom* doms, int ndom, long long ntiles, bool fused,
+cudaError_t launch_batch_step(int q, int storage, const BatchDom* doms, int ndom, long long ntiles, int fused,
                               const StepParams& p, int parity_in, int shape, cudaStream_t st);
 int batch_shape_count();
 // Every link of the entries (one condition position across the batch).

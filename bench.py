@@ -449,7 +449,7 @@ def batch_run(W, n: int, steps: int, peak: float):
     cells = sum(w.cells for w in ws)
     batch, lbs, bcs = W.build_batch(ws, storage="f32", fuse=True)
     st = torch.cuda.ExternalStream(lbs[0].stream)
-    batch.run(6, bcs)
+    batch.run(16, bcs)  # warm-up, long enough for the launch-shape tuner (2 steps per shape)
     batch.sync()
     torch.cuda.synchronize()
 
@@ -482,7 +482,9 @@ def batch_run(W, n: int, steps: int, peak: float):
     bpc = BYTES_PER_CELL[("f32", 19)]
     res = {"domains": n, "cells": cells, "steps": steps, "value": cells * steps / t / 1e6, "unit": "MLUPS",
            "ms_per_step": t / steps * 1e3, "launches_per_step": launches, "tiles_per_step": batch.tiles,
-           "layout": "packed rows", "launch_shape": {"chosen": batch.shape, "blocks_per_sm": [4, 3, 2],
+           "layout": "packed rows", "launch_shape": {"chosen": batch.shape,
+                                                     "shapes": ["1 cell, 4 blocks/SM", "1 cell, 3", "1 cell, 2",
+                                                                "2 cells, 3", "2 cells, 2"],
                                                      "tuning_ms_per_2_steps": batch.shape_times},
            "kernel_ms": tk * 1e3, "kernel_frac_of_peak": bpc * cells / tk / 1e9 / peak,
            "separate_launches": {"value": cells * sep_steps / t_sep / 1e6, "unit": "MLUPS", "steps": sep_steps,

@@ -414,8 +414,11 @@ int aslb_batch_run(aslb_batch* b, int nsteps, aslb_bc* const* bcs, const int* nb
 int aslb_batch_sync(aslb_batch* b);
 /* Tiles (x planes) of one batched step, over all domains. */
 long long aslb_batch_tiles(aslb_batch* b);
-/* Launch shape of the batched step: resident blocks of 256 threads per SM,
- * shape 0: 4, 1: 3, 2: 2. By default (or after shape -1) the first
+/* Launch shape of the batched step: shape 0, 1, 2: one cell per thread at
+ * 4, 3, 2 resident blocks of 256 threads per SM; 3, 4: two cells per thread
+ * at 3, 2 blocks (D3Q15 / D3Q19, FP32 / FP16, one-word link masks; other
+ * batches take the one-cell shape of the same residency). By default (or
+ * after shape -1) the first
  * aslb_batch_run that records a graph first times two real steps with every
  * shape and keeps the fastest (all shapes give identical results);
  * aslb_batch_shape_times returns those timings (ms, up to n; the count). */

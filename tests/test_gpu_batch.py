@@ -78,11 +78,15 @@ def test_batch_rejects_mismatched_domains(gpu):
         batch.run(2, bcs)
 
 
-def test_batch_launch_shapes_identical_and_tuned(gpu):
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_batch_launch_shapes_identical_and_tuned(gpu, storage):
+    """Every launch shape (one cell per thread at 4 / 3 / 2 blocks per SM, two
+    cells per thread at 3 / 2) gives the same populations; the tuner times
+    them all and keeps the fastest."""
     ws = small_batch(3, seed=17)
     out = []
-    for shape in (0, 1, 2):
-        batch, lbs, bcs = W.build_batch(ws)
+    for shape in (0, 1, 2, 3, 4):
+        batch, lbs, bcs = W.build_batch(ws, storage=storage)
         batch.setShape(shape)
         batch.run(6, bcs)
         batch.sync()
@@ -91,10 +95,10 @@ def test_batch_launch_shapes_identical_and_tuned(gpu):
     for other in out[1:]:
         for a, b in zip(out[0], other):
             assert np.array_equal(a, b, equal_nan=True)
-    batch, lbs, bcs = W.build_batch(ws)
-    batch.run(12, bcs)  # long enough for the tuner: 2 steps per shape first
+    batch, lbs, bcs = W.build_batch(ws, storage=storage)
+    batch.run(14, bcs)  # long enough for the tuner: a first step, then 2 steps per shape
     batch.sync()
     t = batch.shape_times
-    assert len(t) == 3 and batch.shape == int(np.argmin(t))
+    assert len(t) == 5 and batch.shape == int(np.argmin(t))
     for lb in lbs:
-        assert lb.steps == 12
+        assert lb.steps == 14
