@@ -144,10 +144,12 @@ __global__ void __launch_bounds__(256) k_export_f(const S* __restrict__ F, const
                                                   int parity, int i0, int i1,
                                                   typename MacroT<S>::T* __restrict__ out) {
   using M = typename MacroT<S>::T;
-  for (long long a = (long long)blockIdx.x * blockDim.x + threadIdx.x; a < g.L; a += (long long)gridDim.x * blockDim.x) {
-    const int z = (int)(a % g.gz);
-    const long long r = a / g.gz;
-    const int y = (int)(r % g.gy), x = (int)(r / g.gy);
+  // 32-bit index arithmetic (L < 2^32): 64-bit divisions cost a slow subroutine per cell
+  const unsigned L = (unsigned)g.L, gz = (unsigned)g.gz, gy = (unsigned)g.gy;
+  for (unsigned a = blockIdx.x * blockDim.x + threadIdx.x; a < L; a += gridDim.x * blockDim.x) {
+    const unsigned r = a / gz;
+    const int z = (int)(a - r * gz);
+    const int x = (int)(r / gy), y = (int)(r - (unsigned)x * gy);
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
       if (i < i0 || i >= i1) continue;
@@ -173,9 +175,11 @@ cudaError_t launch_export_f(const DomainDev& d, const StepParams& p, int parity,
 template <int Q, class S>
 __global__ void __launch_bounds__(256) k_import_f(S* __restrict__ F, const GridDesc g, const StepParams p, int i0,
                                                   int i1, const typename MacroT<S>::T* __restrict__ in) {
-  for (long long a = (long long)blockIdx.x * blockDim.x + threadIdx.x; a < g.L; a += (long long)gridDim.x * blockDim.x) {
+  const unsigned L = (unsigned)g.L, gz = (unsigned)g.gz;
+  for (unsigned a = blockIdx.x * blockDim.x + threadIdx.x; a < L; a += gridDim.x * blockDim.x) {
     // storage index: the rows (x, y) are in the same order in both layouts
-    const long long s = (a / g.gz) * g.pitch + g.zoff + a % g.gz;
+    const unsigned r = a / gz;
+    const long long s = (long long)r * g.pitch + g.zoff + (a - r * gz);
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
       if (i < i0 || i >= i1) continue;
