@@ -528,6 +528,23 @@ inline SPDistanceFunction generateDFCylinder(double R, const AVec<>& l, const AV
   return generateDFCylinderInf(R, l, c) & generateDFPlane(l, c + l * 0.5) & generateDFPlane(-l, c - l * 0.5);
 }
 
+// The block's outer layer as a solid: the union of the six half-spaces
+// beyond the planes nG - 1/2 cells inside its faces (src/aslGeomInc.cxx:
+// 162-183), positive inside those planes and negative beyond them.
+inline SPDistanceFunction generateDFInBlock(const Block& b, unsigned int nG) {
+  if (nD(b) != 3) errorMessage("generateDFInBlock: three-dimensional blocks only");
+  const AVec<> offs(3, (double(nG) - .5) * b.dx);
+  const AVec<> p0 = b.position + offs, pE = b.getBPosition() - offs;
+  SPDistanceFunction res;
+  for (int d = 0; d < 3; ++d) {
+    AVec<> nc(3, 0.);
+    nc[d] = 1.;
+    SPDistanceFunction pair = generateDFPlane(nc, p0) | generateDFPlane(-nc, pE);
+    res = d == 0 ? pair : (res | pair);
+  }
+  return res;
+}
+
 // normalize(df, dx) = clip(df / (1.8 dx), -1, 1) (DistFNormalization,
 // src/math/aslDistanceFunction.cxx:142-165)
 inline SPDistanceFunction normalize(SPDistanceFunction a, double dx) {
