@@ -528,6 +528,41 @@ inline SPDistanceFunction generateDFCylinder(double R, const AVec<>& l, const AV
   return generateDFCylinderInf(R, l, c) & generateDFPlane(l, c + l * 0.5) & generateDFPlane(-l, c - l * 0.5);
 }
 
+// Convex solids over a convex polygon given by its points in order
+// (src/aslGeomInc.cxx:123-160): the intersection of the half-spaces behind
+// the plane through each edge, that plane parallel to the polygon's axis (a
+// prism, unbounded along the axis) or through the apex a (a pyramid, closed
+// by the polygon's own plane).
+namespace aslb_detail {
+inline AVec<> polygon_center(const std::vector<AVec<double>>& points) {
+  if (points.size() < 3) errorMessage("generateDFConvexPolygon: three points at least");
+  AVec<> c = points[0];
+  for (size_t i = 1; i < points.size(); ++i) c += points[i];
+  return c / double(points.size());
+}
+}  // namespace aslb_detail
+inline SPDistanceFunction generateDFConvexPolygonPrism(std::vector<AVec<double>> points) {
+  const AVec<> c = aslb_detail::polygon_center(points);
+  const AVec<> axis = crossProduct(points[0] - c, points[1] - c);
+  SPDistanceFunction res;
+  for (size_t i = 0; i < points.size(); ++i) {
+    const AVec<>& p = points[i];
+    SPDistanceFunction side = generateDFPlane(crossProduct(points[(i + 1) % points.size()] - p, axis), p);
+    res = i == 0 ? side : (res & side);
+  }
+  return res;
+}
+inline SPDistanceFunction generateDFConvexPolygonPyramid(std::vector<AVec<double>> points, AVec<double> a) {
+  const AVec<> c = aslb_detail::polygon_center(points);
+  const AVec<> axis = crossProduct(points[0] - c, points[1] - c);
+  SPDistanceFunction res = generateDFPlane(-axis, c);
+  for (size_t i = 0; i < points.size(); ++i) {
+    const AVec<>& p = points[i];
+    res = res & generateDFPlane(crossProduct(points[(i + 1) % points.size()] - p, a - p), p);
+  }
+  return res;
+}
+
 // The block's outer layer as a solid: the union of the six half-spaces
 // beyond the planes nG - 1/2 cells inside its faces (src/aslGeomInc.cxx:
 // 162-183), positive inside those planes and negative beyond them.
@@ -586,6 +621,25 @@ inline void initData(SPAbstractData d, SPDistanceFunction df) {
 template <class D>
 inline void initData(std::shared_ptr<D> d, SPDistanceFunction df) {
   initData(std::static_pointer_cast<AbstractData>(d), df);
+}
+// The same value in every cell, per component (src/aslDataInc.h:36-37),
+// for host containers.
+inline void initData(SPAbstractData d, const AVec<double>& a) {
+  if (d->bound()) errorMessage("initData: the container is a view of a device field");
+  if (a.getSize() != d->getEContainerSize()) errorMessage("initData: the value has another number of components");
+  std::vector<double>& v = d->values();
+  const size_t n = d->cells();
+  for (unsigned int c = 0; c < a.getSize(); ++c)
+    std::fill(v.begin() + (std::ptrdiff_t)(c * n), v.begin() + (std::ptrdiff_t)((c + 1) * n), a[c]);
+}
+inline void initData(SPAbstractData d, double a) { initData(d, AVec<double>(d->getEContainerSize(), a)); }
+template <class D>
+inline void initData(std::shared_ptr<D> d, const AVec<double>& a) {
+  initData(std::static_pointer_cast<AbstractData>(d), a);
+}
+template <class D>
+inline void initData(std::shared_ptr<D> d, double a) {
+  initData(std::static_pointer_cast<AbstractData>(d), a);
 }
 
 // A container holding the function's values (ASL's formula-backed data,

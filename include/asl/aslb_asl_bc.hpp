@@ -72,6 +72,16 @@ class BCSlices : public BCLBGKCommon {
   }
 };
 
+// The free forms of src/num/aslBCond.h:311-319 (programs call them on the
+// condition object, e.g. addSliceX0(bcIn)).
+inline void addSliceX0(BCSlices& b) { b.addSliceX0(); }
+inline void addSliceXE(BCSlices& b) { b.addSliceXE(); }
+inline void addSliceY0(BCSlices& b) { b.addSliceY0(); }
+inline void addSliceYE(BCSlices& b) { b.addSliceYE(); }
+inline void addSliceZ0(BCSlices& b) { b.addSliceZ0(); }
+inline void addSliceZE(BCSlices& b) { b.addSliceZE(); }
+inline void addSlices(BCSlices& b, const std::vector<SlicesNames>& sl) { b.addSlices(sl); }
+
 // f_k(p) = f_inv(k)(q)
 class BCNoSlip : public BCSlices {
  public:

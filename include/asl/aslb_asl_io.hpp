@@ -9,6 +9,9 @@
 #ifndef ASLB_ASL_IO_HPP
 #define ASLB_ASL_IO_HPP
 
+#include <cctype>
+#include <filesystem>
+
 #include "aslb_asl.hpp"
 
 namespace asl {
@@ -214,9 +217,13 @@ class Parameter {
 class ParametersManager {
  protected:
   std::string name_, version_;
+  std::string dir_;  // absolute directory of the parameters file, with a trailing '/'
 
  public:
   ParametersManager() {}
+  // the directory of the parameters file given to load(), else the current
+  // one (src/utilities/aslParametersManager.cxx:352-355, 487-492)
+  std::string getDir() { return dir_; }
   // "key = value" lines
   void loadParametersFile(const std::string& path) {
     std::ifstream in(path);
@@ -255,6 +262,7 @@ class ApplicationParametersManager : public ParametersManager {
   }
   void load(int argc, char* argv[]) {
     int device = -1;
+    std::filesystem::path dir(".");
     for (int i = 1; i < argc; ++i) {
       std::string a = argv[i];
       if (a == "-h" || a == "--help") {
@@ -283,13 +291,93 @@ class ApplicationParametersManager : public ParametersManager {
         }
       } else {
         loadParametersFile(a);
+        dir = std::filesystem::path(a).parent_path();
+        if (dir.empty()) dir = ".";
       }
     }
+    std::error_code ec;
+    const std::filesystem::path abs = std::filesystem::canonical(dir, ec);
+    dir_ = (ec ? dir : abs).string();
+    if (dir_.empty() || dir_.back() != '/') dir_ += '/';
     for (auto& e : aslb_detail::param_registry())
       if (e.required) errorMessage("the parameter \"" + e.key + "\" is required");
     if (device >= 0) aslb_detail::check(aslb_set_device(device), "ApplicationParametersManager: --device");
   }
 };
+
+// ---- readSurface (src/readers/aslVTKFormatReaders.h:66-80) -------------------
+//
+// An STL surface (binary or ASCII) sampled into a map by the library's CUDA
+// distance kernels (aslb_read_stl, aslb_surface_map), as ASL's surfaceToData
+// samples VTK's implicit modeller (src/readers/aslVTKFormatReaders.cxx:
+// 132-216): the unsigned distance d to the nearest triangle (exact within
+// four cells of the surface) stored as (d - 1.2 dx) / (1.8 dx) on the given
+// block, or as (d - 1.8 dx) / (1.8 dx) on the surface's bounds grown by
+// 3.6 dx, or by the given fractions of its extent per face. The sampled grid
+// is the container's block with its ghost layer. File coordinates (x, y, z)
+// are ASL's (z, y, x). VTK XML PolyData (.vtp) is read by the Python
+// library's reader (asl_b200.surface); here it is reported as unsupported.
+namespace aslb_detail {
+inline std::vector<float> surface_triangles(const std::string& fileName) {
+  std::string ext = fileName.size() >= 4 ? fileName.substr(fileName.size() - 4) : std::string();
+  for (char& ch : ext) ch = (char)std::tolower((unsigned char)ch);
+  if (ext != ".stl") errorMessage("Reader: file format not supported");
+  long long n = 0;
+  check(aslb_read_stl(fileName.c_str(), nullptr, 0, &n), "readSurface");
+  if (n < 1) errorMessage("readSurface: empty surface");
+  std::vector<float> tri((size_t)n * 9);
+  check(aslb_read_stl(fileName.c_str(), tri.data(), n, &n), "readSurface");
+  for (size_t v = 0; v < tri.size(); v += 3) std::swap(tri[v], tri[v + 2]);
+  return tri;
+}
+inline SPDataWithGhostNodesACLData sample_surface(const std::vector<float>& tri, const AVec<int>& size,
+                                                  const AVec<>& pos0, double dx, double offset, double scale) {
+  if (nD(size) != 3 || minComponent(size) < 3) errorMessage("readSurface: the sampled grid has no interior");
+  std::vector<float> m((size_t)size[0] * size[1] * size[2]);
+  const double p0[3] = {pos0[0], pos0[1], pos0[2]};
+  check(aslb_surface_map(tri.data(), (long long)(tri.size() / 9), size[0], size[1], size[2], p0, dx, 4.0 * dx, 0,
+                         offset, scale, m.data()),
+        "readSurface");
+  auto d = std::make_shared<DataWithGhostNodesACLData>(
+      Block(size - AVec<int>(3, 2), dx, pos0 + AVec<>(3, dx)), 1u, 1u, acl::TYPE_FLOAT);
+  std::vector<double>& v = d->values();
+  for (size_t i = 0; i < m.size(); ++i) v[i] = m[i];
+  return d;
+}
+inline SPDataWithGhostNodesACLData surface_on_bounds(const std::vector<float>& tri, double dx, const double* off) {
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) lo[a] = hi[a] = tri[a];
+  for (size_t v = 0; v < tri.size(); v += 3)
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], (double)tri[v + a]);
+      hi[a] = std::max(hi[a], (double)tri[v + a]);
+    }
+  AVec<int> size(3);
+  AVec<> pos0(3);
+  for (int a = 0; a < 3; ++a) {
+    const double ext = hi[a] - lo[a];
+    const double l = off ? lo[a] - ext * off[2 * a] : lo[a] - 3.6 * dx;
+    const double h = off ? hi[a] + ext * off[2 * a + 1] : hi[a] + 3.6 * dx;
+    size[a] = int(std::floor((h - l) / dx)) + 1;
+    pos0[a] = l;
+  }
+  return sample_surface(tri, size, pos0, dx, 1.8 * dx, 1.8 * dx);
+}
+}  // namespace aslb_detail
+
+inline SPDataWithGhostNodesACLData readSurface(const std::string& fileName, Block& b) {
+  return aslb_detail::sample_surface(aslb_detail::surface_triangles(fileName), b.getSize(), b.position, b.dx,
+                                     1.2 * b.dx, 1.8 * b.dx);
+}
+inline SPDataWithGhostNodesACLData readSurface(const std::string& fileName, double dx) {
+  return aslb_detail::surface_on_bounds(aslb_detail::surface_triangles(fileName), dx, nullptr);
+}
+inline SPDataWithGhostNodesACLData readSurface(const std::string& fileName, double dx, double offset_X0,
+                                               double offset_XE, double offset_Y0, double offset_YE,
+                                               double offset_Z0, double offset_ZE) {
+  const double off[6] = {offset_X0, offset_XE, offset_Y0, offset_YE, offset_Z0, offset_ZE};
+  return aslb_detail::surface_on_bounds(aslb_detail::surface_triangles(fileName), dx, off);
+}
 
 }  // namespace asl
 

@@ -2,5 +2,5 @@
  * aslb_asl.hpp (over the C ABI of libaslb.so, aslb.h). */
 #ifndef ASLB_FACADE_WRITERS_ASLVTKFORMATWRITERS_H
 #define ASLB_FACADE_WRITERS_ASLVTKFORMATWRITERS_H
-#include "../aslb_asl_io.hpp"
+#include "../aslb_asl_std.hpp"
 #endif
