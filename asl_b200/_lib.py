@@ -38,6 +38,7 @@ PROTOTYPES = {
     "aslb_last_error": (C.c_char_p, []),
     "aslb_version": (C.c_char_p, []),
     "aslb_set_device": (C.c_int, [C.c_int]),
+    "aslb_synchronize": (C.c_int, []),
     "aslb_lbgk_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint,
                                    C.POINTER(_vp)]),
     "aslb_lbgk_destroy": (C.c_int, [_vp]),

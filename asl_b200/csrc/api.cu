@@ -397,6 +397,17 @@ int aslb_set_device(int device) {
   return ASLB_OK;
 }
 
+int aslb_synchronize(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(ASLB_ERR_CUDA, "aslb_synchronize: no CUDA device");
+  }
+  ASLB_CUDA(cudaSetDevice(g_device));
+  ASLB_CUDA(cudaDeviceSynchronize());
+  return ASLB_OK;
+}
+
 int aslb_lbgk_create(int nx, int ny, int nz, int q, int storage, double nu, unsigned flags, aslb_lbgk** out) {
   if (!out) return fail(ASLB_ERR_ARG, "aslb_lbgk_create: out is null");
   *out = nullptr;

@@ -509,17 +509,27 @@ inline SPDistanceFunction generateDFPlane(const AVec<>& n, const AVec<>& p0) {
 }
 
 // union (min), intersection (max), inversion (negation)
+// An operand that is not initialised (a null pointer) leaves the other one
+// as the result, as in src/aslGeomInc.cxx:39-66 (programs start unions from
+// an empty SPDistanceFunction); both null, or a null negated, is an error.
 inline SPDistanceFunction operator|(SPDistanceFunction a, SPDistanceFunction b) {
+  if (!a && !b) errorMessage("DistanceFunction::operator| - both operands are not initialized");
+  if (!a) return b;
+  if (!b) return a;
   return aslb_detail::make_df([=](auto x, auto y, auto z) {
     return std::min(a->getDistance(x, y, z), b->getDistance(x, y, z));
   });
 }
 inline SPDistanceFunction operator&(SPDistanceFunction a, SPDistanceFunction b) {
+  if (!a && !b) errorMessage("DistanceFunction::operator& - both operands are not initialized");
+  if (!a) return b;
+  if (!b) return a;
   return aslb_detail::make_df([=](auto x, auto y, auto z) {
     return std::max(a->getDistance(x, y, z), b->getDistance(x, y, z));
   });
 }
 inline SPDistanceFunction operator-(SPDistanceFunction a) {
+  if (!a) errorMessage("DistanceFunction::operator- - operand is not initialized");
   return aslb_detail::make_df([=](auto x, auto y, auto z) { return -a->getDistance(x, y, z); });
 }
 
@@ -583,6 +593,7 @@ inline SPDistanceFunction generateDFInBlock(const Block& b, unsigned int nG) {
 // normalize(df, dx) = clip(df / (1.8 dx), -1, 1) (DistFNormalization,
 // src/math/aslDistanceFunction.cxx:142-165)
 inline SPDistanceFunction normalize(SPDistanceFunction a, double dx) {
+  if (!a) errorMessage("DistanceFunction::normalize - argument is not initialized");
   const double factor = 1.0 / dx / 1.8;
   return aslb_detail::make_df([=](auto x, auto y, auto z) {
     using T = decltype(x);
@@ -595,6 +606,7 @@ inline SPDistanceFunction normalize(SPDistanceFunction a, double dx) {
 // Values of df at the positions of the container's (ghosted) cells,
 // position + (i - ghost) dx (src/aslGeomInc.cxx:198-210).
 inline void initData(SPAbstractData d, SPDistanceFunction df) {
+  if (!df) errorMessage("initData: the distance function is not initialized");
   const Block g = d->getBlock();
   const AVec<int> s = g.getSize();
   std::vector<double>& v = d->values();

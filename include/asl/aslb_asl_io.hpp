@@ -103,6 +103,10 @@ class WriterVTKXML {
 
 // ---- Timer (src/utilities/aslTimer.h:32-52) ----------------------------------
 
+//
+// start() and stop() first wait for the work queued on the device
+// (aslb_synchronize), so the timer measures finished steps as ASL's blocking
+// launches do; without a device they only read the clocks.
 class Timer {
   std::chrono::high_resolution_clock::time_point realTimeMark_;
   std::clock_t processorTimeMark_ = 0;
@@ -111,10 +115,12 @@ class Timer {
 
  public:
   void start() {
+    (void)aslb_synchronize();
     processorTimeMark_ = std::clock();
     realTimeMark_ = std::chrono::high_resolution_clock::now();
   }
   void stop() {
+    (void)aslb_synchronize();
     processorTimeElapsed_ += double(std::clock() - processorTimeMark_);
     realTimeElapsed_ += std::chrono::duration_cast<std::chrono::duration<double>>(
         std::chrono::high_resolution_clock::now() - realTimeMark_);

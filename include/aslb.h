@@ -103,6 +103,11 @@ const char* aslb_version(void);
 /* Select the CUDA device used by subsequent create calls
  * (ApplicationParametersManager --device, src/acl/aclHardware.cxx:98-120). */
 int aslb_set_device(int device);
+/* Wait until every launch and copy the library queued on the selected device
+ * has finished. ASL's kernels block the host (src/acl/aclKernel.cxx:311), so
+ * a program's Timer measures finished work; the C++ API's Timer::start/stop
+ * call this so that it still does when steps are queued asynchronously. */
+int aslb_synchronize(void);
 
 /* ---- LBGK domain ------------------------------------------------------- */
 

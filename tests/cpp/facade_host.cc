@@ -65,6 +65,9 @@ int main(int argc, char* argv[]) {
              ->getDistance(0., 0., 0.) == 0.0);
   auto cyl = asl::generateDFCylinder(1.0, makeAVec(0., 0., 2.), makeAVec(0., 0., 0.));
   EXPECT(cyl->getDistance(0., 0., 0.) == -1.0 && cyl->getDistance(0., 0., 3.) == 2.0);
+  // an empty operand leaves the other one (unions built up from nothing)
+  asl::SPDistanceFunction none;
+  EXPECT((none | u) == u && (u & none) == u);
   auto inb = asl::generateDFInBlock(asl::Block(makeAVec(10, 10, 10), 1.0), 0);
   EXPECT(inb->getDistance(4.5, 4.5, 4.5) == 5.0 && inb->getDistance(-1., 4.5, 4.5) == -0.5 &&
          inb->getDistance(4.5, 4.5, 10.) == -0.5);
