@@ -21,11 +21,20 @@ class DistanceFunction:
     def distance(self, pos: np.ndarray) -> np.ndarray:  # pos: (3, ...) float32
         raise NotImplementedError
 
+    # An operand that is None leaves the other one, as ASL's operators do
+    # with an uninitialised SPDistanceFunction (aslGeomInc.cxx:39-66), so a
+    # union can be built up from nothing.
     def __or__(self, other):  # union
-        return _Binary(self, other, np.minimum)
+        return self if other is None else _Binary(self, other, np.minimum)
+
+    def __ror__(self, other):
+        return self if other is None else _Binary(other, self, np.minimum)
 
     def __and__(self, other):  # intersection
-        return _Binary(self, other, np.maximum)
+        return self if other is None else _Binary(self, other, np.maximum)
+
+    def __rand__(self, other):
+        return self if other is None else _Binary(other, self, np.maximum)
 
     def __neg__(self):
         return _Unary(self, lambda d: -d)

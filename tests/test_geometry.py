@@ -115,3 +115,13 @@ def test_vehicle_workload_is_seeded_and_on_the_floor():
     # every obstacle stands on the floor: solid cells in the first layer, none at the top
     assert solid[:, :, 0].any() and not solid[:, :, -1].any()
     assert [s.kind for s in a.bcs] == ["velocity", "pressure", "map_noslip"]
+
+
+def test_union_and_intersection_start_from_none():
+    """ASL's operators take an uninitialised operand as the identity."""
+    s = G.generateDFSphere(2.0, (3.0, 3.0, 3.0))
+    block = Block((6, 6, 6), 1.0)
+    acc = None
+    acc = acc | s
+    assert acc is s and (s | None) is s and (None & s) is s and (s & None) is s
+    assert np.array_equal(G.initData(block, acc), G.initData(block, s))
