@@ -1695,6 +1695,8 @@ struct aslb_batch {
   std::vector<BatchDom> host_doms;
   BatchDom* dev_doms = nullptr;
   long long ntiles = 0;
+  long long* dev_starts = nullptr;  // the work split's run tables (BatchWork)
+  BatchWork work{};
   bool any_mask = false;
   int mask_mode = 0;  // 0 no fused links, 1 two-word masks, 2 one-word masks in every masked domain
   std::vector<BatchBc*> dev_pos;  // one table per condition position
@@ -1728,6 +1730,9 @@ namespace {
 void batch_free_tables(aslb_batch* b) {
   cudaFree(b->dev_doms);
   b->dev_doms = nullptr;
+  cudaFree(b->dev_starts);
+  b->dev_starts = nullptr;
+  b->work = BatchWork{};
   for (BatchBc* t : b->dev_pos) cudaFree(t);
   b->dev_pos.clear();
   b->pos_n.clear();
@@ -1776,6 +1781,22 @@ int batch_tables(aslb_batch* b, aslb_bc* const* bcs, const int* nbc) {
   b->mask_mode = b->any_mask ? (all_m32 ? 2 : 1) : 0;
   ASLB_CUDA(cudaMalloc((void**)&b->dev_doms, n * sizeof(BatchDom)));
   ASLB_CUDA(cudaMemcpy(b->dev_doms, b->host_doms.data(), n * sizeof(BatchDom), cudaMemcpyHostToDevice));
+  // the work split: contiguous runs of tiles with equal shares of the cells
+  {
+    std::vector<long long> tile_cells;
+    tile_cells.reserve((size_t)b->ntiles);
+    for (const BatchDom& D : b->host_doms)
+      for (int x = 0; x < D.g.nx; ++x) tile_cells.push_back((long long)D.g.ny * D.g.nz);
+    int dev = 0, sms = 0;
+    ASLB_CUDA(cudaGetDevice(&dev));
+    ASLB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    std::vector<long long> starts;
+    batch_work_tables(tile_cells, sms, starts, b->work.grid, b->work.off);
+    ASLB_CUDA(cudaMalloc((void**)&b->dev_starts, starts.size() * sizeof(long long)));
+    ASLB_CUDA(cudaMemcpy(b->dev_starts, starts.data(), starts.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    b->work.ntiles = b->ntiles;
+    b->work.starts = b->dev_starts;
+  }
   // condition positions: the j-th separate condition of every domain
   std::vector<std::vector<BatchBc>> pos;
   std::vector<long long> pos_total;
@@ -1826,7 +1847,7 @@ int batch_step(aslb_batch* b) {
   aslb_lbgk* h0 = b->doms[0];
   prepare_params(h0);
   const int parity = h0->parity;
-  cudaError_t e = launch_batch_step(b->q, b->storage, b->dev_doms, (int)b->doms.size(), b->ntiles, b->mask_mode,
+  cudaError_t e = launch_batch_step(b->q, b->storage, b->dev_doms, (int)b->doms.size(), b->work, b->mask_mode,
                                     h0->p, parity, b->shape, b->stream);
   for (size_t j = 0; e == cudaSuccess && j < b->dev_pos.size(); ++j)
     if (b->pos_n[j] > 0)

@@ -4,7 +4,10 @@
 // launch per domain and condition. Each domain keeps its own allocation and
 // layout; a device table maps the launch's tiles (one x plane of one domain,
 // its cells taken 256 at a time, z fastest across y rows) and links to
-// domains. Instantiated per storage in batch_<type>.cu.
+// domains. Each block of the persistent grid takes a contiguous run of tiles
+// holding an equal share of the batch's cells (BatchWork), so its domain
+// changes rarely and consecutive planes of a domain follow one another.
+// Instantiated per storage in batch_<type>.cu.
 #pragma once
 #include "kernels.h"
 #include "stream_collide.cuh"
@@ -34,64 +37,88 @@ __device__ __forceinline__ uint2 batch_links(const BatchDom& D, unsigned s) {
   return D.mask[s];
 }
 
+// The domain holding `tile`, searched from d (tiles ascend in the table).
+__device__ __forceinline__ int batch_domain(const BatchDom* __restrict__ doms, int ndom, long long tile, int d) {
+  if (d < 0) {
+    int lo = 0, hi = ndom - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (doms[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+  }
+  while (d + 1 < ndom && doms[d + 1].tile0 <= tile) ++d;
+  return d;
+}
+
+// One cell per thread. A block walks its run of tiles; the tiles of one
+// domain in the run are consecutive x planes, walked as one sequence of
+// cells 256 at a time, so the next cell's link word is fetched one step
+// ahead across plane boundaries too and the domain's table entry is read
+// once per domain, not once per plane.
 template <int Q, class S, bool ODD, bool FUSED, bool M32, int BLOCKS>
 __global__ void __launch_bounds__(256, BLOCKS)
-    k_batch_step(const BatchDom* __restrict__ doms, int ndom, long long ntiles, const StepParams p) {
+    k_batch_step(const BatchDom* __restrict__ doms, int ndom, const long long* __restrict__ starts,
+                 const StepParams p) {
   using C = typename Store<S>::C;
   using M = typename MacroT<S>::T;
+  long long tile = starts[blockIdx.x];
+  const long long tend = starts[blockIdx.x + 1];
   int d = -1;
-  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    // a block's tiles only move forward: advance the domain index
-    if (d < 0) {
-      int lo = 0, hi = ndom - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (doms[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
-      }
-      d = lo;
-    }
-    while (d + 1 < ndom && doms[d + 1].tile0 <= tile) ++d;
+  while (tile < tend) {
+    d = batch_domain(doms, ndom, tile, d);
     const BatchDom& D = doms[d];
     const GridDesc g = D.g;
-    const int x = (int)(tile - D.tile0) + 1;  // one tile = one x plane
+    // this domain's planes in the run
+    const int xa = (int)(tile - D.tile0) + 1;
+    const int xb = (int)(min(tend, D.tile0 + g.nx) - D.tile0);
+    tile = D.tile0 + xb;
     const unsigned plane_cells = (unsigned)(g.ny * g.nz);
     const unsigned nz = (unsigned)g.nz, nz_inv = D.nz_inv;
     S* F = (S*)D.F;
-    const uint2* mask = D.mask;
     const C om0 = std::is_same<C, double>::value ? C(D.om0d) : C(D.om0f);
-    // storage index of plane cell l (y rows of nz cells, z fastest)
-    auto cell_index = [&](unsigned l, int& y, int& z) {
+    const bool masked = FUSED && (M32 ? D.mask32 != nullptr : D.mask != nullptr);
+    // storage index of cell l of plane x (y rows of nz cells, z fastest)
+    auto cell_index = [&](int x, unsigned l, int& y, int& z) {
       unsigned yq = __umulhi(l, nz_inv);
       if (yq * nz > l) --yq;  // exact quotient for l < 2^32 / nz
       y = (int)yq + 1;
       z = (int)(l - yq * nz) + 1;
       return (unsigned)sidx(g, x, y, z);
     };
-    // the fused-link words of a thread's next cell are loaded one iteration
-    // ahead: the population addresses depend on them, so they must not cost
-    // a second memory round trip
-    uint2 mnext = make_uint2(0u, 0u);
-    if (FUSED && mask && threadIdx.x < plane_cells) {
-      int y1, z1;
-      mnext = batch_links<M32>(D, cell_index(threadIdx.x, y1, z1));
+    // (x, l): this thread's cell; advancing by 256 cells may cross planes
+    int x = xa;
+    unsigned l = threadIdx.x;
+    while (l >= plane_cells && x <= xb) {
+      l -= plane_cells;
+      ++x;
     }
-    for (unsigned l = threadIdx.x; l < plane_cells; l += 256u) {
+    uint2 mnext = make_uint2(0u, 0u);
+    if (masked && x <= xb) {
+      int y1, z1;
+      mnext = batch_links<M32>(D, cell_index(x, l, y1, z1));
+    }
+    while (x <= xb) {
       int y, z;
-      const unsigned s = cell_index(l, y, z);
-      uint32_t bounce = 0, elide = 0;
-      if (FUSED && mask) {
-        bounce = mnext.x;
-        elide = mnext.y;
-        if (l + 256u < plane_cells) {
-          int y1, z1;
-          mnext = batch_links<M32>(D, cell_index(l + 256u, y1, z1));
-        }
+      const unsigned s = cell_index(x, l, y, z);
+      const uint32_t bounce = mnext.x, elide = mnext.y;
+      int xn = x;
+      unsigned ln = l + 256u;
+      while (ln >= plane_cells && xn <= xb) {
+        ln -= plane_cells;
+        ++xn;
+      }
+      if (masked && xn <= xb) {
+        int y1, z1;
+        mnext = batch_links<M32>(D, cell_index(xn, ln, y1, z1));
       }
       int ox[3], oy[3], oz[3];
       nb_offsets(g, x, y, z, ox, oy, oz);
       C f[Q];
       cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, s, ox, oy, oz, bounce, f);
       cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, (M*)D.rho, (M*)D.u, x, y, z, s, ox, oy, oz, elide, f, om0);
+      x = xn;
+      l = ln;
     }
   }
 }
@@ -99,20 +126,14 @@ __global__ void __launch_bounds__(256, BLOCKS)
 // Two cells per thread: cells l and l + 256 of the plane.
 template <int Q, class S, bool ODD, bool FUSED, bool M32, int BLOCKS>
 __global__ void __launch_bounds__(256, BLOCKS)
-    k_batch_step_pair(const BatchDom* __restrict__ doms, int ndom, long long ntiles, const StepParams p) {
+    k_batch_step_pair(const BatchDom* __restrict__ doms, int ndom, const long long* __restrict__ starts,
+                      const StepParams p) {
   using C = typename Store<S>::C;
   using M = typename MacroT<S>::T;
   int d = -1;
-  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    if (d < 0) {
-      int lo = 0, hi = ndom - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (doms[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
-      }
-      d = lo;
-    }
-    while (d + 1 < ndom && doms[d + 1].tile0 <= tile) ++d;
+  const long long tend = starts[blockIdx.x + 1];
+  for (long long tile = starts[blockIdx.x]; tile < tend; ++tile) {
+    d = batch_domain(doms, ndom, tile, d);
     const BatchDom& D = doms[d];
     const GridDesc g = D.g;
     const int x = (int)(tile - D.tile0) + 1;
@@ -175,37 +196,27 @@ __global__ void __launch_bounds__(256)
   link_apply<Q, S>((S*)B.F, B.dstride, B.links, (int)(t - B.link0), B.ls, B.bp, parity);
 }
 
-inline int batch_sm_count() {
-  static int g_sms = 0;
-  if (!g_sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-  }
-  return g_sms;
-}
-
 template <int Q, class S, int SHAPE, bool M32>
-cudaError_t batch_step_shape(const BatchDom* doms, int ndom, long long ntiles, bool fused, const StepParams& p,
+cudaError_t batch_step_shape(const BatchDom* doms, int ndom, const BatchWork& w, bool fused, const StepParams& p,
                              int parity_in, cudaStream_t st) {
   constexpr int BLOCKS = batch_shape_blocks(SHAPE);
-  const long long cap = (long long)batch_sm_count() * BLOCKS;
-  const int grid = (int)(ntiles < cap ? ntiles : cap);
+  const int grid = w.grid[BLOCKS - 2];
+  const long long* starts = w.starts + w.off[BLOCKS - 2];
   if constexpr (batch_shape_pair(SHAPE)) {
     if (parity_in == 0) {
-      if (fused) k_batch_step_pair<Q, S, true, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
-      else k_batch_step_pair<Q, S, true, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+      if (fused) k_batch_step_pair<Q, S, true, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
+      else k_batch_step_pair<Q, S, true, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
     } else {
-      if (fused) k_batch_step_pair<Q, S, false, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
-      else k_batch_step_pair<Q, S, false, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+      if (fused) k_batch_step_pair<Q, S, false, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
+      else k_batch_step_pair<Q, S, false, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
     }
   } else {
     if (parity_in == 0) {
-      if (fused) k_batch_step<Q, S, true, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
-      else k_batch_step<Q, S, true, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+      if (fused) k_batch_step<Q, S, true, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
+      else k_batch_step<Q, S, true, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
     } else {
-      if (fused) k_batch_step<Q, S, false, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
-      else k_batch_step<Q, S, false, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, ntiles, p);
+      if (fused) k_batch_step<Q, S, false, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
+      else k_batch_step<Q, S, false, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
     }
   }
   return cudaGetLastError();
@@ -216,32 +227,32 @@ cudaError_t batch_step_shape(const BatchDom* doms, int ndom, long long ntiles, b
 // with one-word link masks (or none); other cases take the one-cell shape
 // with the same residency.
 template <int Q, class S, int SHAPE>
-cudaError_t batch_step_m(const BatchDom* doms, int ndom, long long ntiles, int fused, const StepParams& p,
+cudaError_t batch_step_m(const BatchDom* doms, int ndom, const BatchWork& w, int fused, const StepParams& p,
                          int parity_in, cudaStream_t st) {
   if constexpr (batch_shape_pair(SHAPE)) {
     constexpr int ONE = SHAPE == 3 ? 1 : 2;
     if constexpr (Q == 27 || sizeof(S) == 8) {
-      return batch_step_m<Q, S, ONE>(doms, ndom, ntiles, fused, p, parity_in, st);
+      return batch_step_m<Q, S, ONE>(doms, ndom, w, fused, p, parity_in, st);
     } else {
-      if (fused == 1) return batch_step_m<Q, S, ONE>(doms, ndom, ntiles, fused, p, parity_in, st);
-      return batch_step_shape<Q, S, SHAPE, true>(doms, ndom, ntiles, fused != 0, p, parity_in, st);
+      if (fused == 1) return batch_step_m<Q, S, ONE>(doms, ndom, w, fused, p, parity_in, st);
+      return batch_step_shape<Q, S, SHAPE, true>(doms, ndom, w, fused != 0, p, parity_in, st);
     }
   } else {
-    if (fused == 2) return batch_step_shape<Q, S, SHAPE, true>(doms, ndom, ntiles, true, p, parity_in, st);
-    return batch_step_shape<Q, S, SHAPE, false>(doms, ndom, ntiles, fused != 0, p, parity_in, st);
+    if (fused == 2) return batch_step_shape<Q, S, SHAPE, true>(doms, ndom, w, true, p, parity_in, st);
+    return batch_step_shape<Q, S, SHAPE, false>(doms, ndom, w, fused != 0, p, parity_in, st);
   }
 }
 
 template <int Q, class S>
-cudaError_t batch_step_impl(const BatchDom* doms, int ndom, long long ntiles, int fused, const StepParams& p,
+cudaError_t batch_step_impl(const BatchDom* doms, int ndom, const BatchWork& w, int fused, const StepParams& p,
                             int parity_in, int shape, cudaStream_t st) {
-  if (ntiles <= 0) return cudaSuccess;
+  if (w.ntiles <= 0) return cudaSuccess;
   switch (shape) {
-    case 0: return batch_step_m<Q, S, 0>(doms, ndom, ntiles, fused, p, parity_in, st);
-    case 1: return batch_step_m<Q, S, 1>(doms, ndom, ntiles, fused, p, parity_in, st);
-    case 2: return batch_step_m<Q, S, 2>(doms, ndom, ntiles, fused, p, parity_in, st);
-    case 3: return batch_step_m<Q, S, 3>(doms, ndom, ntiles, fused, p, parity_in, st);
-    case 4: return batch_step_m<Q, S, 4>(doms, ndom, ntiles, fused, p, parity_in, st);
+    case 0: return batch_step_m<Q, S, 0>(doms, ndom, w, fused, p, parity_in, st);
+    case 1: return batch_step_m<Q, S, 1>(doms, ndom, w, fused, p, parity_in, st);
+    case 2: return batch_step_m<Q, S, 2>(doms, ndom, w, fused, p, parity_in, st);
+    case 3: return batch_step_m<Q, S, 3>(doms, ndom, w, fused, p, parity_in, st);
+    case 4: return batch_step_m<Q, S, 4>(doms, ndom, w, fused, p, parity_in, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -3,12 +3,12 @@
 
 namespace aslb {
 
-cudaError_t batch_step_f16(int q, const BatchDom* doms, int ndom, long long ntiles, int fused, const StepParams& p,
+cudaError_t batch_step_f16(int q, const BatchDom* doms, int ndom, const BatchWork& w, int fused, const StepParams& p,
                            int parity_in, int shape, cudaStream_t st) {
   switch (q) {
-    case 15: return batch_step_impl<15, __half>(doms, ndom, ntiles, fused, p, parity_in, shape, st);
-    case 19: return batch_step_impl<19, __half>(doms, ndom, ntiles, fused, p, parity_in, shape, st);
-    case 27: return batch_step_impl<27, __half>(doms, ndom, ntiles, fused, p, parity_in, shape, st);
+    case 15: return batch_step_impl<15, __half>(doms, ndom, w, fused, p, parity_in, shape, st);
+    case 19: return batch_step_impl<19, __half>(doms, ndom, w, fused, p, parity_in, shape, st);
+    case 27: return batch_step_impl<27, __half>(doms, ndom, w, fused, p, parity_in, shape, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -1,5 +1,6 @@
 // Host-side launch interface of the CUDA kernels (implemented in kernels.cu).
 #pragma once
+#include <vector>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
@@ -119,10 +120,24 @@ struct BatchBc {
   LinkSet ls;
   BcParams bp;
 };
+// The work split of a batched step: the tiles in order, each block of the
+// persistent grid a contiguous run of them holding an equal share of the
+// cells (block b: tiles starts[b] .. starts[b + 1] - 1), one table per
+// residency (2, 3, 4 blocks per SM), back to back in device memory.
+struct BatchWork {
+  long long ntiles;
+  const long long* starts;  // device
+  int grid[3];              // blocks at 2, 3, 4 resident blocks per SM
+  long long off[3];         // each residency's table in starts
+};
+// Host side of the split: the per-residency tables for tiles of the given
+// cell counts on `sms` SMs (grid = min(tiles, sms x residency)).
+void batch_work_tables(const std::vector<long long>& tile_cells, int sms, std::vector<long long>& starts,
+                       int (&grid)[3], long long (&off)[3]);
 // One stream-collide step of every domain of a batch (same lattice, storage
 // and parity; CL_NONE), a persistent grid over all domains' tiles; `shape`
 // (0 .. batch_shape_count() - 1) picks the resident blocks per SM.
-cudaError_t launch_batch_step(int q, int storage, const BatchDom* doms, int ndom, long long ntiles, int fused,
+cudaError_t launch_batch_step(int q, int storage, const BatchDom* doms, int ndom, const BatchWork& w, int fused,
                               const StepParams& p, int parity_in, int shape, cudaStream_t st);
 int batch_shape_count();
 // Every link of the entries (one condition position across the batch).
