@@ -37,6 +37,22 @@ __device__ __forceinline__ uint2 batch_links(const BatchDom& D, unsigned s) {
   return D.mask[s];
 }
 
+// Collision and stores of one cell whose store offsets are recomputed after
+// the collision (y and s are made to depend on its result), so the offsets
+// used by the loads die with them instead of living across the collision.
+template <int Q, class S, bool ODD, bool MASKED>
+__device__ __forceinline__ void batch_finish(S* __restrict__ F, const GridDesc& g, const StepParams& p,
+                                             typename MacroT<S>::T* __restrict__ rho_out,
+                                             typename MacroT<S>::T* __restrict__ u_out, int x, int y, int z,
+                                             unsigned s, uint32_t elide, typename Store<S>::C (&f)[Q],
+                                             typename Store<S>::C om0) {
+  cell_collide<Q, S, CL_NONE>(g, p, rho_out, u_out, x, y, z, s, f, om0);
+  const int y2 = (int)after((unsigned)y, f[0]);
+  int ox[3], oy[3], oz[3];
+  nb_offsets(g, x, y2, z, ox, oy, oz);
+  cell_store<Q, S, ODD, MASKED>(F, p, (unsigned)g.dstride, after(s, f[0]), ox, oy, oz, elide, f);
+}
+
 // The domain holding `tile`, searched from d (tiles ascend in the table).
 __device__ __forceinline__ int batch_domain(const BatchDom* __restrict__ doms, int ndom, long long tile, int d) {
   if (d < 0) {
@@ -116,7 +132,7 @@ __global__ void __launch_bounds__(256, BLOCKS)
       nb_offsets(g, x, y, z, ox, oy, oz);
       C f[Q];
       cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, s, ox, oy, oz, bounce, f);
-      cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, (M*)D.rho, (M*)D.u, x, y, z, s, ox, oy, oz, elide, f, om0);
+      batch_finish<Q, S, ODD, FUSED>(F, g, p, (M*)D.rho, (M*)D.u, x, y, z, s, elide, f, om0);
       x = xn;
       l = ln;
     }
@@ -174,10 +190,8 @@ __global__ void __launch_bounds__(256, BLOCKS)
         nb_offsets(g, x, yb, zb, ox, oyb, ozb);
         cell_load<Q, S, ODD, FUSED>(F, (unsigned)g.dstride, sb, ox, oyb, ozb, mb.x, fb);
       }
-      cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, (M*)D.rho, (M*)D.u, x, ya, za, sa, ox, oya, oza, ma.y, fa, om0);
-      if (has_b)
-        cell_finish<Q, S, CL_NONE, ODD, FUSED>(F, g, p, (M*)D.rho, (M*)D.u, x, yb, zb, sb, ox, oyb, ozb, mb.y, fb,
-                                               om0);
+      batch_finish<Q, S, ODD, FUSED>(F, g, p, (M*)D.rho, (M*)D.u, x, ya, za, sa, ma.y, fa, om0);
+      if (has_b) batch_finish<Q, S, ODD, FUSED>(F, g, p, (M*)D.rho, (M*)D.u, x, yb, zb, sb, mb.y, fb, om0);
     }
   }
 }
