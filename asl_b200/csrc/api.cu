@@ -1791,7 +1791,7 @@ int batch_tables(aslb_batch* b, aslb_bc* const* bcs, const int* nbc) {
     ASLB_CUDA(cudaGetDevice(&dev));
     ASLB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     std::vector<long long> starts;
-    batch_work_tables(tile_cells, sms, starts, b->work.grid, b->work.off);
+    batch_work_tables(tile_cells, sms, starts, b->work.grid, b->work.group, b->work.off);
     ASLB_CUDA(cudaMalloc((void**)&b->dev_starts, starts.size() * sizeof(long long)));
     ASLB_CUDA(cudaMemcpy(b->dev_starts, starts.data(), starts.size() * sizeof(long long), cudaMemcpyHostToDevice));
     b->work.ntiles = b->ntiles;

@@ -18,19 +18,22 @@ cudaError_t batch_links_f64(int q, const BatchBc* bcs, int nbc, long long nlinks
 int batch_shape_count() { return 5; }
 
 void batch_work_tables(const std::vector<long long>& tile_cells, int sms, std::vector<long long>& starts,
-                       int (&grid)[3], long long (&off)[3]) {
+                       int (&grid)[3], int (&group)[3], long long (&off)[3]) {
   const long long T = (long long)tile_cells.size();
   long long C = 0;
   for (long long c : tile_cells) C += c;
   starts.clear();
   for (int k = 0; k < 3; ++k) {
     const long long G = std::max(1LL, std::min(T, (long long)sms * (k + 2)));
+    const int K = (G % 4 == 0) ? 4 : 1;
+    const long long NG = G / K;
     grid[k] = (int)G;
+    group[k] = K;
     off[k] = (long long)starts.size();
-    // block b starts at the first tile whose preceding cells reach b C / G
+    // group b starts at the first tile whose preceding cells reach b C / NG
     long long t = 0, before = 0;
-    for (long long b = 0; b < G; ++b) {
-      const long long target = (long long)(((__int128)b * C + G - 1) / G);
+    for (long long b = 0; b < NG; ++b) {
+      const long long target = (long long)(((__int128)b * C + NG - 1) / NG);
       while (t < T && before < target) before += tile_cells[t++];
       starts.push_back(t);
     }

@@ -5,8 +5,9 @@
 // layout; a device table maps the launch's tiles (one x plane of one domain,
 // its cells taken 256 at a time, z fastest across y rows) and links to
 // domains. Each block of the persistent grid takes a contiguous run of tiles
-// holding an equal share of the batch's cells (BatchWork), so its domain
-// changes rarely and consecutive planes of a domain follow one another.
+// holding an equal share of the batch's cells (BatchWork), the blocks of a
+// group of four interleaving its planes, so a block's domain changes rarely
+// and neighbouring planes of a domain are streamed together.
 // Instantiated per storage in batch_<type>.cu.
 #pragma once
 #include "kernels.h"
@@ -67,28 +68,31 @@ __device__ __forceinline__ int batch_domain(const BatchDom* __restrict__ doms, i
   return d;
 }
 
-// One cell per thread. A block walks its run of tiles; the tiles of one
-// domain in the run are consecutive x planes, walked as one sequence of
-// cells 256 at a time, so the next cell's link word is fetched one step
-// ahead across plane boundaries too and the domain's table entry is read
-// once per domain, not once per plane.
+// One cell per thread. The blocks of a group share a run of tiles and take
+// every group-th tile of it (block j: tiles j, j + K, ...), so neighbouring
+// planes, whose populations each pulls from the other, are streamed at the
+// same time by neighbouring blocks; a block's planes of one domain are walked
+// as one sequence of cells 256 at a time, so the next cell's link word is
+// fetched one step ahead across plane boundaries too and the domain's table
+// entry is read once per domain, not once per plane.
 template <int Q, class S, bool ODD, bool FUSED, bool M32, int BLOCKS>
 __global__ void __launch_bounds__(256, BLOCKS)
-    k_batch_step(const BatchDom* __restrict__ doms, int ndom, const long long* __restrict__ starts,
+    k_batch_step(const BatchDom* __restrict__ doms, int ndom, const long long* __restrict__ starts, int K,
                  const StepParams p) {
   using C = typename Store<S>::C;
   using M = typename MacroT<S>::T;
-  long long tile = starts[blockIdx.x];
-  const long long tend = starts[blockIdx.x + 1];
+  const int grp = (int)blockIdx.x / K;
+  long long tile = starts[grp] + (int)blockIdx.x % K;
+  const long long tend = starts[grp + 1];
   int d = -1;
   while (tile < tend) {
     d = batch_domain(doms, ndom, tile, d);
     const BatchDom& D = doms[d];
     const GridDesc g = D.g;
-    // this domain's planes in the run
+    // this block's planes of the domain in the run: xa, xa + K, ... <= xb
     const int xa = (int)(tile - D.tile0) + 1;
     const int xb = (int)(min(tend, D.tile0 + g.nx) - D.tile0);
-    tile = D.tile0 + xb;
+    tile += (long long)K * ((xb - xa) / K + 1);
     const unsigned plane_cells = (unsigned)(g.ny * g.nz);
     const unsigned nz = (unsigned)g.nz, nz_inv = D.nz_inv;
     S* F = (S*)D.F;
@@ -107,7 +111,7 @@ __global__ void __launch_bounds__(256, BLOCKS)
     unsigned l = threadIdx.x;
     while (l >= plane_cells && x <= xb) {
       l -= plane_cells;
-      ++x;
+      x += K;
     }
     uint2 mnext = make_uint2(0u, 0u);
     if (masked && x <= xb) {
@@ -122,7 +126,7 @@ __global__ void __launch_bounds__(256, BLOCKS)
       unsigned ln = l + 256u;
       while (ln >= plane_cells && xn <= xb) {
         ln -= plane_cells;
-        ++xn;
+        xn += K;
       }
       if (masked && xn <= xb) {
         int y1, z1;
@@ -142,13 +146,14 @@ __global__ void __launch_bounds__(256, BLOCKS)
 // Two cells per thread: cells l and l + 256 of the plane.
 template <int Q, class S, bool ODD, bool FUSED, bool M32, int BLOCKS>
 __global__ void __launch_bounds__(256, BLOCKS)
-    k_batch_step_pair(const BatchDom* __restrict__ doms, int ndom, const long long* __restrict__ starts,
+    k_batch_step_pair(const BatchDom* __restrict__ doms, int ndom, const long long* __restrict__ starts, int K,
                       const StepParams p) {
   using C = typename Store<S>::C;
   using M = typename MacroT<S>::T;
   int d = -1;
-  const long long tend = starts[blockIdx.x + 1];
-  for (long long tile = starts[blockIdx.x]; tile < tend; ++tile) {
+  const int grp = (int)blockIdx.x / K;
+  const long long tend = starts[grp + 1];
+  for (long long tile = starts[grp] + (int)blockIdx.x % K; tile < tend; tile += K) {
     d = batch_domain(doms, ndom, tile, d);
     const BatchDom& D = doms[d];
     const GridDesc g = D.g;
@@ -214,23 +219,23 @@ template <int Q, class S, int SHAPE, bool M32>
 cudaError_t batch_step_shape(const BatchDom* doms, int ndom, const BatchWork& w, bool fused, const StepParams& p,
                              int parity_in, cudaStream_t st) {
   constexpr int BLOCKS = batch_shape_blocks(SHAPE);
-  const int grid = w.grid[BLOCKS - 2];
+  const int grid = w.grid[BLOCKS - 2], K = w.group[BLOCKS - 2];
   const long long* starts = w.starts + w.off[BLOCKS - 2];
   if constexpr (batch_shape_pair(SHAPE)) {
     if (parity_in == 0) {
-      if (fused) k_batch_step_pair<Q, S, true, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
-      else k_batch_step_pair<Q, S, true, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
+      if (fused) k_batch_step_pair<Q, S, true, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, K, p);
+      else k_batch_step_pair<Q, S, true, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, K, p);
     } else {
-      if (fused) k_batch_step_pair<Q, S, false, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
-      else k_batch_step_pair<Q, S, false, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
+      if (fused) k_batch_step_pair<Q, S, false, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, K, p);
+      else k_batch_step_pair<Q, S, false, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, K, p);
     }
   } else {
     if (parity_in == 0) {
-      if (fused) k_batch_step<Q, S, true, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
-      else k_batch_step<Q, S, true, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
+      if (fused) k_batch_step<Q, S, true, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, K, p);
+      else k_batch_step<Q, S, true, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, K, p);
     } else {
-      if (fused) k_batch_step<Q, S, false, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
-      else k_batch_step<Q, S, false, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, p);
+      if (fused) k_batch_step<Q, S, false, true, M32, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, K, p);
+      else k_batch_step<Q, S, false, false, false, BLOCKS><<<grid, 256, 0, st>>>(doms, ndom, starts, K, p);
     }
   }
   return cudaGetLastError();

@@ -120,20 +120,23 @@ struct BatchBc {
   LinkSet ls;
   BcParams bp;
 };
-// The work split of a batched step: the tiles in order, each block of the
-// persistent grid a contiguous run of them holding an equal share of the
-// cells (block b: tiles starts[b] .. starts[b + 1] - 1), one table per
+// The work split of a batched step: the tiles in order, each group of
+// `group` blocks of the persistent grid a contiguous run of them holding an
+// equal share of the cells (group g: tiles starts[g] .. starts[g + 1] - 1,
+// block j of the group every group-th of them from the j-th), one table per
 // residency (2, 3, 4 blocks per SM), back to back in device memory.
 struct BatchWork {
   long long ntiles;
   const long long* starts;  // device
   int grid[3];              // blocks at 2, 3, 4 resident blocks per SM
+  int group[3];             // blocks per group (the grid is a multiple)
   long long off[3];         // each residency's table in starts
 };
 // Host side of the split: the per-residency tables for tiles of the given
-// cell counts on `sms` SMs (grid = min(tiles, sms x residency)).
+// cell counts on `sms` SMs (grid = min(tiles, sms x residency), in groups of
+// four blocks where that divides it).
 void batch_work_tables(const std::vector<long long>& tile_cells, int sms, std::vector<long long>& starts,
-                       int (&grid)[3], long long (&off)[3]);
+                       int (&grid)[3], int (&group)[3], long long (&off)[3]);
 // One stream-collide step of every domain of a batch (same lattice, storage
 // and parity; CL_NONE), a persistent grid over all domains' tiles; `shape`
 // (0 .. batch_shape_count() - 1) picks the resident blocks per SM.
