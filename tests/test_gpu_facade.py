@@ -81,3 +81,41 @@ def test_pressure_channel_program_matches_oracle(gpu, oracle_mod, tmp_path):
     guard = (m[1:-1, 1:-1, 1:-1] <= 0) & (m[1:-1, 1:-1, 1:-1] > -0.9999)
     assert guard.any()
     assert rel(out["v"][:, guard], o.get_u()[:, 1:-1, 1:-1, 1:-1][:, guard]) <= 1e-4
+
+
+def test_read_surface_matches_python_reader(gpu, tmp_path):
+    """readSurface (STL) through the C++ API: the block, spacing and offset
+    overloads give the Python reader's maps and blocks bit for bit."""
+    from asl_b200 import surface as S
+    # a box and a tilted triangle fan, file coordinates (x, y, z)
+    lo, hi = np.array([1.0, 0.5, -1.5]), np.array([4.0, 3.0, 2.5])
+    v = np.array([[lo[0], lo[1], lo[2]], [hi[0], lo[1], lo[2]], [hi[0], hi[1], lo[2]], [lo[0], hi[1], lo[2]],
+                  [lo[0], lo[1], hi[2]], [hi[0], lo[1], hi[2]], [hi[0], hi[1], hi[2]], [lo[0], hi[1], hi[2]]])
+    faces = [(0, 2, 1), (0, 3, 2), (4, 5, 6), (4, 6, 7), (0, 1, 5), (0, 5, 4), (2, 3, 7), (2, 7, 6), (1, 2, 6),
+             (1, 6, 5), (0, 4, 7), (0, 7, 3)]
+    tri = np.array([[v[a], v[b], v[c]] for a, b, c in faces] + [[[0.0, 0.0, 0.0], [1.0, 0.2, 0.1], [0.3, 1.0, 0.4]]])
+    path = tmp_path / "shape.stl"
+    S.writeSTL(str(path), tri)
+    src = ROOT / "tests" / "cpp" / "facade_surface.cc"
+    cxx = shutil.which("g++") or "/usr/bin/g++"
+    exe = tmp_path / "facade_surface"
+    r = subprocess.run([cxx, "-std=c++17", "-O2", "-Wall", "-Werror", "-I", str(ROOT / "include" / "asl"), "-I",
+                        str(ROOT / "include"), str(src), "-L", str(ROOT / "asl_b200"), "-laslb",
+                        "-Wl,-rpath," + str(ROOT / "asl_b200"), "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe), str(path)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    got = {ln.split(" ", 1)[0]: ln.split(" ", 1)[1] for ln in r.stdout.splitlines()}
+    want = {"block": S.readSurface(str(path), Block((24, 16, 12), 0.5, (-2.0, -1.0, 0.5))),
+            "spacing": S.readSurface(str(path), 0.5),
+            "offsets": S.readSurface(str(path), 0.5, 0.5, 0.25, 0.0, 1.0, 1.0, 0.5)}
+    for k, m in want.items():
+        f = got[k].split()
+        b = m.getInternalBlock()
+        assert tuple(int(x) for x in f[:3]) == tuple(b.size), k
+        assert np.allclose([float(x) for x in f[3:6]], b.position, rtol=0, atol=1e-12), k
+        assert float(f[6]) == b.dx, k
+        vals = np.array([int(h, 16) for h in f[7:]], dtype=np.uint32).view(np.float32)
+        assert np.array_equal(vals.reshape(m.shape), np.asarray(m, dtype=np.float32)), k
+        assert np.asarray(m).min() < 0 < np.asarray(m).max()  # the surface lies inside the sampled grid
+    assert got["error"] == "ASL ERROR: Reader: file format not supported"
