@@ -99,6 +99,16 @@ int main(int argc, char* argv[]) {
   std::printf("writes %u\n", writer.getNumOfWrites());
   std::printf("params %d %d %d %.3f %s\n", size.v()[0], size.v()[1], size.v()[2], radius.v(), out.v().c_str());
 
+  // constant values per component, and the parameters directory
+  auto cv = asl::generateDataContainerACL_SP<float>(asl::Block(makeAVec(3, 2, 2)), 3, 1u);
+  asl::initData(cv, makeAVec(1.5, -2., 0.25));
+  const std::vector<double>& cvv = cv->values();
+  const size_t cn = cv->cells();
+  EXPECT(cvv[0] == 1.5 && cvv[cn - 1] == 1.5 && cvv[cn] == -2. && cvv[3 * cn - 1] == 0.25);
+  asl::initData(cv, 0.75);
+  EXPECT(cv->values()[2 * cn] == 0.75);
+  std::printf("dir %s\n", pm.getDir().c_str());
+
   // errors carry ASL's prefix
   try {
     asl::offset(asl::Block(makeAVec(1, 1, 1)), -2);

@@ -46,6 +46,7 @@ def test_facade_host_side(tmp_path):
     assert r.returncode == 0, r.stderr
     lines = {ln.split(" ", 1)[0]: ln.split(" ", 1)[1] for ln in r.stdout.splitlines()}
     assert lines["params"] == "9 7 6 2.500 " + str(tmp_path / "fh")
+    assert lines["dir"] == str(tmp_path.resolve()) + "/"  # no parameters file: the working directory
     assert lines["writes"] == "2"
     assert lines["error"] == "ASL ERROR: The inset is larger than the block size"
     # the FP32 map is bit for bit the Python rasteriser's (ASL's FP32 evaluation)
