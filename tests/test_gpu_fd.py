@@ -136,3 +136,22 @@ def test_electric_field_term_matches_oracle(gpu, q, with_flow, dtype, tol):
     assert np.abs(got - ref).max() <= tol
     plain = fd_step(fd_step(c, 0.05, q), 0.05, q)
     assert np.abs(ref - plain).max() > 1e-5  # the term acts
+
+
+@pytest.mark.parametrize("q", [15, 19])
+@pytest.mark.parametrize("cc", [False, True])
+def test_register_blocked_runs_across_tiles_match_oracle(gpu, q, cc):
+    """FP32 d3q15 / d3q19 on a grid with more plane-tile units than resident
+    blocks (each block walks a run of planes that crosses into the next
+    tile, restarting its ring there), partial tiles in y and z."""
+    w = W.channel_cylinder(size=(200, 20, 70), radius=4.0, center=(40.0, 10.0), u_in=0.04)
+    lb, bcs = W.build_lbgk(w, "f32")
+    c = blob(tuple(s + 2 for s in w.size), np.float32)
+    fd = FD.generateFDAdvectionDiffusion(c, 0.05, lb, q, compressibilityCorrection=cc)
+    FD.generateBCConstantValue(fd, 1.0, [A.X0])
+    ref = fd.getC()
+    for _ in range(3):
+        lb.run(1, bcs)
+        fd.execute()
+        ref = fd_step(ref, 0.05, q, lb.getVelocity(np.float32), cc)
+    assert np.abs(fd.getC() - ref).max() <= 5e-6
