@@ -102,3 +102,25 @@ def test_batch_launch_shapes_identical_and_tuned(gpu, storage):
     assert len(t) == 5 and batch.shape == int(np.argmin(t))
     for lb in lbs:
         assert lb.steps == 14
+
+
+def test_batch_runs_across_domains_bitwise(gpu):
+    """More tiles than resident blocks: every group of blocks walks a run of
+    planes crossing domain boundaries, its blocks interleaving the planes.
+    Every launch shape gives the populations of the domains stepped alone."""
+    ws = small_batch(12, seed=23)
+    steps = 6
+    refs = []
+    for w in ws:
+        ref, rbcs = W.build_lbgk(w, storage="f32", compVel=False, compRho=False, fuse=True)
+        ref.run(steps, rbcs)
+        ref.sync()
+        refs.append(ref.getF())
+    for shape in (0, 1, 2, 3, 4):
+        batch, lbs, bcs = W.build_batch(ws, storage="f32")
+        batch.setShape(shape)
+        batch.run(steps, bcs)
+        batch.sync()
+        assert batch.tiles > 4 * 148  # more tiles than blocks at every residency of a B200
+        for w, lb, ref in zip(ws, lbs, refs):
+            assert np.array_equal(lb.getF(), ref, equal_nan=True), (shape, w.name)
