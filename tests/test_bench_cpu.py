@@ -27,3 +27,18 @@ def test_reference_arm_other_ranks_exit_quietly():
                         "--steps", "1", "--warmup", "1"], capture_output=True, text=True, timeout=600,
                        env={**os.environ, **env})
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_reference_arm_rank0_names_the_slab_job():
+    """Under a launcher with N ranks, rank 0 samples one slab of the N-slab
+    job our arm runs and names that job in its config."""
+    import os
+    env = {"RANK": "0", "WORLD_SIZE": "2", "LOCAL_RANK": "0"}
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2", "--size",
+                        "48,24,24", "--steps", "1", "--warmup", "1"], capture_output=True, text=True, timeout=600,
+                       env={**os.environ, **env})
+    assert r.returncode == 0, r.stderr
+    line = json.loads([s for s in r.stdout.splitlines() if s.startswith("{")][-1])
+    assert line["config"]["workload"] == "porous_channel_d3q19_96x24x24"
+    assert line["config"]["cells"] == 2 * 48 * 24 * 24
+    assert "slab" in line["cpu_baseline"]["sample"] and line["n_gpus"] == 2
