@@ -196,8 +196,8 @@ __global__ void __launch_bounds__(kFdTZ * kFdTY) k_fd_step(const T* __restrict__
 // with the laplacian and both sums accumulated per coefficient class (axis,
 // edge or corner vectors) and scaled once; q_i = -q_opp(i) is formed once per
 // pair. Work: the tiles' planes in tile-major order, an equal run of them per
-// resident block (a run crosses at most into the next tile and restarts the
-// ring there).
+// resident block (a run that crosses into the next tile restarts the ring
+// there).
 constexpr int kRbTZ = 32;
 
 // The tile and its ring (two resident blocks of 256 threads per SM). KZ
