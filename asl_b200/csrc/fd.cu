@@ -183,14 +183,14 @@ __global__ void __launch_bounds__(kFdTZ * kFdTY) k_fd_step(const T* __restrict__
 }
 
 // Register-blocked FP32 step (no electric term) for the d3q15 / d3q19
-// templates: a block of 32 (z) x 8 (y) threads owns a 64 x 16 tile of a
-// plane, each thread a 2 x 2 block of cells (two consecutive z, two
+// templates: a block of 32 (z) x 4 (y) threads owns a 64 x 16 tile of a
+// plane, each thread a 4 x 2 block of cells (two consecutive z, four
 // consecutive y). Three planes of the tile with its one-cell halo sit in a
 // ring of four shared-memory slots; plane x + 2 is loaded into registers
 // during plane x and stored to its slot at the top of the next iteration.
 // The stencil reads of a thread's cells overlap, the unrolled cells read each
 // shared value once, and a thread's two middle columns are one 8-byte load
-// (about 23 shared loads per d3q19 cell instead of 52). The update is ASL's,
+// (about 19 shared loads per d3q19 cell instead of 52). The update is ASL's,
 // regrouped per link i:
 //   divProduct = sum_i GC_i / 2 (c_i + c_0) (p_i + q_i),
 //   p_i = e_i . u(x + e_i), q_i = e_i . u(x), div(u) = sum_i GC_i p_i,
@@ -201,12 +201,13 @@ __global__ void __launch_bounds__(kFdTZ * kFdTY) k_fd_step(const T* __restrict__
 // there).
 constexpr int kRbTZ = 32;
 
-// The tile and its ring (two resident blocks of 256 threads per SM). KZ
+// The tile and its ring (two resident blocks of 128 threads per SM: eight
+// cells per thread outweigh the lower occupancy; 198 registers). KZ
 // consecutive z cells per thread: with two, a row's columns are shifted by
 // one (column c holds z0 - 1 + c) so each thread's pair sits on an 8-byte
 // boundary and is one shared load.
 struct RbConf {
-  static constexpr int TY = 8, KY = 2, KZ = 2, MINB = 2;
+  static constexpr int TY = 4, KY = 4, KZ = 2, MINB = 2;
   static constexpr int CO = KZ == 2 ? 1 : 0;       // column of ghosted z0
   static constexpr int TZ = kRbTZ * KZ;            // tile cells along z
   static constexpr int H = TY * KY + 2;            // tile rows with the halo

@@ -441,7 +441,7 @@ def fd_run(W, w, steps: int, peak: float):
         fd.close()
     out["bytes_per_cell"] = 20
     out["note"] = ("FP32, velocity read from the LBGK's device field; d3q7: k_fd_step (32 x 8 cell tiles walking 32 "
-                   "x planes); d3q19: k_fd_step_rb (64 x 16 tiles, 2 x 2 cells per thread, a ring of four "
+                   "x planes); d3q19: k_fd_step_rb (64 x 16 tiles, 4 x 2 cells per thread, a ring of four "
                    "shared-memory planes, equal runs of planes per resident block)")
     del lb, bcs
     return out
